@@ -1,0 +1,225 @@
+/*
+ * droplet.h -- C ABI of the B200 (sm_100a) Lagrangian droplet engine.
+ *
+ * Drop-in boundary for the particle block of thenumer8or/MPI_2D_domain_decomp_turb_particles
+ * (turb.f90:546-623).  Each entry point replaces one external Fortran subroutine of
+ * partlib.f90; the citation beside each declaration names the subroutine and the
+ * lines it replaces.  All arrays crossing this boundary keep the reference's Fortran
+ * column-major layouts (module PARAMS, global.f90:1-57):
+ *
+ *   yp(8, nps)      1-3 position, 4-6 droplet velocity, 7 radius (DNS units), 8 id
+ *   vp(3, nps)      fluid velocity interpolated at the droplet
+ *   fvp(3, 0:2, nps), fdp(3, 0:3, nps)   velocity / fluid-velocity history levels
+ *   dmove(3, nps)   displacement of the current step
+ *   v(llx, ly, lz)  one physical-space velocity component, x fastest
+ *
+ * Conventions
+ *   - Every function returns int: 0 = OK, > 0 = warning (e.g. GMRES not converged),
+ *     < 0 = error (capacity overflow, overlap under HDI, iteration cap, CUDA failure).
+ *     dl_last_error() returns the message of the last non-zero status.  Where the
+ *     reference calls `mpi_finalize; STOP` the library returns an error instead.
+ *   - One context per device; a context is not thread-safe.  Calls are ordered on the
+ *     context's CUDA stream; functions that return host data synchronise it.
+ *   - The droplet state lives in device memory between calls, in a device order of
+ *     its own (sorted by space); the order and indices seen through this ABI are the
+ *     reference's (yp column ih <-> droplet ih), including the reordering PERIODIC and
+ *     COALESCE perform.
+ *   - Single GPU: the reference's 2D pencil decomposition collapses to one rank
+ *     (nprocY = nprocZ = 1, every MPI neighbour is the rank itself).
+ */
+#ifndef DROPLET_H
+#define DROPLET_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DL_FP64 0   /* every particle quantity in FP64 */
+#define DL_MIXED 1  /* FP32 interpolation/drag/HI iterations; FP64 positions, wrap, pair tests, HI residual */
+
+#define DL_OK 0
+#define DL_W_GMRES_NOT_CONVERGED 1
+#define DL_E_ARG -1
+#define DL_E_CUDA -2
+#define DL_E_ALLOC -3
+#define DL_E_GEOMETRY -4        /* partlib.f90:169-222 feasibility STOPs */
+#define DL_E_CAPACITY -5        /* msize/newsize/collist/event buffers full */
+#define DL_E_OVERLAP_HDI -6     /* partlib.f90:3294-3299 */
+#define DL_E_NEI_CAPACITY -7    /* partlib.f90:3308 */
+#define DL_E_ITER_CAP -8        /* OVERLAP_DET sweeps or a device loop hit its cap */
+#define DL_E_STATE -9           /* call out of sequence (e.g. no field set) */
+
+typedef struct dl_ctx dl_ctx;
+
+/* parameter.d fields read by the particle path (turb.f90:101-167), plus build choices. */
+typedef struct dl_params {
+    int nx, ny, nz;              /* grid (cubic grids; ncdy = ncdz = nx as partlib.f90:33-35) */
+    int npart;                   /* total droplets */
+    int nset;                    /* number of radius sets (<= 10) */
+    double radius_um[10];        /* set radii in micrometres */
+    double dt, rnu;
+    double rho_water, rho_air;   /* g/cm^3 */
+    double etk_dns, tauk_dns;    /* DNS Kolmogorov length and time */
+    double st;                   /* shell thickness in % */
+    double ediss_cloud, viscosity_cloud, gravity;  /* cgs */
+    int new_particle, nonoverlap, hdi_included, ndrag;
+    double hdi_trunc;            /* HDI truncation radius in droplet radii */
+    int msize;                   /* droplet capacity; 0 -> 20*npart (partlib.f90:30-31) */
+    int ncollmax;                /* collided-pair capacity per step; 0 -> 100 (partlib.f90:38) */
+    int nei_max;                 /* HDI neighbours per droplet; 0 -> 100 (partlib.f90:3230) */
+    int mevent;                  /* contact records per step; 0 -> 10*npart (partlib.f90:1198) */
+    /* ---- B200 build choices (no reference counterpart) ---- */
+    int precision;               /* DL_FP64 or DL_MIXED */
+    int init_velocity;           /* 0: terminal velocity (partlib.f90:564-566); 1: fluid velocity; 2: fluid + terminal */
+    int resort_interval;         /* steps between spatial re-sorts of the device order; 0 -> 16 */
+    int device;                  /* CUDA device ordinal */
+} dl_params;
+
+/* Derived scalars of PART_INIT (partlib.f90:104-157). */
+typedef struct dl_scalars {
+    double radius[10];           /* set radii in DNS units */
+    double radmax, d_coll, d_hdi;
+    double tau_cloud_const, tau_cloud_const2, sv_const, gravity_dns, ucharac;
+    double etk_cloud, tauk_cloud, vk_ratio, etk_ratio, tauk_ratio, pi2;
+    int ncdx, ncdy, ncdz, nx_coll, ny_coll, nz_coll, nx_hdi, ny_hdi, nz_hdi, nx_max, ny_max, nz_max;
+    int nps, msize, newsize;
+} dl_scalars;
+
+/* Outputs of one COLLISION_DET call (partlib.f90:1166-1846). */
+typedef struct dl_coll_report {
+    int icc[3];                  /* type I, II, III counts */
+    int ncoll;                   /* length of the sorted removal list removepart(:,0) */
+    int ntotpair;                /* collided pairs recorded in collist */
+    int ncontact;                /* contact-shell records (Vp11/12/22.dat) */
+    int written;                 /* 1 if this call reached the 5-step histogram boundary */
+    int64_t candidate_pairs;     /* (ih1, ih2 > ih1) pairs visited in the searched cells */
+} dl_coll_report;
+
+/* GMRES summary (partlib.f90:2795-3005). */
+typedef struct dl_gmres_report {
+    int iterations;              /* Krylov iterations in the last solve */
+    int refinements;             /* FP64 residual-refinement sweeps (mixed precision) */
+    double residual;             /* final relative residual */
+    double norm_rhs;             /* ||b - A x0|| */
+} dl_gmres_report;
+
+/* ---------------------------------------------------------------------------------------
+ * Context
+ * ------------------------------------------------------------------------------------- */
+/* Allocates device state for p->msize droplets; no reference counterpart (the Fortran
+ * module allocates in PART_INIT, partlib.f90:40-77). */
+int dl_create(const dl_params *p, dl_ctx **out);
+int dl_destroy(dl_ctx *ctx);
+const char *dl_last_error(const dl_ctx *ctx);
+int dl_sync(dl_ctx *ctx);
+/* Step counter istep and physical time (turb.f90:496-497, 693). */
+int dl_set_step(dl_ctx *ctx, int istep, double time);
+
+/* ---------------------------------------------------------------------------------------
+ * Droplet state, Fortran layouts
+ * ------------------------------------------------------------------------------------- */
+/* PART_INIT(id, part_in), partlib.f90:15-301: unit scaling, cell sizes, feasibility
+ * checks and (new_particle) the seeded ranpp positions with radius by index block. */
+int dl_part_init(dl_ctx *ctx);
+int dl_get_scalars(dl_ctx *ctx, dl_scalars *out);
+/* LOAD_PARTICLE, load_save.f90:100-125: nps then yp(:,1:nps), fvp(:,0:2,1:nps),
+ * fdp(:,0:3,1:nps) from host memory.  vp is reset to 0. */
+int dl_set_particles(dl_ctx *ctx, int nps, const double *yp, const double *fvp, const double *fdp);
+/* SAVE_PARTICLE, load_save.f90:129-154 (plus vp and dmove): any pointer may be NULL. */
+int dl_get_particles(dl_ctx *ctx, int *nps, double *yp, double *fvp, double *fdp, double *vp, double *dmove);
+/* Fortran-layout HDI disturbance velocity pertvel(3, nps) (partlib.f90:69). */
+int dl_get_pertvel(dl_ctx *ctx, double *pertvel);
+int dl_set_pertvel(dl_ctx *ctx, const double *pertvel);
+
+/* ---------------------------------------------------------------------------------------
+ * Velocity field
+ * ------------------------------------------------------------------------------------- */
+/* Sets component icpt (1..3) of the physical-space field that INTERPOLATE reads:
+ * element (ix, iy, iz) (0-based) is v[ix + pitch_y*iy + pitch_z*iz]; pitch_y = llx = nx+2
+ * and pitch_z = llx*lly for the reference's v(llx, lly, lz).  on_device != 0 means v is
+ * a device pointer that stays valid until the next call; otherwise it is copied.  The
+ * mixed path converts it to its FP32 periodic-halo copy. */
+int dl_set_field(dl_ctx *ctx, int icpt, const double *v, int64_t pitch_y, int64_t pitch_z, int on_device);
+/* Mixed path only: the FP32 periodic-halo field produced on the device by a flow solver,
+ * layout [3][nz+7][ny+7][dl_field_f32_pitch()] with 3 halo planes below and 4 above in
+ * every direction.  Used in place of dl_set_field. */
+int dl_set_field_f32(dl_ctx *ctx, const float *dev_ptr);
+int64_t dl_field_f32_pitch(const dl_ctx *ctx);
+int64_t dl_field_f32_elems(const dl_ctx *ctx);
+
+/* ---------------------------------------------------------------------------------------
+ * The particle subroutines, in the order turb.f90:553-610 calls them
+ * ------------------------------------------------------------------------------------- */
+int dl_prepare_interp(dl_ctx *ctx);                         /* PREPARE_INTERP(id), partlib.f90:305-347 */
+/* PREPARE_INTERP outputs in reference order: lhnode(3, nps) as lhnode[ih*3 + d] and
+ * bg(6, 3, nps) as bg[(ih*3 + d)*6 + n] (the reference stores bg(msize,6,3)). */
+int dl_get_interp_weights(dl_ctx *ctx, int *lhnode, double *bg);
+/* INTERPOLATE(v, icpt, id), partlib.f90:351-520, on the field set for icpt.  bg/lhnode
+ * are recomputed from the positions, which PREPARE_INTERP left unchanged. */
+int dl_interpolate(dl_ctx *ctx, int icpt);
+int dl_part_history_fvp(dl_ctx *ctx);                       /* PART_HISTORY_FVP(id), partlib.f90:553-595 */
+int dl_headlist(dl_ctx *ctx, double dist);                  /* HEADLIST(id, dist), partlib.f90:2171-2444 */
+int dl_nei_list_precomp(dl_ctx *ctx);                       /* NEI_LIST_PRECOMP(id), partlib.f90:3218-3371 */
+int dl_hdi_gmres(dl_ctx *ctx, dl_gmres_report *rep);        /* HDI_GMRES(id), partlib.f90:2795-3005 */
+int dl_part_history_fdp(dl_ctx *ctx);                       /* PART_HISTORY_FDP(id), partlib.f90:599-625 */
+int dl_part_advance(dl_ctx *ctx);                           /* PART_ADVANCE(id), partlib.f90:629-726 */
+int dl_complete_ypn(dl_ctx *ctx);                           /* COMPLETE_YPN(id), partlib.f90:761-838 */
+/* MEAN_VEL(id), partlib.f90:1889-1980: out = vpmean(3,nset), vpvar(3,nset),
+ * vpabs(3,nset), vphoriz(nset), vpxyz(nset) (11*nset doubles, already reduced). */
+int dl_mean_vel(dl_ctx *ctx, double *out);
+int dl_collision_det(dl_ctx *ctx, dl_coll_report *rep);     /* COLLISION_DET(id), partlib.f90:1166-1846 */
+int dl_update_part_position(dl_ctx *ctx);                   /* UPDATE_PART_POSITION(id), partlib.f90:730-757 */
+int dl_relocate(dl_ctx *ctx);                               /* RELOCATE(id), partlib.f90:1984-2012 */
+int dl_coalesce(dl_ctx *ctx);                               /* COALESCE(id), partlib.f90:3642-3825 */
+int dl_periodic(dl_ctx *ctx);                               /* PERIODIC(id), partlib.f90:842-1162 */
+int dl_overlap_det(dl_ctx *ctx, int *sweeps);               /* OVERLAP_DET(id), partlib.f90:2047-2167 */
+
+/* ---------------------------------------------------------------------------------------
+ * Fused paths (same results as the separate calls above)
+ * ------------------------------------------------------------------------------------- */
+/* The particle block of one time step, turb.f90:553-610 in order (PREPARE_INTERP ...
+ * OVERLAP_DET), with interpolation, history, advance and position update fused into
+ * one kernel when HDI is off.  istep is incremented first (turb.f90:492). */
+int dl_particle_step(dl_ctx *ctx, dl_coll_report *coll, dl_gmres_report *gmres);
+/* Interpolation + history + advance + position update + periodic wrap only (no cell
+ * list, statistics or collisions): the unit the particle-update throughput counts. */
+int dl_update_step(dl_ctx *ctx);
+
+/* ---------------------------------------------------------------------------------------
+ * Statistics (COLLISION_DET outputs), reference layouts
+ * ------------------------------------------------------------------------------------- */
+/* Accumulated histograms (nset, nset, 0:nbin-1) as written on the last 5-step boundary
+ * (partlib.f90:1659-1718): nirbin (int) and wrbin, wxbin, wybin, wzbin, urbin, thetabin,
+ * wrtanbin (double, in that order, 7*nset*nset*180 values).  Either pointer may be NULL. */
+int dl_get_histograms(dl_ctx *ctx, int written, int *nirbin, double *sums7);
+/* colltype(nset,nset) and nir(nset,nset) of the last COLLISION_DET call. */
+int dl_get_collision_counts(dl_ctx *ctx, int *colltype, int *nir);
+/* Sorted removal list removepart(1:ncoll, 0) (1-based reference indices). */
+int dl_get_removal_list(dl_ctx *ctx, int *removepart, int cap, int *ncoll);
+/* Detected pairs of the last COLLISION_DET call as rows (ih1, src2, jid2, type) with
+ * 1-based reference indices; jid2 = 0 when droplet 2 is owned, else the ghost slot
+ * 1..8 whose source is src2.  Unordered. */
+int dl_get_pairs(dl_ctx *ctx, int *rows4, int cap, int *npairs);
+/* Contact-shell records (partlib.f90:1431-1438): ints (ih1, src2, jid2) and 12 doubles
+ * (index1, index2, va(3), vb(3), xd(3), Wr) per record.  Unordered. */
+int dl_get_contacts(dl_ctx *ctx, int *ids3, double *rec12, int cap, int *ncontact);
+/* collist(20, ntotpair) in the reference's detection order (partlib.f90:1557-1562). */
+int dl_get_collist(dl_ctx *ctx, double *collist20, int cap, int *ntotpair);
+
+/* ---------------------------------------------------------------------------------------
+ * HDI neighbour lists (NEI_LIST_PRECOMP outputs)
+ * ------------------------------------------------------------------------------------- */
+/* nei_num(nps) and, per neighbour, (ih1, partner, 6 coefficients) with 1-based
+ * reference indices (partner = the ghost's source index for ghost partners). */
+int dl_get_nei(dl_ctx *ctx, int *nei_num, int *pairs2, double *coef6, int cap, int *nnz);
+
+/* Device timing of the phases of the last dl_particle_step (ms): interpolation+advance,
+ * cell list, collision detection, HDI, periodic/relocate, overlap detection. */
+int dl_get_phase_times(dl_ctx *ctx, double *ms6);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DROPLET_H */

@@ -1,0 +1,898 @@
+// Cell lists (HEADLIST), collision detection and statistics (COLLISION_DET), overlap
+// detection (OVERLAP_DET), the periodic reorder (PERIODIC) and position scatter.
+//
+// Reference: partlib.f90 HEADLIST (2171-2444), COLLISION_DET (1166-1846), FINDINDEX
+// (1850-1885), OVERLAP_DET (2047-2167), PERIODIC (842-1162).
+//
+// Single rank: HEADLIST's halo droplets are this rank's own droplets near a y or z face,
+// shifted by +-2*pi (the eight "ghost" slots).  They are materialised exactly as the
+// reference builds them, so every cell index and every shifted coordinate is the same
+// double.  Instead of a dense head/list array over (nx * (ny+2*ny_max) * (nz+2*nz_max))
+// cells, entries are counting-sorted by cell row (iy, iz) and sorted by ix inside each
+// row; a neighbour cell is then a binary search in a short row.  The set of visited
+// (ih1, ih2 > ih1) pairs is the reference's: owned partners are compared by reference
+// index (ypn order), ghosts always follow owned droplets in ypn order.
+#include "dl_internal.cuh"
+
+#include <algorithm>
+#include <climits>
+
+namespace {
+
+template <typename T>
+T *tp(void *p) { return reinterpret_cast<T *>(p); }
+
+// ---------------------------------------------------------------------------------------
+// HEADLIST cell of one ypn entry, partlib.f90:2404-2429
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void hl_cell(const DevConst &D, double x, double y, double z, int &ix, int &iy, int &iz)
+{
+    ix = 1 + (int)(x / D.hx * (double)D.ncd);
+    double dist_r = y - 0.0 * D.hy;
+    if (dist_r > 0) iy = 1 + (int)(dist_r / D.hy * (double)D.ncd);
+    else iy = -(int)(fabs(dist_r) / D.hy * (double)D.ncd);
+    double dist_b = z - 0.0 * D.hz;
+    if (dist_b > 0) iz = 1 + (int)(dist_b / D.hz * (double)D.ncd);
+    else iz = -(int)(fabs(dist_b) / D.hz * (double)D.ncd);
+    if (ix > D.ncd) ix = D.ncd;
+    if (iy > D.ncd + D.ny_max) iy = D.ncd + D.ny_max;
+    if (iy < 1 - D.ny_max) iy = 1 - D.ny_max;
+    if (iz > D.ncd + D.nz_max) iz = D.ncd + D.nz_max;
+    if (iz < 1 - D.nz_max) iz = 1 - D.nz_max;
+}
+
+// search cell of an owned droplet, partlib.f90:1253-1261 (clamped to the pencil)
+__device__ __forceinline__ void own_cell(const DevConst &D, double x, double y, double z, int &ix, int &iy, int &iz)
+{
+    ix = 1 + (int)(x / D.hx * (double)D.ncd);
+    iy = 1 + (int)((y - 0.0 * D.hy) / D.hy * (double)D.ncd);
+    iz = 1 + (int)((z - 0.0 * D.hz) / D.hz * (double)D.ncd);
+    if (ix > D.ncd) ix = D.ncd;
+    if (iy > D.ncd) iy = D.ncd;
+    if (iz > D.ncd) iz = D.ncd;
+}
+
+__device__ __forceinline__ int row_of(const DevConst &D, int iy, int iz)
+{
+    return (iz - (1 - D.nz_max)) * D.nyh + (iy - (1 - D.ny_max));
+}
+
+// ---------------------------------------------------------------------------------------
+// Ghosts, partlib.f90:2211-2351 (single rank: every shift applies)
+// ---------------------------------------------------------------------------------------
+__global__ void k_ghosts(DevConst D, int nps, const double *py, const double *pz, double dist, Ghost *g, int cap,
+                         int *cnt)
+{
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= nps) return;
+    double y = py[d], z = pz[d];
+    double d_e = fabs(1.0 * D.hy - y);
+    double d_w = fabs(0.0 * D.hy - y);
+    double d_n = fabs(1.0 * D.hz - z);
+    double d_s = fabs(0.0 * D.hz - z);
+    bool tag[8];
+    tag[0] = d_e <= dist;
+    tag[1] = sqrt(d_e * d_e + d_n * d_n) <= dist;
+    tag[2] = d_n <= dist;
+    tag[3] = sqrt(d_w * d_w + d_n * d_n) <= dist;
+    tag[4] = d_w <= dist;
+    tag[5] = sqrt(d_w * d_w + d_s * d_s) <= dist;
+    tag[6] = d_s <= dist;
+    tag[7] = sqrt(d_e * d_e + d_s * d_s) <= dist;
+    const double p = D.pi2;
+    for (int k = 0; k < 8; k++) {
+        if (!tag[k]) continue;
+        Ghost gh;
+        gh.y = y; gh.z = z; gh.src = d; gh.jid = k + 1;
+        switch (k + 1) {
+        case 1: gh.y = y - p; break;
+        case 2: gh.y = y - p; gh.z = z - p; break;
+        case 3: gh.z = z - p; break;
+        case 4: gh.y = y + p; gh.z = z - p; break;
+        case 5: gh.y = y + p; break;
+        case 6: gh.y = y + p; gh.z = z + p; break;
+        case 7: gh.z = z + p; break;
+        case 8: gh.y = y - p; gh.z = z + p; break;
+        }
+        int s = atomicAdd(cnt, 1);
+        if (s < cap) g[s] = gh;
+    }
+}
+
+__global__ void k_entry_cells(DevConst D, int nps, int ng, const double *px, const double *py, const double *pz,
+                              const Ghost *g, int *ent_row, int *ent_ix, int *row_cnt)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nps + ng) return;
+    double x, y, z;
+    if (e < nps) { x = px[e]; y = py[e]; z = pz[e]; }
+    else { const Ghost &gh = g[e - nps]; x = px[gh.src]; y = gh.y; z = gh.z; }
+    int ix, iy, iz;
+    hl_cell(D, x, y, z, ix, iy, iz);
+    int r = row_of(D, iy, iz);
+    ent_row[e] = r;
+    ent_ix[e] = ix;
+    atomicAdd(&row_cnt[r], 1);
+}
+
+__global__ void k_row_scatter(int ne, const int *ent_row, const int *ent_ix, const int *row_start, int *row_fill,
+                              long long *row_ent)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    int r = ent_row[e];
+    int s = row_start[r] + atomicAdd(&row_fill[r], 1);
+    row_ent[s] = ((long long)ent_ix[e] << 32) | (unsigned)e;
+}
+
+// Sort each row by (ix, entry).  Rows hold tens of entries for uniformly spread droplets;
+// a thread sorts a row of up to kShortRow entries, longer rows are handed to k_row_sort_long.
+constexpr int kShortRow = 64;
+constexpr int kLongRowMax = 4096;   // entries a CTA can sort in (static) shared memory
+
+__global__ void k_row_sort(int nrows, const int *row_start, long long *row_ent, int *long_rows, int *n_long)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrows) return;
+    int s = row_start[r], e = row_start[r + 1];
+    if (e - s > kShortRow) {
+        long_rows[atomicAdd(n_long, 1)] = r;
+        return;
+    }
+    for (int i = s + 1; i < e; i++) {
+        long long v = row_ent[i];
+        int j = i - 1;
+        while (j >= s && row_ent[j] > v) { row_ent[j + 1] = row_ent[j]; j--; }
+        row_ent[j + 1] = v;
+    }
+}
+
+// One CTA per long row: bitonic sort in shared memory (length padded to a power of two).
+__global__ void __launch_bounds__(1024) k_row_sort_long(const int *long_rows, const int *n_long,
+                                                        const int *row_start, long long *row_ent)
+{
+    __shared__ long long sk[kLongRowMax];
+    if ((int)blockIdx.x >= *n_long) return;
+    const int r = long_rows[blockIdx.x];
+    const int s = row_start[r], len = row_start[r + 1] - s;
+    if (len > kLongRowMax) return;   // rejected on the host before launch
+    int np2 = 1;
+    while (np2 < len) np2 <<= 1;
+    for (int i = threadIdx.x; i < np2; i += blockDim.x) sk[i] = i < len ? row_ent[s + i] : LLONG_MAX;
+    __syncthreads();
+    for (int k = 2; k <= np2; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+                int ixj = i ^ j;
+                if (ixj > i) {
+                    bool up = (i & k) == 0;
+                    long long a = sk[i], b = sk[ixj];
+                    if ((a > b) == up) { sk[i] = b; sk[ixj] = a; }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = threadIdx.x; i < len; i += blockDim.x) row_ent[s + i] = sk[i];
+}
+
+__global__ void k_max_row(int nrows, const int *row_start, int *mx)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < nrows) atomicMax(mx, row_start[r + 1] - row_start[r]);
+}
+
+// first index in [s, e) whose ix >= key
+__device__ __forceinline__ int lower_ix(const long long *re, int s, int e, int key)
+{
+    long long k = (long long)key << 32;
+    while (s < e) {
+        int m = (s + e) >> 1;
+        if (re[m] < k) s = m + 1;
+        else e = m;
+    }
+    return s;
+}
+
+// FINDINDEX, partlib.f90:1850-1885
+__device__ __forceinline__ void findindex(const DevConst &D, double r1, double r2, int &i1, int &i2)
+{
+    double diff1 = 1000000.0, diff2 = 1000000.0;
+    i1 = 1; i2 = 1;
+    for (int il = 1; il <= D.nset; il++) {
+        double a = fabs(D.radius[il - 1] - r1), b = fabs(D.radius[il - 1] - r2);
+        if (a <= diff1) { diff1 = a; i1 = il; }
+        if (b <= diff2) { diff2 = b; i2 = il; }
+    }
+    if (i2 < i1) { int t = i2; i2 = i1; i1 = t; }
+}
+
+__device__ __forceinline__ double dot3(const double *a, const double *b)
+{
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+template <typename T>
+struct CollArgs {
+    DevConst D;
+    int nps;
+    const double *px, *py, *pz;
+    const Ghost *g;
+    const int *row_start;
+    const long long *row_ent;
+    const int *ref;
+    const double *rad;
+    const T *dm[3], *vo[3], *vn[3], *up[3];
+    int imax, jmax, kmax;
+    int nbinsz;
+    int *hist_i;
+    double *hist_d;       // 7 arrays: wr, wx, wy, wz, ur, theta, wrtan
+    int *counts;          // [0..2] icc, [3] npairs, [4] ncontact, [5] nremove, [6] overflow,
+                          // [8 ..] colltype(nset^2), [8+nset^2 ..] nir(nset^2)
+    unsigned long long *cand;
+    PairRec *pairs;
+    int pair_cap;
+    ContactRec *contacts;
+    int contact_cap;
+    int *remove;
+    int remove_cap;
+};
+
+template <typename T>
+__device__ __forceinline__ void load_entry(const CollArgs<T> &A, int e, double *x, int &src, int &jid)
+{
+    if (e < A.nps) {
+        src = e; jid = 0;
+        x[0] = A.px[e]; x[1] = A.py[e]; x[2] = A.pz[e];
+    } else {
+        const Ghost &gh = A.g[e - A.nps];
+        src = gh.src; jid = gh.jid;
+        x[0] = A.px[src]; x[1] = gh.y; x[2] = gh.z;
+    }
+}
+
+// COLLISION_DET body for one owned droplet ih1 (partlib.f90:1233-1590)
+template <typename T>
+__global__ void __launch_bounds__(128) k_collision(CollArgs<T> A)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= A.nps) return;
+    const DevConst &D = A.D;
+    const int nset = D.nset;
+    double xa[3] = {A.px[a], A.py[a], A.pz[a]}, xan[3], va[3], van[3], ua[3];
+    for (int i = 0; i < 3; i++) {
+        xan[i] = xa[i] + (double)A.dm[i][a];
+        va[i] = (double)A.vo[i][a];
+        van[i] = (double)A.vn[i][a];
+        ua[i] = (double)A.up[i][a];
+    }
+    const double ra = A.rad[a];
+    const int refa = A.ref[a];
+    const double dma[3] = {(double)A.dm[0][a], (double)A.dm[1][a], (double)A.dm[2][a]};
+    int ix, iy, iz;
+    own_cell(D, xa[0], xa[1], xa[2], ix, iy, iz);
+    int ncollip1 = 0;
+    unsigned long long ncand = 0;
+    const int nj = 2 * A.jmax + 1, nk = 2 * A.kmax + 1;
+
+    for (int jj = -A.jmax; jj <= A.jmax; jj++) {
+        const int iy2 = iy + jj;
+        if (iy2 < 1 - D.ny_coll || iy2 > D.ncd + D.ny_coll) continue;
+        for (int kk = -A.kmax; kk <= A.kmax; kk++) {
+            const int iz2 = iz + kk;
+            if (iz2 < 1 - D.nz_coll || iz2 > D.ncd + D.nz_coll) continue;
+            if (iz2 < 1) continue;
+            if (iz2 <= D.ncd && iy2 < 1) continue;
+            const int row = row_of(D, iy2, iz2);
+            const int rs = A.row_start[row], re_ = A.row_start[row + 1];
+            if (rs == re_) continue;
+            // up to three x ranges: [lo, hi] with shift sx
+            int lo_raw = ix - A.imax, hi_raw = ix + A.imax;
+            int rlo[3], rhi[3];
+            double rsx[3];
+            int nr = 0;
+            rlo[nr] = max(1, lo_raw); rhi[nr] = min(D.ncd, hi_raw); rsx[nr] = 0.0; nr++;
+            if (lo_raw < 1) { rlo[nr] = lo_raw + D.ncd; rhi[nr] = D.ncd; rsx[nr] = -1.0; nr++; }
+            if (hi_raw > D.ncd) { rlo[nr] = 1; rhi[nr] = hi_raw - D.ncd; rsx[nr] = 1.0; nr++; }
+            for (int q = 0; q < nr; q++) {
+                const double sx = rsx[q];
+                for (int s = lower_ix(A.row_ent, rs, re_, rlo[q]); s < re_; s++) {
+                    const long long ke = A.row_ent[s];
+                    const int ix2 = (int)(ke >> 32);
+                    if (ix2 > rhi[q]) break;
+                    const int e = (int)(ke & 0xffffffffLL);
+                    double xb0[3];
+                    int src, jid;
+                    load_entry(A, e, xb0, src, jid);
+                    if (jid == 0 && A.ref[src] <= refa) continue;   // ih2 <= ih1
+                    const int ii = (sx == 0.0) ? ix2 - ix : (sx < 0.0 ? ix2 - D.ncd - ix : ix2 + D.ncd - ix);
+                    ncand++;
+                    double xb[3], xbn[3], vb[3], xd[3];
+                    xb[0] = xb0[0] + sx * D.hx;
+                    xb[1] = xb0[1];
+                    xb[2] = xb0[2];
+                    const double dmb[3] = {(double)A.dm[0][src], (double)A.dm[1][src], (double)A.dm[2][src]};
+                    for (int i = 0; i < 3; i++) {
+                        xbn[i] = xb[i] + dmb[i];
+                        vb[i] = (double)A.vo[i][src];
+                        xd[i] = xa[i] - xb[i];
+                    }
+                    const double dnij0 = sqrt(xd[0] * xd[0] + xd[1] * xd[1] + xd[2] * xd[2]);
+                    const double rb = A.rad[src];
+                    const double rcoll = ra + rb;
+                    const double rcolla = D.hdi ? rcoll : rcoll * (1.0 - D.st / 100.0);
+                    const double rcollb = rcoll * (1.0 + D.st / 100.0);
+                    int index1 = 1, index2 = 1;
+                    double wr = 0.0;
+                    const int loopkey = ((ii + A.imax) * nj + (jj + A.jmax)) * nk + (kk + A.kmax);
+                    if (dnij0 > rcolla && dnij0 <= 10 * rcoll) {
+                        if (dnij0 > rcoll) {
+                            for (int i = 0; i < 3; i++) xd[i] = xd[i] / dnij0;
+                            double vr1 = dot3(va, xd), vr2 = dot3(vb, xd);
+                            wr = vr1 - vr2;
+                            int ir = (int)((dnij0 - rcoll) / ((9.0 / (double)DL_NBIN) * rcoll));
+                            if (ir > DL_NBIN - 1) ir = DL_NBIN - 1;
+                            if (ir < 0) ir = 0;
+                            findindex(D, ra, rb, index1, index2);
+                            const int hb = (index1 - 1) + nset * ((index2 - 1) + nset * ir);
+                            atomicAdd(&A.hist_i[hb], 1);
+                            double dwx = 0.0, dwy = 0.0, dwz = 0.0;
+                            if (index2 == index1) { dwx = va[0] - vb[0]; dwy = va[1] - vb[1]; dwz = va[2] - vb[2]; }
+                            if (ra > rb) {
+                                dwx = dwx + (va[0] - vb[0]); dwy = dwy + (va[1] - vb[1]); dwz = dwz + (va[2] - vb[2]);
+                            } else if (ra < rb) {
+                                dwx = dwx + (vb[0] - va[0]); dwy = dwy + (vb[1] - va[1]); dwz = dwz + (vb[2] - va[2]);
+                            }
+                            double *H = A.hist_d;
+                            const int nb = A.nbinsz;
+                            atomicAdd(&H[0 * nb + hb], wr);
+                            atomicAdd(&H[1 * nb + hb], dwx);
+                            atomicAdd(&H[2 * nb + hb], dwy);
+                            atomicAdd(&H[3 * nb + hb], dwz);
+                            double du[3], dv[3];
+                            for (int i = 0; i < 3; i++) {
+                                du[i] = ua[i] - (double)A.up[i][src];
+                                dv[i] = va[i] - vb[i];
+                            }
+                            atomicAdd(&H[4 * nb + hb], dot3(du, xd));
+                            double aaa = dot3(dv, xd);
+                            double bbb = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+                            if (bbb != 0.0) {
+                                double vangle = acos(fabs(aaa / bbb));
+                                atomicAdd(&H[5 * nb + hb], vangle);
+                                double sv = bbb * sin(vangle);
+                                atomicAdd(&H[6 * nb + hb], sv * sv / dnij0);
+                            }
+                        }
+                        if (dnij0 <= rcollb) {
+                            if (dnij0 <= rcoll) {
+                                for (int i = 0; i < 3; i++) xd[i] = xd[i] / dnij0;
+                                double vr1 = dot3(va, xd), vr2 = dot3(vb, xd);
+                                wr = vr1 - vr2;
+                                findindex(D, ra, rb, index1, index2);
+                            }
+                            atomicAdd(&A.counts[8 + nset * nset + (index1 - 1) + nset * (index2 - 1)], 1);
+                            int slot = atomicAdd(&A.counts[4], 1);
+                            if (slot < A.contact_cap) {
+                                ContactRec &cr = A.contacts[slot];
+                                cr.a = a; cr.b = e; cr.loopkey = loopkey; cr.pad = 0;
+                                cr.rec[0] = (double)index1;
+                                cr.rec[1] = (double)index2;
+                                for (int i = 0; i < 3; i++) {
+                                    cr.rec[2 + i] = va[i];
+                                    cr.rec[5 + i] = vb[i];
+                                    cr.rec[8 + i] = xd[i];
+                                }
+                                cr.rec[11] = wr;
+                            } else {
+                                A.counts[6] = 1;
+                            }
+                        }
+                    }
+                    // detection, neighbouring cells only (partlib.f90:1445-1518)
+                    if (abs(ii) > 1 || abs(jj) > 1 || abs(kk) > 1) continue;
+                    const double dmove_a = sqrt(dma[0] * dma[0] + dma[1] * dma[1] + dma[2] * dma[2]);
+                    const double dmove_b = sqrt(dmb[0] * dmb[0] + dmb[1] * dmb[1] + dmb[2] * dmb[2]);
+                    const double tmove = rcoll + dmove_a + dmove_b;
+                    if (dnij0 > tmove) continue;
+                    for (int i = 0; i < 3; i++) xd[i] = xan[i] - xbn[i];
+                    const double dnij1 = sqrt(xd[0] * xd[0] + xd[1] * xd[1] + xd[2] * xd[2]);
+                    if (dnij0 < rcoll && dnij1 > rcoll) continue;
+                    int hit = 0;
+                    if (dnij0 > rcoll && dnij1 <= rcoll) {
+                        hit = 1;
+                    } else {
+                        double vbn[3];
+                        for (int i = 0; i < 3; i++) vbn[i] = (double)A.vn[i][src];
+                        for (int icheck = 1; icheck <= 19; icheck++) {
+                            const double tfac = 0.05 * (double)icheck;
+                            const double tfac1 = D.dt * tfac;
+                            const double tfac2 = tfac * tfac;
+                            const double tfac3 = tfac2 * tfac;
+                            double dd[3];
+                            for (int i = 0; i < 3; i++) {
+                                double xta = xa[i] + va[i] * tfac1 + (3.0 * dma[i] - (2.0 * va[i] + van[i]) * D.dt) * tfac2 +
+                                             ((van[i] + va[i]) * D.dt - 2.0 * dma[i]) * tfac3;
+                                double xtb = xb[i] + vb[i] * tfac1 + (3.0 * dmb[i] - (2.0 * vb[i] + vbn[i]) * D.dt) * tfac2 +
+                                             ((vbn[i] + vb[i]) * D.dt - 2.0 * dmb[i]) * tfac3;
+                                dd[i] = xta - xtb;
+                            }
+                            const double dnij = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+                            if (dnij0 > rcoll && dnij < rcoll) { hit = 2; break; }
+                            if (dnij1 <= rcoll && dnij > rcoll) { hit = 3; break; }
+                        }
+                    }
+                    if (!hit) continue;
+                    ncollip1++;
+                    atomicAdd(&A.counts[hit - 1], 1);
+                    findindex(D, ra, rb, index1, index2);
+                    atomicAdd(&A.counts[8 + (index1 - 1) + nset * (index2 - 1)], 1);
+                    int ps = atomicAdd(&A.counts[3], 1);
+                    if (ps < A.pair_cap) {
+                        A.pairs[ps].a = a; A.pairs[ps].b = e; A.pairs[ps].type = hit; A.pairs[ps].loopkey = loopkey;
+                    } else {
+                        A.counts[6] = 1;
+                    }
+                    // removal lists (partlib.f90:1527-1553): owned partner, or a ghost of slots 5..8
+                    if (jid == 0 || jid >= 5) {
+                        int rs2 = atomicAdd(&A.counts[5], 1);
+                        if (rs2 < A.remove_cap) A.remove[rs2] = A.ref[src] + 1;
+                        else A.counts[6] = 1;
+                    }
+                }
+            }
+        }
+    }
+    if (ncollip1 != 0) {
+        int rs2 = atomicAdd(&A.counts[5], 1);
+        if (rs2 < A.remove_cap) A.remove[rs2] = refa + 1;
+        else A.counts[6] = 1;
+    }
+    if (ncand) atomicAdd(A.cand, ncand);
+}
+
+__global__ void k_accumulate(int nbinsz, const int *hi, const double *hd, int *acc_i, double *acc_d)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nbinsz) acc_i[i] += hi[i];
+    if (i < 7 * nbinsz) acc_d[i] += hd[i];
+}
+
+// OVERLAP_DET sweep (partlib.f90:2069-2156): per owned droplet, number of partners
+// (ypn index > ih1, 27 neighbour cells, half shell) within rcoll.
+__global__ void k_overlap(DevConst D, int nps, const double *px, const double *py, const double *pz, const Ghost *g,
+                          const int *row_start, const long long *row_ent, const int *ref, const double *rad,
+                          int jmax, int kmax, int2 *hits, int cap, int *cnt)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nps) return;
+    const double xa[3] = {px[a], py[a], pz[a]};
+    const int refa = ref[a];
+    int ix, iy, iz;
+    own_cell(D, xa[0], xa[1], xa[2], ix, iy, iz);
+    int nov = 0;
+    for (int jj = -1; jj <= 1; jj++) {
+        int iy2 = iy + jj;
+        if (iy2 < 1 - jmax || iy2 > D.ncd + jmax) continue;
+        for (int kk = -1; kk <= 1; kk++) {
+            int iz2 = iz + kk;
+            if (iz2 < 1 - kmax || iz2 > D.ncd + kmax) continue;
+            if (iz2 < 1) continue;
+            if (iz2 <= D.ncd && iy2 < 1) continue;
+            const int row = row_of(D, iy2, iz2);
+            const int rs = row_start[row], re_ = row_start[row + 1];
+            for (int ii = -1; ii <= 1; ii++) {
+                int ix2 = ix + ii;
+                double sx = 0.0;
+                if (ix2 < 1) { ix2 = D.ncd + ix2; sx = -1.0; }
+                else if (ix2 > D.ncd) { ix2 = ix2 % D.ncd; sx = 1.0; }
+                for (int s = lower_ix(row_ent, rs, re_, ix2); s < re_; s++) {
+                    long long ke = row_ent[s];
+                    if ((int)(ke >> 32) != ix2) break;
+                    int e = (int)(ke & 0xffffffffLL);
+                    double xb[3];
+                    int src;
+                    if (e < nps) {
+                        src = e;
+                        if (ref[src] <= refa) continue;
+                        xb[1] = py[e]; xb[2] = pz[e];
+                    } else {
+                        src = g[e - nps].src;
+                        xb[1] = g[e - nps].y; xb[2] = g[e - nps].z;
+                    }
+                    xb[0] = px[src] + sx * D.hx;
+                    double xd[3] = {xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2]};
+                    double dnij = sqrt(xd[0] * xd[0] + xd[1] * xd[1] + xd[2] * xd[2]);
+                    double rcoll = rad[a] + rad[src];
+                    if (dnij <= rcoll) nov++;
+                }
+            }
+        }
+    }
+    if (nov) {
+        int s = atomicAdd(cnt, 1);
+        if (s < cap) hits[s] = make_int2(refa, nov);
+    }
+}
+
+// PERIODIC for the separate-call path: neighbour code of every droplet, then wrap.
+__device__ __forceinline__ int leave_nid_of(double y, double z, double pi2)
+{
+    const double ylo = 0.0, yhi = pi2, zlo = 0.0, zhi = pi2;
+    if (y > yhi && z <= zhi && z >= zlo) return 1;
+    if (y > yhi && z > zhi) return 2;
+    if (y >= ylo && y <= yhi && z > zhi) return 3;
+    if (y < ylo && z > zhi) return 4;
+    if (y < ylo && z <= zhi && z >= zlo) return 5;
+    if (y < ylo && z < zlo) return 6;
+    if (z < zlo && y <= yhi && y >= ylo) return 7;
+    if (z < zlo && y > yhi) return 8;
+    return 0;
+}
+
+__global__ void k_periodic_flags(int nps, double pi2, double *px, double *py, double *pz, const int *ref,
+                                 signed char *leave_nid)
+{
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= nps) return;
+    double x = px[d], y = py[d], z = pz[d];
+    int nid = leave_nid_of(y, z, pi2);
+    if (nid) leave_nid[ref[d]] = (signed char)nid;
+    if (x >= pi2) x = x - pi2;
+    if (x < 0.0) x = x + pi2;
+    if (y >= pi2) y = y - pi2;
+    if (y < 0.0) y = y + pi2;
+    if (z >= pi2) z = z - pi2;
+    if (z < 0.0) z = z + pi2;
+    px[d] = x; py[d] = y; pz[d] = z;
+}
+
+// ---- PERIODIC reorder (partlib.f90:866-1133) on the device --------------------------
+// 1. count flagged reference indices per block of 1024, 2. scan, 3. compact them in
+// ascending order, 4. one CTA replays the swap-with-last loop over the departing droplets
+// only (thread 0), appends them in neighbour order, and rewrites ref_of_dev/dev_of_ref.
+__global__ void __launch_bounds__(1024) k_lv_count(int n, const signed char *nid, int *blk)
+{
+    int i = blockIdx.x * 1024 + threadIdx.x;
+    int f = (i < n && nid[i] != 0) ? 1 : 0;
+    int c = __syncthreads_count(f);
+    if (threadIdx.x == 0) blk[blockIdx.x] = c;
+}
+
+__global__ void __launch_bounds__(1024) k_lv_compact(int n, const signed char *nid, const int *off, int *refs)
+{
+    __shared__ int wsum[32];
+    const int i = blockIdx.x * 1024 + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const bool f = i < n && nid[i] != 0;
+    unsigned m = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) wsum[w] = __popc(m);
+    __syncthreads();
+    if (w == 0) {
+        int v = wsum[lane], incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        wsum[lane] = incl - v;
+    }
+    __syncthreads();
+    if (f) refs[off[blockIdx.x] + wsum[w] + __popc(m & ((1u << lane) - 1))] = i;
+}
+
+__global__ void __launch_bounds__(1024) k_lv_reorder(int n, const int *ktot, const int *P, signed char *nid,
+                                                     int *dep, int *old_ref, int *new_ref, int *dev_tmp,
+                                                     int *ref_of_dev, int *dev_of_ref, int *err)
+{
+    __shared__ int s_m, s_k;
+    if (threadIdx.x == 0) {
+        const int k = *ktot;
+        int lo = 0, hi = k - 1, sum = 0, nf = 0, nd = 0;
+        while (lo <= hi) {                 // each pass consumes at least one departing droplet
+            const int h = P[lo] + 1;       // 1-based position of the next hole the scan reaches
+            if (h + sum > n) break;
+            lo++;
+            int e = h;
+            for (int guard = 0; guard <= k; guard++) {
+                dep[nd++] = e - 1;
+                sum++;
+                const int t = n - sum + 1; // tail position pulled into the hole
+                if (t == h) break;
+                if (hi >= lo && P[hi] + 1 == t) { hi--; e = t; continue; }
+                old_ref[nf] = t - 1;
+                new_ref[nf] = h - 1;
+                nf++;
+                break;
+            }
+        }
+        if (nd != k) {
+            atomicOr(err, DL_DERR_REORDER);
+            s_m = 0;
+        } else {
+            int slot = n - k, m = nf;
+            for (int q = 1; q <= 8; q++)
+                for (int j = 0; j < nd; j++)
+                    if (nid[dep[j]] == q) { old_ref[m] = dep[j]; new_ref[m] = slot++; m++; }
+            s_m = m;
+        }
+        s_k = k;
+    }
+    __syncthreads();
+    const int m = s_m, k = s_k;
+    for (int j = threadIdx.x; j < m; j += blockDim.x) dev_tmp[j] = dev_of_ref[old_ref[j]];
+    __syncthreads();
+    for (int j = threadIdx.x; j < m; j += blockDim.x) {
+        ref_of_dev[dev_tmp[j]] = new_ref[j];
+        dev_of_ref[new_ref[j]] = dev_tmp[j];
+    }
+    for (int j = threadIdx.x; j < k; j += blockDim.x) nid[P[j]] = 0;
+}
+
+// new reference indices for a set of droplets (old ref -> new ref, both 0-based)
+__global__ void k_remap_read(int m, const int *old_ref, const int *dev_of_ref, int *dev_out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) dev_out[i] = dev_of_ref[old_ref[i]];
+}
+__global__ void k_remap_write(int m, const int *dev, const int *new_ref, int *ref_of_dev, int *dev_of_ref)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) { ref_of_dev[dev[i]] = new_ref[i]; dev_of_ref[new_ref[i]] = dev[i]; }
+}
+
+__global__ void k_set_positions(int m, const int *refs, const int *dev, const double *xyz, double *px, double *py,
+                                double *pz, signed char *leave_nid)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    int d = dev[i];
+    px[d] = xyz[3 * i]; py[d] = xyz[3 * i + 1]; pz[d] = xyz[3 * i + 2];
+    if (leave_nid) leave_nid[refs[i]] = 0;   // moved back inside: not departing any more
+}
+
+}  // namespace
+
+// =======================================================================================
+// HEADLIST
+// =======================================================================================
+int launch_headlist(dl_ctx *c, double dist)
+{
+    const DevConst &D = c->dc;
+    const int nps = c->nps, t = 256;
+    const double *P[3] = {c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2]};
+    DL_CUDA(c, cudaMemsetAsync(c->d_nghost, 0, sizeof(int), c->stream));
+    if (nps > 0) {
+        k_ghosts<<<dl_blocks(nps, t), t, 0, c->stream>>>(D, nps, P[1], P[2], dist, c->ghosts, c->gcap, c->d_nghost);
+        DL_CHECK_LAUNCH(c);
+    }
+    int ng = 0;
+    DL_CUDA(c, cudaMemcpyAsync(&ng, c->d_nghost, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (ng > c->gcap) return dl_fail(c, DL_E_CAPACITY, "HEADLIST: halo droplet capacity exceeded");
+    c->nghost = ng;
+    const int ne = nps + ng;
+    DL_CUDA(c, cudaMemsetAsync(c->row_fill, 0, sizeof(int) * (c->nrows + 1), c->stream));
+    if (ne > 0) {
+        k_entry_cells<<<dl_blocks(ne, t), t, 0, c->stream>>>(D, nps, ng, P[0], P[1], P[2], c->ghosts, c->ent_row,
+                                                             c->ent_ix, c->row_fill);
+        DL_CHECK_LAUNCH(c);
+    }
+    int r = dl_scan(c, c->row_fill, c->row_start, c->nrows);   // exclusive scan of row counts
+    if (r) return r;
+    DL_CUDA(c, cudaMemsetAsync(c->row_fill, 0, sizeof(int) * (c->nrows + 1), c->stream));
+    if (ne > 0) {
+        k_row_scatter<<<dl_blocks(ne, t), t, 0, c->stream>>>(ne, c->ent_row, c->ent_ix, c->row_start, c->row_fill,
+                                                             (long long *)c->row_ent);
+        DL_CHECK_LAUNCH(c);
+        DL_CUDA(c, cudaMemsetAsync(c->n_long, 0, sizeof(int), c->stream));
+        k_row_sort<<<dl_blocks(c->nrows, t), t, 0, c->stream>>>(c->nrows, c->row_start, (long long *)c->row_ent,
+                                                                c->long_rows, c->n_long);
+        DL_CHECK_LAUNCH(c);
+        int nl = 0;
+        DL_CUDA(c, cudaMemcpyAsync(&nl, c->n_long, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaStreamSynchronize(c->stream));
+        if (nl > 0) {
+            // crowded rows: every one must fit a CTA's shared-memory sort
+            DL_CUDA(c, cudaMemsetAsync(c->d_nghost, 0, sizeof(int), c->stream));
+            k_max_row<<<dl_blocks(c->nrows, t), t, 0, c->stream>>>(c->nrows, c->row_start, c->d_nghost);
+            DL_CHECK_LAUNCH(c);
+            int mx = 0;
+            DL_CUDA(c, cudaMemcpyAsync(&mx, c->d_nghost, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            DL_CUDA(c, cudaStreamSynchronize(c->stream));
+            if (mx > kLongRowMax)
+                return dl_fail(c, DL_E_CAPACITY, "HEADLIST: more than 4096 droplets in one row of cells");
+            k_row_sort_long<<<nl, 1024, 0, c->stream>>>(c->long_rows, c->n_long, c->row_start,
+                                                        (long long *)c->row_ent);
+            DL_CHECK_LAUNCH(c);
+        }
+    }
+    c->hl_dist = dist;
+    c->hl_valid = 1;
+    return 0;
+}
+
+// =======================================================================================
+// COLLISION_DET
+// =======================================================================================
+template <typename T>
+static int collision_t(dl_ctx *c, dl_coll_report *rep)
+{
+    const DevConst &D = c->dc;
+    const int nset = D.nset, nbz = c->nbinsz, t = 128;
+    CollArgs<T> A;
+    memset(&A, 0, sizeof(A));
+    A.D = D;
+    A.nps = c->nps;
+    A.px = c->pos[c->pcur][0]; A.py = c->pos[c->pcur][1]; A.pz = c->pos[c->pcur][2];
+    A.g = c->ghosts;
+    A.row_start = c->row_start;
+    A.row_ent = (const long long *)c->row_ent;
+    A.ref = c->ref_of_dev;
+    A.rad = c->rad;
+    const int vnew = c->have_vnew ? c->vnew : c->vcur;
+    for (int k = 0; k < 3; k++) {
+        A.dm[k] = tp<T>(c->dmv[k]);
+        A.vo[k] = tp<T>(c->vel[c->vcur][k]);
+        A.vn[k] = tp<T>(c->vel[vnew][k]);
+        A.up[k] = tp<T>(dl_vp_ptr(c, k));   // vp: fluid ring slot (fused step) or vpv
+    }
+    const double d_stat = 20.0 * D.radmax;
+    A.imax = 1 + (int)(d_stat * (double)D.ncd / D.hx);
+    A.jmax = 1 + (int)(d_stat * (double)D.ncd / D.hy);
+    A.kmax = 1 + (int)(d_stat * (double)D.ncd / D.hz);
+    A.nbinsz = nbz;
+    A.hist_i = c->hist_i;
+    A.hist_d = c->hist_d;
+    A.counts = c->counts;
+    A.cand = c->cand;
+    A.pairs = c->pairs;
+    A.pair_cap = c->pair_cap;
+    A.contacts = c->contacts;
+    A.contact_cap = c->contact_cap;
+    A.remove = c->remove_dev;
+    A.remove_cap = c->remove_cap;
+    const int ncount = 8 + 2 * nset * nset;
+    DL_CUDA(c, cudaMemsetAsync(c->hist_i, 0, sizeof(int) * nbz, c->stream));
+    DL_CUDA(c, cudaMemsetAsync(c->hist_d, 0, sizeof(double) * 7 * nbz, c->stream));
+    DL_CUDA(c, cudaMemsetAsync(c->counts, 0, sizeof(int) * ncount, c->stream));
+    DL_CUDA(c, cudaMemsetAsync(c->cand, 0, sizeof(unsigned long long), c->stream));
+    if (c->nps > 0) {
+        k_collision<T><<<dl_blocks(c->nps, t), t, 0, c->stream>>>(A);
+        DL_CHECK_LAUNCH(c);
+    }
+    k_accumulate<<<dl_blocks(7 * nbz, 256), 256, 0, c->stream>>>(nbz, c->hist_i, c->hist_d, c->acc_i, c->acc_d);
+    DL_CHECK_LAUNCH(c);
+    std::vector<int> cnt(ncount);
+    unsigned long long cand = 0;
+    DL_CUDA(c, cudaMemcpyAsync(cnt.data(), c->counts, sizeof(int) * ncount, cudaMemcpyDeviceToHost, c->stream));
+    DL_CUDA(c, cudaMemcpyAsync(&cand, c->cand, sizeof(cand), cudaMemcpyDeviceToHost, c->stream));
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (cnt[6]) return dl_fail(c, DL_E_CAPACITY, "COLLISION_DET: pair, contact or removal buffer full");
+    const int npairs = cnt[3], ncontact = cnt[4], nremove = cnt[5];
+    if (npairs > c->p.ncollmax)
+        return dl_fail(c, DL_E_CAPACITY, "COLLISION_DET: more collided pairs than ncollmax (collist capacity)");
+    // removal list: sort (hpsort, partlib.f90:1631)
+    c->removepart.resize(nremove);
+    if (nremove)
+        DL_CUDA(c, cudaMemcpy(c->removepart.data(), c->remove_dev, sizeof(int) * nremove, cudaMemcpyDeviceToHost));
+    std::sort(c->removepart.begin(), c->removepart.end());
+    // pairs in the reference's detection order -> collist and the pair rows
+    std::vector<PairRec> pr(npairs);
+    if (npairs) DL_CUDA(c, cudaMemcpy(pr.data(), c->pairs, sizeof(PairRec) * npairs, cudaMemcpyDeviceToHost));
+    c->last_npairs = npairs;
+    c->last_ncontact = ncontact;
+    c->last_ntotpair = npairs;
+    int r = dl_pairs_to_host(c, pr);
+    if (r) return r;
+    // histograms: 5-step boundary (partlib.f90:1659-1718)
+    c->last_written = 0;
+    if ((c->istep + 1) % 5 == 0) {
+        r = dl_hist_boundary(c);
+        if (r) return r;
+        c->last_written = 1;
+    }
+    if (rep) {
+        rep->icc[0] = cnt[0]; rep->icc[1] = cnt[1]; rep->icc[2] = cnt[2];
+        rep->ncoll = nremove;
+        rep->ntotpair = npairs;
+        rep->ncontact = ncontact;
+        rep->written = c->last_written;
+        rep->candidate_pairs = (int64_t)cand;
+    }
+    c->last_ncoll = nremove;
+    return 0;
+}
+
+int launch_collision(dl_ctx *c, dl_coll_report *rep)
+{
+    return c->mixed ? collision_t<float>(c, rep) : collision_t<double>(c, rep);
+}
+
+// =======================================================================================
+// OVERLAP_DET sweep
+// =======================================================================================
+int launch_overlap_sweep(dl_ctx *c, std::vector<int2> &hits)
+{
+    const DevConst &D = c->dc;
+    const double d_overl = 2.0 * D.radmax;
+    int r = launch_headlist(c, d_overl);
+    if (r) return r;
+    const int jmax = 1 + (int)(d_overl * (double)D.ncd / D.hy);
+    const int kmax = 1 + (int)(d_overl * (double)D.ncd / D.hz);
+    DL_CUDA(c, cudaMemsetAsync(c->ovl_cnt, 0, sizeof(int), c->stream));
+    if (c->nps > 0) {
+        k_overlap<<<dl_blocks(c->nps, 128), 128, 0, c->stream>>>(
+            D, c->nps, c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2], c->ghosts, c->row_start,
+            (const long long *)c->row_ent, c->ref_of_dev, c->rad, jmax, kmax, c->ovl_list, c->ovl_cap, c->ovl_cnt);
+        DL_CHECK_LAUNCH(c);
+    }
+    int n = 0;
+    DL_CUDA(c, cudaMemcpyAsync(&n, c->ovl_cnt, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (n > c->ovl_cap) return dl_fail(c, DL_E_CAPACITY, "OVERLAP_DET: overlap list capacity exceeded");
+    hits.resize(n);
+    if (n) DL_CUDA(c, cudaMemcpy(hits.data(), c->ovl_list, sizeof(int2) * n, cudaMemcpyDeviceToHost));
+    // the sweep's cell list was built for d_overl; the collision cell list is stale now
+    c->hl_valid = 0;
+    return 0;
+}
+
+// =======================================================================================
+// PERIODIC (flags + wrap for the separate-call path; the fused kernel did both itself)
+// =======================================================================================
+int launch_periodic(dl_ctx *c)
+{
+    if (c->nps > 0) {
+        k_periodic_flags<<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(
+            c->nps, c->dc.pi2, c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2], c->ref_of_dev,
+            c->leave_nid);
+        DL_CHECK_LAUNCH(c);
+    }
+    return launch_periodic_reorder(c);
+}
+
+// Reorders the reference indices of the droplets flagged in leave_nid (no host round trip).
+int launch_periodic_reorder(dl_ctx *c)
+{
+    const int n = c->nps;
+    if (n == 0) return 0;
+    const int nblk = dl_blocks(n, 1024);
+    k_lv_count<<<nblk, 1024, 0, c->stream>>>(n, c->leave_nid, c->lv_blk);
+    DL_CHECK_LAUNCH(c);
+    int r = dl_scan(c, c->lv_blk, c->lv_blk, nblk);   // in place: the scan reads before it writes per chunk
+    if (r) return r;
+    k_lv_compact<<<nblk, 1024, 0, c->stream>>>(n, c->leave_nid, c->lv_blk, c->lv_refs);
+    DL_CHECK_LAUNCH(c);
+    k_lv_reorder<<<1, 1024, 0, c->stream>>>(n, c->lv_blk + nblk, c->lv_refs, c->leave_nid, c->lv_dep, c->lv_old,
+                                            c->lv_new, c->lv_dev, c->ref_of_dev, c->dev_of_ref, c->d_err);
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}
+
+// Applies a reference-index permutation to a subset: old_ref[i] -> new_ref[i] (0-based).
+int dl_apply_remap(dl_ctx *c, const std::vector<int> &old_ref, const std::vector<int> &new_ref)
+{
+    const int m = (int)old_ref.size();
+    if (m == 0) return 0;
+    DL_CUDA(c, cudaMemcpyAsync(c->lv_old, old_ref.data(), sizeof(int) * m, cudaMemcpyHostToDevice, c->stream));
+    DL_CUDA(c, cudaMemcpyAsync(c->lv_new, new_ref.data(), sizeof(int) * m, cudaMemcpyHostToDevice, c->stream));
+    k_remap_read<<<dl_blocks(m, 256), 256, 0, c->stream>>>(m, c->lv_old, c->dev_of_ref, c->lv_dev);
+    k_remap_write<<<dl_blocks(m, 256), 256, 0, c->stream>>>(m, c->lv_dev, c->lv_new, c->ref_of_dev, c->dev_of_ref);
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}
+
+// Writes positions of droplets given by reference index (0-based) into the current buffer.
+int launch_set_positions(dl_ctx *c, const std::vector<int> &refs, const std::vector<double> &xyz, int clear_leave)
+{
+    const int m = (int)refs.size();
+    if (m == 0) return 0;
+    if (m > c->msize) return dl_fail(c, DL_E_CAPACITY, "position update list longer than msize");
+    DL_CUDA(c, cudaMemcpyAsync(c->lv_old, refs.data(), sizeof(int) * m, cudaMemcpyHostToDevice, c->stream));
+    DL_CUDA(c, cudaMemcpyAsync(c->xfer64, xyz.data(), sizeof(double) * 3 * m, cudaMemcpyHostToDevice, c->stream));
+    k_remap_read<<<dl_blocks(m, 256), 256, 0, c->stream>>>(m, c->lv_old, c->dev_of_ref, c->lv_dev);
+    k_set_positions<<<dl_blocks(m, 256), 256, 0, c->stream>>>(m, c->lv_old, c->lv_dev, c->xfer64,
+                                                              c->pos[c->pcur][0], c->pos[c->pcur][1],
+                                                              c->pos[c->pcur][2], clear_leave ? c->leave_nid : nullptr);
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}

@@ -1,0 +1,247 @@
+// Internal declarations of the droplet engine (device state, kernels, helpers).
+// Reference: thenumer8or/MPI_2D_domain_decomp_turb_particles partlib.f90 (single rank).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/droplet.h"
+
+#define DL_NBIN 180
+#define DL_PAD_LO 3   // FP32 halo field: planes below the grid in every direction
+#define DL_PAD_HI 4   // planes above
+
+// ---------------------------------------------------------------------------------------
+// Device-side view of the physical constants (single rank, partlib.f90:104-157).
+// ---------------------------------------------------------------------------------------
+struct DevConst {
+    int n;            // nx = ny = nz
+    int ncd;          // ncdx = ncdy = ncdz
+    int nset;
+    int ndrag, hdi;
+    int nx_coll, ny_coll, nz_coll;   // collision search half-widths in cells
+    int nx_max, ny_max, nz_max;      // halo depth of the cell grid (partlib.f90:137-151)
+    int nyh, nzh;                    // rows of the cell grid including halo cells
+    double dt, rnu, pi2, hx, hy, hz, dx;   // dx = pi2 / n (partlib.f90:315-317)
+    double tau2, sv;                 // tau_CLOUD_const2, Sv_const
+    double st, radmax;
+    double radius[10];
+    double hdi_trunc;
+};
+
+// ---------------------------------------------------------------------------------------
+// Ghost record of HEADLIST (one periodic image of a droplet near a y/z face).
+// ---------------------------------------------------------------------------------------
+struct Ghost {
+    double y, z;   // shifted coordinates (partlib.f90:2231-2348)
+    int src;       // device index of the source droplet
+    int jid;       // slot 1..8 it is received in (partlib.f90:2358-2394)
+};
+
+// One detected collision with the keys that restore the reference's detection order.
+struct PairRec {
+    int a;         // device index of droplet 1 (owned)
+    int b;         // cell-list entry of droplet 2 (owned device index, or nps + ghost index)
+    int type;      // 1, 2, 3
+    int loopkey;   // ((ii+imax)*(2jmax+1) + jj+jmax)*(2kmax+1) + kk+kmax
+};
+
+struct ContactRec {
+    int a, b, loopkey, pad;
+    double rec[12];
+};
+
+// HDI neighbour (CSR entry): partner entry and the 6 tensor coefficients.
+template <typename T>
+struct NeiCoef {
+    T c[6];
+};
+
+struct dl_ctx {
+    dl_params p;
+    DevConst dc;
+    std::string err;
+    int mixed;
+    int device;
+    cudaStream_t stream;
+
+    // ---- host copies of the PART_INIT scalars ----
+    dl_scalars sc;
+    int nps, msize;
+    int istep;
+    double time;
+    int new_particle;
+    int initialized;
+
+    // relocation RNG (ranff2 state, partlib.f90:89-92), host side
+    int iseedr, iyr, ivr[32], idum2;
+
+    // ---- device droplet state, device order ----
+    size_t esz;                  // sizeof(T): 8 (FP64) or 4 (mixed)
+    double *pos[2][3];           // positions, two buffers (pcur = yp(1:3))
+    int pcur;
+    void *vel[4][3];             // droplet velocity ring: V[vcur] = yp(4:6), V[vcur+1] = fvp(:,1), ...
+    int vcur, vnew;
+    void *flu[4][3];             // fluid-velocity ring: F[fcur] = fdp(:,1), ... F[fnew] = fdp(:,0)
+    int fcur, fnew;
+    void *vpv[3];                // vp (interpolated fluid velocity) when vp_slot < 0
+    int vp_slot;                 // >= 0: vp lives in the fluid-velocity ring slot flu[vp_slot]
+    int has_dead;                // COALESCE removed droplets: the next re-sort compacts
+    void *dmv[3];                // dmove
+    void *pert[3];               // HDI disturbance velocity
+    double *rad, *gid;           // yp(7), yp(8)
+    int *ref_of_dev, *dev_of_ref;
+    int have_vnew, have_fnew, have_dmove;   // sequence flags within a step
+
+    // ---- re-sort (device order by brick) ----
+    int bx, by, bz;              // brick size in cells for the interpolation kernel
+    int nbx, nby, nbz, nbricks;
+    int *brick_start;            // nbricks + 1
+    int *brick_cnt;              // nbricks
+    int *keys, *perm;            // per droplet
+    void *scratch8;              // permutation scratch for 8-byte arrays (msize * 8 bytes)
+    void *scratch4;              // permutation scratch for 4-byte arrays (msize * 4 bytes)
+    int steps_since_sort;
+    int resort_interval;
+    int sorted;
+
+    // ---- velocity field ----
+    const double *f64[3];
+    int64_t fpy[3], fpz[3];
+    double *f64_own[3];
+    float *f32;                  // [3][nz+7][ny+7][pitch]
+    float *f32_own;
+    int64_t f32_pitch, f32_ny, f32_plane, f32_comp;
+    int field_set[3];
+    int f32_valid;
+
+    // ---- PREPARE_INTERP outputs ----
+    int *lhnode;                 // (nps, 3) in reference order on download
+    double *bg;
+
+    // ---- cell list (HEADLIST) ----
+    double hl_dist;
+    int hl_valid;
+    Ghost *ghosts;
+    int gcap, nghost;
+    int *d_nghost;
+    int *ent_row;                // row of each entry (owned + ghosts)
+    int *ent_ix;                 // ix of each entry
+    int *row_start;              // nrows + 1
+    int *row_fill;
+    int64_t *row_ent;            // sorted (ix << 32 | entry) per row
+    int nrows;
+    int *long_rows;              // rows longer than the per-thread sort limit
+    int *n_long;
+    // PERIODIC: departing droplets flagged by reference index, then reordered on the device
+    signed char *leave_nid;      // [msize] neighbour code 1..8 of a droplet leaving the pencil, else 0
+    int *lv_blk;                 // [nblk + 1] per-1024-block counts -> offsets
+    int *lv_refs;                // [msize] leaving reference indices, ascending
+    int *lv_old, *lv_new, *lv_dev, *lv_dep;   // [msize] remap scratch
+    int *d_err;                  // device error flags (see DL_DERR_*)
+    double *xfer64;              // [3 * msize] host<->device transfer scratch
+    int *xfer_i;                 // [4 * msize] host<->device transfer scratch
+
+    // ---- COLLISION_DET outputs ----
+    int nbinsz;
+    int *hist_i;                 // nirbin: per call [nbinsz], accumulated, written
+    double *hist_d;              // 7 sums: per call [7*nbinsz], accumulated, written
+    int *acc_i, *out_i;
+    double *acc_d, *out_d;
+    int *counts;                 // icc[3], colltype[nset^2], nir[nset^2], npairs, ncontact, overflow, ...
+    unsigned long long *cand;
+    PairRec *pairs;
+    int pair_cap;
+    ContactRec *contacts;
+    int contact_cap;
+    int *remove_dev;             // removal entries (ref indices 1-based), unsorted
+    double *pair_buf;            // [2 * pair_cap * 8] yp rows of collided droplets
+    int *pair_ibuf;              // [2 * pair_cap * 3] device indices in, (ref, ypn index) out
+    int remove_cap;
+    int last_ncoll, last_npairs, last_ncontact, last_written, last_ntotpair;
+    std::vector<int> removepart; // sorted removal list (host)
+    std::vector<double> collist; // collist(20, ntotpair) (host)
+    std::vector<int> pairs_host; // rows (ih1, src2, jid2, type)
+
+    // ---- MEAN_VEL ----
+    double *mv_acc;
+
+    // ---- HDI ----
+    int *nei_cnt, *nei_start;    // CSR over owned droplets
+    int *nei_idx;                // partner entry
+    void *nei_coef;              // NeiCoef<T>
+    double *nei_coef64;          // FP64 coefficients for the residual (mixed)
+    int nei_cap, nnz;
+    int *overlap_flag;
+    // GMRES work
+    void *kry;                   // Krylov basis (maxiter+1) x 3*msize, T
+    double *xg, *rg, *bg64, *tmp64;   // FP64 vectors (3*msize)
+    void *wv, *xt;               // T vectors
+    double *dots;                // device scratch for dot products
+    int gmres_iters, gmres_refine;
+    double gmres_res, gmres_norm_rhs;
+
+    // ---- overlap detection ----
+    int2 *ovl_list;
+    int *ovl_cnt;
+    int ovl_cap;
+
+    // ---- timing ----
+    cudaEvent_t ev[8];
+    double phase_ms[6];
+};
+
+// ---------------------------------------------------------------------------------------
+// Error helpers
+// ---------------------------------------------------------------------------------------
+int dl_fail(dl_ctx *c, int code, const std::string &msg);
+#define DL_CUDA(ctx, call)                                                                  \
+    do {                                                                                    \
+        cudaError_t e__ = (call);                                                           \
+        if (e__ != cudaSuccess)                                                             \
+            return dl_fail((ctx), DL_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)); \
+    } while (0)
+#define DL_CHECK_LAUNCH(ctx) DL_CUDA(ctx, cudaGetLastError())
+
+// ---------------------------------------------------------------------------------------
+// Kernel launchers implemented in the .cu files
+// ---------------------------------------------------------------------------------------
+// dl_interp.cu
+int launch_brick_sort(dl_ctx *c);
+int launch_interp(dl_ctx *c, int icpt_or_all, int fused);
+int launch_prepare_interp(dl_ctx *c);
+int launch_history_fvp(dl_ctx *c);
+int launch_history_fdp(dl_ctx *c);
+int launch_advance(dl_ctx *c);
+int launch_update_position(dl_ctx *c, int track_leave);
+int launch_convert_field(dl_ctx *c, int icpt);
+int launch_mean_vel(dl_ctx *c, double *host_out);
+// dl_cells.cu
+int launch_headlist(dl_ctx *c, double dist);
+int launch_collision(dl_ctx *c, dl_coll_report *rep);
+int launch_overlap_sweep(dl_ctx *c, std::vector<int2> &hits);
+int launch_periodic(dl_ctx *c);
+int launch_set_positions(dl_ctx *c, const std::vector<int> &refs, const std::vector<double> &xyz, int clear_leave);
+int launch_periodic_reorder(dl_ctx *c);
+int dl_check_device_errors(dl_ctx *c);
+#define DL_DERR_REORDER 1        // PERIODIC bookkeeping mismatch
+// dl_hdi.cu
+int launch_nei_list(dl_ctx *c);
+int run_gmres(dl_ctx *c, dl_gmres_report *rep);
+
+// dl_abi.cu helpers
+int dl_scan(dl_ctx *c, const int *cnt, int *start, int m);
+void *dl_vp_ptr(dl_ctx *c, int k);
+int dl_pairs_to_host(dl_ctx *c, std::vector<PairRec> &pr);
+int dl_hist_boundary(dl_ctx *c);
+int dl_apply_remap(dl_ctx *c, const std::vector<int> &old_ref, const std::vector<int> &new_ref);
+void dl_brick_dims(int mixed, int *bx, int *by, int *bz);
+
+// Host RNGs (accesories.f90)
+double dl_ranpp(int *idum, int *iy, int *iv);
+double dl_ranff2(int *idum, int *iv, int *iy, int *idum2);
+
+// shared small utilities
+static inline int dl_blocks(long n, int t) { return (int)((n + t - 1) / t); }

@@ -1,0 +1,998 @@
+// Interpolation, history, advance, position update and the spatial re-sort of the
+// device order.
+//
+// Reference: partlib.f90 PREPARE_INTERP (305-347), INTERPOLATE (351-520),
+// PART_HISTORY_FVP (553-595), PART_HISTORY_FDP (599-625), PART_ADVANCE (629-726),
+// UPDATE_PART_POSITION (730-757), the wrap of PERIODIC (1142-1151) and MEAN_VEL (1889-1980).
+//
+// Design (B200): droplets are kept sorted by "brick" (a BX x BY x BZ block of grid cells).
+// One CTA handles one brick: it stages the brick's field region plus the 6-point stencil
+// halo (2 cells below, 3 above) in shared memory with coalesced loads, then evaluates the
+// 216-point stencil of every (droplet, component) task out of shared memory.  Tasks are
+// grouped so that the 32 (FP32) or 16 (FP64 half-warp) lanes of a group start their
+// stencils in distinct shared-memory banks, which makes every stencil load
+// conflict-free.  The FP64 path sums in the reference's order (x outer, y, z inner,
+// vp = vp + v*bx*by*bz, no FMA contraction) and is bit-identical to the CPU restatement;
+// the mixed path evaluates the same tensor-product sum separably in FP32 with FMA.
+// A droplet that has drifted out of its brick since the last re-sort is evaluated from
+// global memory with the same arithmetic.
+#include "dl_internal.cuh"
+
+#include <algorithm>
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------------------------------
+// 6-point Lagrange weights, partlib.f90:317-338 (FP64, exact source order)
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void lagrange6(double z, double *b)
+{
+    double z2 = z * z, z3 = z2 * z, z4 = z3 * z, z5 = z4 * z;
+    b[0] = (6.0 * z - 5.0 * z2 - 5.0 * z3 + 5.0 * z4 - z5) / 120.0;
+    b[1] = (-12.0 * z + 16.0 * z2 - z3 - 4.0 * z4 + z5) / 24.0;
+    b[2] = (12.0 - 4.0 * z - 15.0 * z2 + 5.0 * z3 + 3.0 * z4 - z5) / 12.0;
+    b[3] = (12.0 * z + 8.0 * z2 - 7.0 * z3 - 2.0 * z4 + z5) / 12.0;
+    b[4] = (-6.0 * z - z2 + 7.0 * z3 + z4 - z5) / 24.0;
+    b[5] = (4.0 * z - 5.0 * z3 + z5) / 120.0;
+}
+
+// FP32 weights (mixed path): the same polynomials in Horner form with FMA.
+__device__ __forceinline__ void lagrange6(float z, float *b)
+{
+    b[0] = z * fmaf(z, fmaf(z, fmaf(z, 5.0f - z, -5.0f), -5.0f), 6.0f) * (1.0f / 120.0f);
+    b[1] = z * fmaf(z, fmaf(z, fmaf(z, z - 4.0f, -1.0f), 16.0f), -12.0f) * (1.0f / 24.0f);
+    b[2] = fmaf(z, fmaf(z, fmaf(z, fmaf(z, 3.0f - z, 5.0f), -15.0f), -4.0f), 12.0f) * (1.0f / 12.0f);
+    b[3] = z * fmaf(z, fmaf(z, fmaf(z, z - 2.0f, -7.0f), 8.0f), 12.0f) * (1.0f / 12.0f);
+    b[4] = z * fmaf(z, fmaf(z, fmaf(z, 1.0f - z, 7.0f), -1.0f), -6.0f) * (1.0f / 24.0f);
+    b[5] = z * fmaf(z * z, fmaf(z, z, -5.0f), 4.0f) * (1.0f / 120.0f);
+}
+
+// node = FLOOR(y/dx); z = (y - node*dx)/dx  (partlib.f90:321-326), always FP64
+__device__ __forceinline__ int node_frac(double y, double dx, double *z)
+{
+    int node = (int)floor(y / dx);
+    *z = (y - (double)node * dx) / dx;
+    return node;
+}
+
+__device__ __forceinline__ int wrapi(int i, int n)
+{
+    int r = i % n;
+    return r < 0 ? r + n : r;
+}
+
+// Ampere+ asynchronous global->shared copy of one 4- or 8-byte element (cp.async.ca).
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem_dst, const void *gmem_src)
+{
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem_src), "n"(BYTES) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------------------
+// Stencil sums.  L(a, b, c) returns the field at stencil offset (x=a, y=b, z=c).
+// ---------------------------------------------------------------------------------------
+template <class L>
+__device__ __forceinline__ double stencil(const L &ld, const double *bx, const double *by, const double *bz)
+{
+    double acc = 0.0;
+#pragma unroll
+    for (int a = 0; a < 6; a++)
+#pragma unroll
+        for (int b = 0; b < 6; b++)
+#pragma unroll
+            for (int c = 0; c < 6; c++)
+                acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(__dmul_rn(ld(a, b, c), bx[a]), by[b]), bz[c]));
+    return acc;
+}
+
+template <class L>
+__device__ __forceinline__ float stencil(const L &ld, const float *bx, const float *by, const float *bz)
+{
+    float acc = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 6; a++) {
+        float t = 0.0f;
+#pragma unroll
+        for (int b = 0; b < 6; b++) {
+            float s = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 6; c++) s = fmaf(ld(a, b, c), bz[c], s);
+            t = fmaf(s, by[b], t);
+        }
+        acc = fmaf(t, bx[a], acc);
+    }
+    return acc;
+}
+
+template <typename T>
+struct SmemLoader {
+    const T *base;
+    int sy, sz;
+    __device__ __forceinline__ T operator()(int a, int b, int c) const { return base[c * sz + b * sy + a]; }
+};
+
+struct GlobalLoader64 {
+    const double *f;
+    int64_t py, pz;
+    int ix[6], iy[6], iz[6];
+    __device__ __forceinline__ double operator()(int a, int b, int c) const
+    {
+        return f[ix[a] + py * iy[b] + pz * iz[c]];
+    }
+};
+
+struct GlobalLoader32 {
+    const float *f;   // points at padded element (x0, y0, z0) of the stencil corner
+    int64_t py, pz;
+    __device__ __forceinline__ float operator()(int a, int b, int c) const { return f[a + py * b + pz * c]; }
+};
+
+// ---------------------------------------------------------------------------------------
+// Kernel arguments
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct InterpArgs {
+    int n, nps;
+    double dx, pi2;
+    const double *px, *py, *pz;     // current positions
+    const int *brick_start;
+    int nbx, nby;
+    // field
+    const double *f64[3];
+    int64_t f64py[3], f64pz[3];
+    const float *f32;               // padded FP32 field
+    int64_t f32py, f32pz, f32comp;
+    int comp_lo, ncomp;             // components evaluated by this launch
+    // outputs (non-fused): vp
+    T *vp[3];
+    // fused advance
+    int fused, first, init_mode, ndrag;
+    T dt, tau2, sv, rnu;
+    const double *rad;
+    T *v0[3], *v1[3], *v2[3];       // V[vcur], V[vcur+1], V[vcur+2]
+    T *vnew[3];                     // V[vnew]
+    T *f1[3], *f2[3], *f3[3];       // F[fcur], F[fcur+1], F[fcur+2]
+    T *fnew[3];                     // F[fnew] (= vp when HDI is off)
+    T *dmv[3];
+    double *qx, *qy, *qz;           // new positions (other buffer)
+    const int *ref_of_dev;
+    signed char *leave_nid;         // PERIODIC departure flags by reference index
+};
+
+template <typename T>
+struct Elems;
+template <>
+struct Elems<double> {
+    static constexpr int R = 16;      // residue modulus: 16 eight-byte words per half-warp
+    static constexpr int LANES = 16;  // lanes per conflict-free group
+};
+template <>
+struct Elems<float> {
+    static constexpr int R = 32;
+    static constexpr int LANES = 32;
+};
+
+template <typename T, int BX, int BY, int BZ, int NCS>
+struct Tile {
+    static constexpr int EX = BX + 5, EY = BY + 5, EZ = BZ + 5;
+    static constexpr int PLANE = EX * EY;
+    static constexpr int VOL = PLANE * EZ;
+    // component stride: >= VOL and congruent to 11 (FP32) / 5 (FP64) modulo R so that the
+    // three components of one droplet start in different banks
+    static constexpr int SHIFT = (sizeof(T) == 8) ? 5 : 11;
+    static constexpr int R = Elems<T>::R;
+    static constexpr int CS = VOL + ((SHIFT - VOL % R) % R + R) % R;
+    static constexpr int FIELD = CS * NCS;
+};
+
+// PERIODIC's neighbour code of a droplet that left the single pencil (partlib.f90:874-1060)
+__device__ __forceinline__ int leave_nid(double y, double z, double pi2)
+{
+    const double ylo = 0.0, yhi = pi2, zlo = 0.0, zhi = pi2;
+    if (y > yhi && z <= zhi && z >= zlo) return 1;
+    if (y > yhi && z > zhi) return 2;
+    if (y >= ylo && y <= yhi && z > zhi) return 3;
+    if (y < ylo && z > zhi) return 4;
+    if (y < ylo && z <= zhi && z >= zlo) return 5;
+    if (y < ylo && z < zlo) return 6;
+    if (z < zlo && y <= yhi && y >= ylo) return 7;
+    if (z < zlo && y > yhi) return 8;
+    return 0;
+}
+
+// partlib.f90:1142-1151
+__device__ __forceinline__ double wrap_coord(double x, double h)
+{
+    if (x >= h) x = x - h;
+    if (x < 0.0) x = x + h;
+    return x;
+}
+
+// Advance of one droplet (partlib.f90:640-684) with the history already loaded.
+template <typename T>
+__device__ __forceinline__ void advance_math(T a, const T *u, const T *f0, const T *f1, const T *f2,
+                                             const T *d0, const T *d1, const T *d2, const T *d3,
+                                             T dt, T tau2, T sv, T rnu, int ndrag, T *vnew, T *dm)
+{
+    T fsn = (T)1.0;
+    if (ndrag == 1) {
+        T e0 = f0[0] - u[0], e1 = f0[1] - u[1], e2 = f0[2] - u[2];
+        T vrel = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
+        fsn = (T)1.0 + (T)0.15 * pow(vrel * (T)2.0 * a / rnu, (T)0.687);
+    }
+    T rad2 = a * a;
+    T taup = tau2 * rad2;
+    T dtau = dt / ((T)24.0 * taup) * fsn;
+    T wp = sv * rad2;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        T unitv = (c == 0) ? (T)1.0 : (T)0.0;
+        T tempv = (T)19.0 * f0[c] - (T)5.0 * f1[c] + f2[c];
+        T tempd = (T)55.0 * d0[c] - (T)59.0 * d1[c] + (T)37.0 * d2[c] - (T)9.0 * d3[c];
+        vnew[c] = (f0[c] + dt * unitv * wp / taup * fsn - dtau * tempv + dtau * tempd) / ((T)1.0 + (T)9.0 * dtau);
+    }
+    T dtc = dt / (T)24.0;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+        dm[c] = dtc * ((T)9.0 * vnew[c] + (T)19.0 * f0[c] - (T)5.0 * f1[c] + f2[c]);
+}
+
+// First-step history (partlib.f90:562-583, 606-615) and the advance epilogue of one droplet.
+template <typename T>
+__device__ __forceinline__ void epilogue_one(const InterpArgs<T> &A, int d, const T *u)
+{
+    T f0[3], f1[3], f2[3], d0[3], d1[3], d2[3], d3[3], vn[3], dm[3];
+    const double ad = A.rad[d];
+    const T a = (T)ad;
+    if (A.first) {
+        // yp(4:6) = terminal velocity (reference) or the fluid velocity (init_mode 1, 2)
+        T w = A.sv * (a * a);
+        if (A.init_mode == 0) {
+            f0[0] = w; f0[1] = (T)0; f0[2] = (T)0;
+        } else if (A.init_mode == 1) {
+            f0[0] = u[0]; f0[1] = u[1]; f0[2] = u[2];
+        } else {
+            f0[0] = u[0] + w; f0[1] = u[1]; f0[2] = u[2];
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            f1[c] = f0[c]; f2[c] = f0[c];
+            d0[c] = u[c]; d1[c] = u[c]; d2[c] = u[c]; d3[c] = u[c];
+            // all history levels hold the initial values after this step's shift
+            A.v0[c][d] = f0[c];
+            A.v1[c][d] = f0[c];
+            A.f1[c][d] = u[c];
+            A.f2[c][d] = u[c];
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            f0[c] = A.v0[c][d]; f1[c] = A.v1[c][d]; f2[c] = A.v2[c][d];
+            d0[c] = u[c]; d1[c] = A.f1[c][d]; d2[c] = A.f2[c][d]; d3[c] = A.f3[c][d];
+        }
+    }
+    advance_math<T>(a, u, f0, f1, f2, d0, d1, d2, d3, A.dt, A.tau2, A.sv, A.rnu, A.ndrag, vn, dm);
+    double xo[3] = {A.px[d], A.py[d], A.pz[d]};
+    double xn[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        A.fnew[c][d] = u[c];
+        A.vnew[c][d] = vn[c];
+        A.dmv[c][d] = dm[c];
+        xn[c] = xo[c] + (double)dm[c];
+    }
+    int nid = leave_nid(xn[1], xn[2], A.pi2);
+    A.qx[d] = wrap_coord(xn[0], A.pi2);
+    A.qy[d] = wrap_coord(xn[1], A.pi2);
+    A.qz[d] = wrap_coord(xn[2], A.pi2);
+    if (nid) A.leave_nid[A.ref_of_dev[d]] = (signed char)nid;
+}
+
+// ---------------------------------------------------------------------------------------
+// The brick kernel
+// ---------------------------------------------------------------------------------------
+template <typename T, int BX, int BY, int BZ, int NCS, int MAXD>
+__global__ void __launch_bounds__(kThreads) k_interp(InterpArgs<T> A)
+{
+    using TL = Tile<T, BX, BY, BZ, NCS>;
+    constexpr int R = Elems<T>::R;
+    constexpr int NW = kThreads / 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *sf = reinterpret_cast<T *>(smem_raw);                      // field tile [NCS][CS]
+    T *sw = sf + TL::FIELD;                                       // weights [MAXD][18]
+    T *sv = sw + MAXD * 18;                                       // results [MAXD][3]
+    int *scorner = reinterpret_cast<int *>(sv + MAXD * 3);        // corner offset or -1
+    int *snode = scorner + MAXD;                                  // [MAXD][3] nodes (fallback)
+    int *scnt = snode + MAXD * 3;                                 // [R]
+    int *sstart = scnt + R;                                       // [R]
+    int *sfill = sstart + R;                                      // [R]
+    int *sfb = sfill + R;                                         // fallback count
+    int *sg = sfb + 1;                                            // max bucket
+    unsigned short *stask = reinterpret_cast<unsigned short *>(sg + 1);   // [MAXD*NCS]
+    unsigned short *sfbt = stask + MAXD * NCS;                             // [MAXD*NCS]
+
+    const int b = blockIdx.x;
+    const int bxi = b % A.nbx, byi = (b / A.nbx) % A.nby, bzi = b / (A.nbx * A.nby);
+    const int d0 = A.brick_start[b], d1 = A.brick_start[b + 1];
+    if (d0 >= d1) return;
+    const int gx0 = bxi * BX - 2, gy0 = byi * BY - 2, gz0 = bzi * BZ - 2;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n = A.n;
+
+    for (int c0 = d0; c0 < d1; c0 += MAXD) {
+        const int nd = min(MAXD, d1 - c0);
+        // ---- Phase A: nodes, weights, corners ----
+        for (int i = tid; i < nd; i += kThreads) {
+            const int d = c0 + i;
+            double pos[3] = {A.px[d], A.py[d], A.pz[d]};
+            int node[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                double z;
+                node[k] = node_frac(pos[k], A.dx, &z);
+                T w[6];
+                lagrange6((T)z, w);
+#pragma unroll
+                for (int q = 0; q < 6; q++) sw[i * 18 + k * 6 + q] = w[q];
+                snode[i * 3 + k] = node[k];
+            }
+            int lx = node[0] - 2 - gx0, ly = node[1] - 2 - gy0, lz = node[2] - 2 - gz0;
+            bool in = lx >= 0 && lx < BX && ly >= 0 && ly < BY && lz >= 0 && lz < BZ;
+            scorner[i] = in ? (lz * TL::EY + ly) * TL::EX + lx : -1;
+        }
+        for (int cg = A.comp_lo; cg < A.comp_lo + A.ncomp; cg += NCS) {
+            const int ncs = min(NCS, A.comp_lo + A.ncomp - cg);
+            if (tid < R) { scnt[tid] = 0; sfill[tid] = 0; }
+            if (tid == 0) *sfb = 0;
+            // ---- stage the field region of this brick: asynchronous copies, all in flight ----
+            for (int cc = 0; cc < ncs; cc++) {
+                T *dst = sf + cc * TL::CS;
+                const int comp = cg + cc;
+                for (int e = tid; e < TL::VOL; e += kThreads) {
+                    int x = e % TL::EX, yz = e / TL::EX, y = yz % TL::EY, z = yz / TL::EY;
+                    int gx = gx0 + x, gy = gy0 + y, gz = gz0 + z;
+                    const T *src;
+                    if constexpr (sizeof(T) == 8) {
+                        gx = gx < 0 ? gx + n : (gx >= n ? gx - n : gx);
+                        gy = gy < 0 ? gy + n : (gy >= n ? gy - n : gy);
+                        gz = gz < 0 ? gz + n : (gz >= n ? gz - n : gz);
+                        src = A.f64[comp] + gx + A.f64py[comp] * gy + A.f64pz[comp] * gz;
+                    } else {
+                        // bricks that overhang the grid (n not a multiple of the brick) wrap
+                        if (gx >= n + DL_PAD_HI) gx -= n;
+                        if (gy >= n + DL_PAD_HI) gy -= n;
+                        if (gz >= n + DL_PAD_HI) gz -= n;
+                        src = A.f32 + comp * A.f32comp + (int64_t)(gx + DL_PAD_LO) + A.f32py * (gy + DL_PAD_LO) +
+                              A.f32pz * (gz + DL_PAD_LO);
+                    }
+                    cp_async<sizeof(T)>(dst + e, src);
+                }
+            }
+            cp_async_wait_all();
+            __syncthreads();
+            // ---- bucket tasks by starting bank ----
+            for (int t = tid; t < nd * ncs; t += kThreads) {
+                int i = t / ncs, cc = t % ncs;
+                int cr = scorner[i];
+                if (cr >= 0) atomicAdd(&scnt[(cr + cc * TL::CS) % R], 1);
+                else sfbt[atomicAdd(sfb, 1)] = (unsigned short)t;
+            }
+            __syncthreads();
+            if (warp == 0) {
+                int v = lane < R ? scnt[lane] : 0;
+                int incl = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                int mx = v;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                if (lane < R) sstart[lane] = incl - v;
+                if (lane == 0) *sg = mx;
+            }
+            __syncthreads();
+            for (int t = tid; t < nd * ncs; t += kThreads) {
+                int i = t / ncs, cc = t % ncs;
+                int cr = scorner[i];
+                if (cr >= 0) {
+                    int r = (cr + cc * TL::CS) % R;
+                    stask[sstart[r] + atomicAdd(&sfill[r], 1)] = (unsigned short)t;
+                }
+            }
+            __syncthreads();
+            // ---- conflict-free groups: lane r of group g takes the g-th task of bucket r ----
+            {
+                const int G = *sg;
+                constexpr int GPW = 32 / Elems<T>::LANES;   // groups per warp instruction
+                const int sub = lane / Elems<T>::LANES, r = lane % Elems<T>::LANES;
+                for (int g = warp * GPW + sub; g < G; g += NW * GPW) {
+                    if (g < scnt[r]) {
+                        int t = stask[sstart[r] + g];
+                        int i = t / ncs, cc = t % ncs;
+                        SmemLoader<T> ld{sf + cc * TL::CS + scorner[i], TL::EX, TL::PLANE};
+                        const T *w = sw + i * 18;
+                        T bx[6], by[6], bz[6];
+#pragma unroll
+                        for (int q = 0; q < 6; q++) { bx[q] = w[q]; by[q] = w[6 + q]; bz[q] = w[12 + q]; }
+                        sv[i * 3 + cg + cc] = stencil(ld, bx, by, bz);
+                    }
+                }
+            }
+            // ---- droplets outside the staged region: global memory, same arithmetic ----
+            for (int q = tid; q < *sfb; q += kThreads) {
+                int t = sfbt[q];
+                int i = t / ncs, cc = t % ncs, comp = cg + cc;
+                const T *w = sw + i * 18;
+                T bx[6], by[6], bz[6];
+#pragma unroll
+                for (int k = 0; k < 6; k++) { bx[k] = w[k]; by[k] = w[6 + k]; bz[k] = w[12 + k]; }
+                T r;
+                if constexpr (sizeof(T) == 8) {
+                    GlobalLoader64 ld;
+                    ld.f = A.f64[comp]; ld.py = A.f64py[comp]; ld.pz = A.f64pz[comp];
+#pragma unroll
+                    for (int k = 0; k < 6; k++) {
+                        ld.ix[k] = wrapi(snode[i * 3 + 0] - 2 + k, n);
+                        ld.iy[k] = wrapi(snode[i * 3 + 1] - 2 + k, n);
+                        ld.iz[k] = wrapi(snode[i * 3 + 2] - 2 + k, n);
+                    }
+                    r = stencil(ld, bx, by, bz);
+                } else {
+                    GlobalLoader32 ld;
+                    int x0 = wrapi(snode[i * 3 + 0], n) - 2 + DL_PAD_LO;
+                    int y0 = wrapi(snode[i * 3 + 1], n) - 2 + DL_PAD_LO;
+                    int z0 = wrapi(snode[i * 3 + 2], n) - 2 + DL_PAD_LO;
+                    ld.f = A.f32 + comp * A.f32comp + x0 + A.f32py * y0 + A.f32pz * z0;
+                    ld.py = A.f32py; ld.pz = A.f32pz;
+                    r = stencil(ld, bx, by, bz);
+                }
+                sv[i * 3 + comp] = r;
+            }
+            __syncthreads();
+        }
+        // ---- epilogue ----
+        for (int i = tid; i < nd; i += kThreads) {
+            const int d = c0 + i;
+            if (A.fused) {
+                T u[3] = {sv[i * 3 + 0], sv[i * 3 + 1], sv[i * 3 + 2]};
+                epilogue_one<T>(A, d, u);
+            } else {
+                for (int comp = A.comp_lo; comp < A.comp_lo + A.ncomp; comp++) A.vp[comp][d] = sv[i * 3 + comp];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int BX, int BY, int BZ, int NCS, int MAXD>
+size_t interp_smem()
+{
+    using TL = Tile<T, BX, BY, BZ, NCS>;
+    constexpr int R = Elems<T>::R;
+    size_t s = sizeof(T) * (TL::FIELD + MAXD * 18 + MAXD * 3);
+    s += sizeof(int) * (MAXD + MAXD * 3 + 3 * R + 2);
+    s += sizeof(unsigned short) * 2 * MAXD * NCS;
+    return (s + 15) & ~size_t(15);
+}
+
+// ---------------------------------------------------------------------------------------
+// Brick sort of the device order
+// ---------------------------------------------------------------------------------------
+__global__ void k_brick_keys(int nps, const double *px, const double *py, const double *pz, double dx, int n,
+                             int bx, int by, int bz, int nbx, int nby, int *keys, int *cnt, const double *rad,
+                             int dead_key)
+{
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= nps) return;
+    if (dead_key >= 0 && rad[d] < 0.0) {   // removed by COALESCE: sorted past the last brick
+        keys[d] = dead_key;
+        atomicAdd(&cnt[dead_key], 1);
+        return;
+    }
+    int ix = (int)floor(px[d] / dx), iy = (int)floor(py[d] / dx), iz = (int)floor(pz[d] / dx);
+    ix = min(max(ix, 0), n - 1);
+    iy = min(max(iy, 0), n - 1);
+    iz = min(max(iz, 0), n - 1);
+    int key = ((iz / bz) * nby + (iy / by)) * nbx + (ix / bx);
+    keys[d] = key;
+    atomicAdd(&cnt[key], 1);
+}
+
+// Exclusive scan of cnt[0..m) into start[0..m] by one CTA of 1024 threads.
+__global__ void k_scan_single(const int *cnt, int *start, int m)
+{
+    __shared__ int warp_sums[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int base = 0; base < m; base += blockDim.x) {
+        int i = base + threadIdx.x;
+        int v = i < m ? cnt[i] : 0;
+        int incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) warp_sums[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            int s = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+            int si = s;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, si, o);
+                if (lane >= o) si += y;
+            }
+            warp_sums[lane] = si - s;
+        }
+        __syncthreads();
+        int excl = carry + warp_sums[w] + incl - v;
+        if (i < m) start[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) start[m] = carry;
+}
+
+__global__ void k_brick_scatter(int nps, const int *keys, const int *start, int *fill, int *perm)
+{
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= nps) return;
+    int k = keys[d];
+    perm[start[k] + atomicAdd(&fill[k], 1)] = d;
+}
+
+template <typename E>
+__global__ void k_gather(int nps, const int *perm, const E *in, E *out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nps) out[i] = in[perm[i]];
+}
+
+__global__ void k_inverse(int nps, const int *ref_of_dev, int *dev_of_ref)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nps && ref_of_dev[i] >= 0) dev_of_ref[ref_of_dev[i]] = i;
+}
+
+// ---------------------------------------------------------------------------------------
+// Separate-call kernels
+// ---------------------------------------------------------------------------------------
+// PREPARE_INTERP outputs in reference order: lhnode(ref, 3), bg(ref, 6, 3)
+__global__ void k_prepare_interp(int nps, const double *px, const double *py, const double *pz, double dx,
+                                 const int *ref_of_dev, int *lh, double *bg)
+{
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= nps) return;
+    int r = ref_of_dev[d];
+    const double pos[3] = {px[d], py[d], pz[d]};
+    for (int k = 0; k < 3; k++) {
+        double z, w[6];
+        int node = node_frac(pos[k], dx, &z);
+        lagrange6(z, w);
+        lh[(int64_t)r * 3 + k] = node;
+        for (int q = 0; q < 6; q++) bg[((int64_t)r * 3 + k) * 6 + q] = w[q];
+    }
+}
+
+// PART_HISTORY_FVP at the first step: yp(4:6) and every fvp level (partlib.f90:562-583)
+template <typename T>
+__global__ void k_history_fvp_first(int nps, const double *rad, T sv, int init_mode, T *v0x, T *v0y, T *v0z,
+                                    T *v1x, T *v1y, T *v1z, T *v2x, T *v2y, T *v2z, const T *ux, const T *uy,
+                                    const T *uz)
+{
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= nps) return;
+    T a = (T)rad[d];
+    T w = sv * (a * a);
+    T f[3];
+    if (init_mode == 0) { f[0] = w; f[1] = (T)0; f[2] = (T)0; }
+    else if (init_mode == 1) { f[0] = ux[d]; f[1] = uy[d]; f[2] = uz[d]; }
+    else { f[0] = ux[d] + w; f[1] = uy[d]; f[2] = uz[d]; }
+    v0x[d] = f[0]; v0y[d] = f[1]; v0z[d] = f[2];
+    v1x[d] = f[0]; v1y[d] = f[1]; v1z[d] = f[2];
+    v2x[d] = f[0]; v2y[d] = f[1]; v2z[d] = f[2];
+}
+
+// PART_HISTORY_FDP (partlib.f90:599-625): fdp(:,0) = vp (+ pertvel); first step: every level
+template <typename T>
+__global__ void k_history_fdp(int nps, int first, int hdi, const T *ux, const T *uy, const T *uz, const T *px_,
+                              const T *py_, const T *pz_, T *f0x, T *f0y, T *f0z, T *f1x, T *f1y, T *f1z, T *f2x,
+                              T *f2y, T *f2z, T *f3x, T *f3y, T *f3z)
+{
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= nps) return;
+    T u[3] = {ux[d], uy[d], uz[d]};
+    if (hdi) { u[0] = u[0] + px_[d]; u[1] = u[1] + py_[d]; u[2] = u[2] + pz_[d]; }
+    f0x[d] = u[0]; f0y[d] = u[1]; f0z[d] = u[2];
+    if (first) {
+        f1x[d] = u[0]; f1y[d] = u[1]; f1z[d] = u[2];
+        f2x[d] = u[0]; f2y[d] = u[1]; f2z[d] = u[2];
+        f3x[d] = u[0]; f3y[d] = u[1]; f3z[d] = u[2];
+    }
+}
+
+template <typename T>
+struct AdvArgs {
+    int nps, ndrag, hdi;
+    T dt, tau2, sv, rnu;
+    const double *rad;
+    const T *v0[3], *v1[3], *v2[3];
+    const T *d0[3], *d1[3], *d2[3], *d3[3];
+    const T *u[3], *pert[3];
+    T *vn[3], *dm[3];
+};
+
+// PART_ADVANCE (partlib.f90:629-726)
+template <typename T>
+__global__ void k_advance(AdvArgs<T> A)
+{
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= A.nps) return;
+    T f0[3], f1[3], f2[3], e0[3], e1[3], e2[3], e3[3], u[3], vn[3], dm[3];
+    for (int c = 0; c < 3; c++) {
+        f0[c] = A.v0[c][d]; f1[c] = A.v1[c][d]; f2[c] = A.v2[c][d];
+        e0[c] = A.d0[c][d]; e1[c] = A.d1[c][d]; e2[c] = A.d2[c][d]; e3[c] = A.d3[c][d];
+        u[c] = A.u[c][d];
+        if (A.hdi) u[c] = u[c] + A.pert[c][d];
+    }
+    advance_math<T>((T)A.rad[d], u, f0, f1, f2, e0, e1, e2, e3, A.dt, A.tau2, A.sv, A.rnu, A.ndrag, vn, dm);
+    for (int c = 0; c < 3; c++) { A.vn[c][d] = vn[c]; A.dm[c][d] = dm[c]; }
+}
+
+// UPDATE_PART_POSITION position part: q = p + dmove (unwrapped; PERIODIC wraps later)
+template <typename T>
+__global__ void k_update_pos(int nps, const double *px, const double *py, const double *pz, const T *dx,
+                             const T *dy, const T *dz, double *qx, double *qy, double *qz)
+{
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= nps) return;
+    qx[d] = px[d] + (double)dx[d];
+    qy[d] = py[d] + (double)dy[d];
+    qz[d] = pz[d] + (double)dz[d];
+}
+
+// FP64 field -> FP32 periodic-halo copy (mixed path)
+__global__ void k_convert_field(const double *v, int64_t py, int64_t pz, int n, float *out, int64_t opy,
+                                int64_t opz)
+{
+    const int e = n + DL_PAD_LO + DL_PAD_HI;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t tot = (int64_t)e * e * e;
+    if (i >= tot) return;
+    int x = (int)(i % e);
+    int64_t yz = i / e;
+    int y = (int)(yz % e), z = (int)(yz / e);
+    int gx = wrapi(x - DL_PAD_LO, n), gy = wrapi(y - DL_PAD_LO, n), gz = wrapi(z - DL_PAD_LO, n);
+    out[x + opy * y + opz * z] = (float)v[gx + py * gy + pz * gz];
+}
+
+// MEAN_VEL partial sums (partlib.f90:1910-1930) -> 11*nset doubles via FP64 atomics.
+template <typename T>
+__global__ void k_mean_vel(int nps, const T *ux, const T *uy, const T *uz, const double *rad, int nset,
+                           const double *radius, double *acc)
+{
+    __shared__ double sacc[110];
+    for (int i = threadIdx.x; i < 11 * nset; i += blockDim.x) sacc[i] = 0.0;
+    __syncthreads();
+    int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d < nps) {
+        double a = rad[d], dmin = 100.0;
+        int idp = 1;
+        for (int ij = 1; ij <= nset; ij++) {
+            double dd = fabs(a - radius[ij - 1]);
+            if (dd < dmin) { dmin = dd; idp = ij; }
+        }
+        double u[3] = {(double)ux[d], (double)uy[d], (double)uz[d]};
+        for (int c = 0; c < 3; c++) {
+            atomicAdd(&sacc[c + 3 * (idp - 1)], u[c]);
+            atomicAdd(&sacc[3 * nset + c + 3 * (idp - 1)], u[c] * u[c]);
+            atomicAdd(&sacc[6 * nset + c + 3 * (idp - 1)], fabs(u[c]));
+        }
+        atomicAdd(&sacc[9 * nset + idp - 1], sqrt(u[1] * u[1] + u[2] * u[2]));
+        atomicAdd(&sacc[10 * nset + idp - 1], sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]));
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 11 * nset; i += blockDim.x)
+        if (sacc[i] != 0.0) atomicAdd(&acc[i], sacc[i]);
+}
+
+// brick configurations (cells) per precision
+constexpr int F32_BX = 16, F32_BY = 16, F32_BZ = 8, F32_NCS = 3, F32_MAXD = 256;
+constexpr int F64_BX = 12, F64_BY = 12, F64_BZ = 8, F64_NCS = 3, F64_MAXD = 192;
+
+template <typename T>
+T *tp(void *p) { return reinterpret_cast<T *>(p); }
+
+}  // namespace
+
+// =======================================================================================
+// Launchers
+// =======================================================================================
+int launch_brick_sort(dl_ctx *c)
+{
+    const int nps = c->nps;
+    c->steps_since_sort = 0;
+    c->sorted = 1;
+    if (nps == 0) {
+        DL_CUDA(c, cudaMemsetAsync(c->brick_start, 0, sizeof(int) * (c->nbricks + 1), c->stream));
+        return 0;
+    }
+    const int t = 256;
+    const int nkeys = c->nbricks + (c->has_dead ? 1 : 0);
+    DL_CUDA(c, cudaMemsetAsync(c->brick_cnt, 0, sizeof(int) * nkeys, c->stream));
+    const double *P[3] = {c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2]};
+    k_brick_keys<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, P[0], P[1], P[2], c->dc.dx, c->dc.n, c->bx, c->by,
+                                                         c->bz, c->nbx, c->nby, c->keys, c->brick_cnt, c->rad,
+                                                         c->has_dead ? c->nbricks : -1);
+    DL_CHECK_LAUNCH(c);
+    k_scan_single<<<1, 1024, 0, c->stream>>>(c->brick_cnt, c->brick_start, nkeys);
+    DL_CHECK_LAUNCH(c);
+    DL_CUDA(c, cudaMemsetAsync(c->brick_cnt, 0, sizeof(int) * nkeys, c->stream));
+    k_brick_scatter<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, c->keys, c->brick_start, c->brick_cnt, c->perm);
+    DL_CHECK_LAUNCH(c);
+    // permute every live array through a scratch buffer of the same element size (pointer swap)
+    auto perm8 = [&](void *&arr) -> int {
+        k_gather<unsigned long long><<<dl_blocks(nps, t), t, 0, c->stream>>>(
+            nps, c->perm, (const unsigned long long *)arr, (unsigned long long *)c->scratch8);
+        std::swap(arr, c->scratch8);
+        return 0;
+    };
+    auto perm4 = [&](void *&arr) -> int {
+        k_gather<unsigned int><<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, c->perm, (const unsigned int *)arr,
+                                                                       (unsigned int *)c->scratch4);
+        std::swap(arr, c->scratch4);
+        return 0;
+    };
+    auto permT = [&](void *&arr) { return c->mixed ? perm4(arr) : perm8(arr); };
+    for (int k = 0; k < 3; k++) {
+        void *p = c->pos[c->pcur][k];
+        perm8(p);
+        c->pos[c->pcur][k] = (double *)p;
+        for (int l = 0; l < 3; l++) permT(c->vel[(c->vcur + l) % 4][k]);
+        for (int l = 0; l < 3; l++) permT(c->flu[(c->fcur + l) % 4][k]);
+        permT(c->vpv[k]);
+        permT(c->dmv[k]);
+        if (c->pert[k]) permT(c->pert[k]);
+    }
+    {
+        void *p = c->rad; perm8(p); c->rad = (double *)p;
+        p = c->gid; perm8(p); c->gid = (double *)p;
+        p = c->ref_of_dev; perm4(p); c->ref_of_dev = (int *)p;
+    }
+    if (c->has_dead) {
+        int live = 0;
+        DL_CUDA(c, cudaMemcpyAsync(&live, c->brick_start + c->nbricks, sizeof(int), cudaMemcpyDeviceToHost,
+                                   c->stream));
+        DL_CUDA(c, cudaStreamSynchronize(c->stream));
+        c->nps = live;
+        c->has_dead = 0;
+    }
+    k_inverse<<<dl_blocks(c->nps, t), t, 0, c->stream>>>(c->nps, c->ref_of_dev, c->dev_of_ref);
+    DL_CHECK_LAUNCH(c);
+    c->hl_valid = 0;
+    return 0;
+}
+
+template <typename T, int BX, int BY, int BZ, int NCS, int MAXD>
+static int launch_interp_t(dl_ctx *c, int comp_lo, int ncomp, int fused)
+{
+    InterpArgs<T> A;
+    memset(&A, 0, sizeof(A));
+    A.n = c->dc.n;
+    A.nps = c->nps;
+    A.dx = c->dc.dx;
+    A.pi2 = c->dc.pi2;
+    A.px = c->pos[c->pcur][0]; A.py = c->pos[c->pcur][1]; A.pz = c->pos[c->pcur][2];
+    A.brick_start = c->brick_start;
+    A.nbx = c->nbx; A.nby = c->nby;
+    for (int k = 0; k < 3; k++) {
+        A.f64[k] = c->f64[k];
+        A.f64py[k] = c->fpy[k];
+        A.f64pz[k] = c->fpz[k];
+        A.vp[k] = tp<T>(c->vpv[k]);
+    }
+    A.f32 = c->f32;
+    A.f32py = c->f32_pitch;
+    A.f32pz = c->f32_plane;
+    A.f32comp = c->f32_comp;
+    A.comp_lo = comp_lo;
+    A.ncomp = ncomp;
+    A.fused = fused;
+    if (fused) {
+        A.first = c->new_particle;
+        A.init_mode = c->p.init_velocity;
+        A.ndrag = c->dc.ndrag;
+        A.dt = (T)c->dc.dt; A.tau2 = (T)c->dc.tau2; A.sv = (T)c->dc.sv; A.rnu = (T)c->dc.rnu;
+        A.rad = c->rad;
+        c->vnew = (c->vcur + 3) % 4;
+        c->fnew = (c->fcur + 3) % 4;
+        for (int k = 0; k < 3; k++) {
+            A.v0[k] = tp<T>(c->vel[c->vcur][k]);
+            A.v1[k] = tp<T>(c->vel[(c->vcur + 1) % 4][k]);
+            A.v2[k] = tp<T>(c->vel[(c->vcur + 2) % 4][k]);
+            A.vnew[k] = tp<T>(c->vel[c->vnew][k]);
+            A.f1[k] = tp<T>(c->flu[c->fcur][k]);
+            A.f2[k] = tp<T>(c->flu[(c->fcur + 1) % 4][k]);
+            A.f3[k] = tp<T>(c->flu[(c->fcur + 2) % 4][k]);
+            A.fnew[k] = tp<T>(c->flu[c->fnew][k]);
+            A.dmv[k] = tp<T>(c->dmv[k]);
+        }
+        A.qx = c->pos[1 - c->pcur][0]; A.qy = c->pos[1 - c->pcur][1]; A.qz = c->pos[1 - c->pcur][2];
+        A.ref_of_dev = c->ref_of_dev;
+        A.leave_nid = c->leave_nid;
+    }
+    size_t sm = interp_smem<T, BX, BY, BZ, NCS, MAXD>();
+    auto kern = k_interp<T, BX, BY, BZ, NCS, MAXD>;
+    DL_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<c->nbricks, kThreads, sm, c->stream>>>(A);
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}
+
+int launch_interp(dl_ctx *c, int icpt, int fused)
+{
+    if (c->nps == 0) return 0;
+    int lo = icpt > 0 ? icpt - 1 : 0, nc = icpt > 0 ? 1 : 3;
+    if (c->mixed) return launch_interp_t<float, F32_BX, F32_BY, F32_BZ, F32_NCS, F32_MAXD>(c, lo, nc, fused);
+    return launch_interp_t<double, F64_BX, F64_BY, F64_BZ, F64_NCS, F64_MAXD>(c, lo, nc, fused);
+}
+
+void dl_brick_dims(int mixed, int *bx, int *by, int *bz)
+{
+    if (mixed) { *bx = F32_BX; *by = F32_BY; *bz = F32_BZ; }
+    else { *bx = F64_BX; *by = F64_BY; *bz = F64_BZ; }
+}
+
+int launch_prepare_interp(dl_ctx *c)
+{
+    if (c->nps == 0) return 0;
+    k_prepare_interp<<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(
+        c->nps, c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2], c->dc.dx, c->ref_of_dev, c->lhnode,
+        c->bg);
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}
+
+template <typename T>
+static int history_fvp_t(dl_ctx *c)
+{
+    auto V = [&](int l, int k) { return tp<T>(c->vel[(c->vcur + l) % 4][k]); };
+    k_history_fvp_first<T><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(
+        c->nps, c->rad, (T)c->dc.sv, c->p.init_velocity, V(0, 0), V(0, 1), V(0, 2), V(1, 0), V(1, 1), V(1, 2),
+        V(2, 0), V(2, 1), V(2, 2), tp<T>(c->vpv[0]), tp<T>(c->vpv[1]), tp<T>(c->vpv[2]));
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}
+
+int launch_history_fvp(dl_ctx *c)
+{
+    // Only the first step writes anything: fvp(:,0) is yp(4:6) itself in the ring layout.
+    if (!c->new_particle || c->nps == 0) return 0;
+    return c->mixed ? history_fvp_t<float>(c) : history_fvp_t<double>(c);
+}
+
+template <typename T>
+static int history_fdp_t(dl_ctx *c)
+{
+    c->fnew = (c->fcur + 3) % 4;
+    auto F = [&](int s, int k) { return tp<T>(c->flu[s % 4][k]); };
+    const T *pz_[3] = {nullptr, nullptr, nullptr};
+    if (c->dc.hdi)
+        for (int k = 0; k < 3; k++) pz_[k] = tp<T>(c->pert[k]);
+    k_history_fdp<T><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(
+        c->nps, c->new_particle, c->dc.hdi, tp<T>(c->vpv[0]), tp<T>(c->vpv[1]), tp<T>(c->vpv[2]), pz_[0], pz_[1],
+        pz_[2], F(c->fnew, 0), F(c->fnew, 1), F(c->fnew, 2), F(c->fcur, 0), F(c->fcur, 1), F(c->fcur, 2),
+        F(c->fcur + 1, 0), F(c->fcur + 1, 1), F(c->fcur + 1, 2), F(c->fcur + 2, 0), F(c->fcur + 2, 1),
+        F(c->fcur + 2, 2));
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}
+
+int launch_history_fdp(dl_ctx *c)
+{
+    if (c->nps == 0) { c->fnew = (c->fcur + 3) % 4; return 0; }
+    return c->mixed ? history_fdp_t<float>(c) : history_fdp_t<double>(c);
+}
+
+template <typename T>
+static int advance_t(dl_ctx *c)
+{
+    AdvArgs<T> A;
+    memset(&A, 0, sizeof(A));
+    A.nps = c->nps; A.ndrag = c->dc.ndrag; A.hdi = c->dc.hdi;
+    A.dt = (T)c->dc.dt; A.tau2 = (T)c->dc.tau2; A.sv = (T)c->dc.sv; A.rnu = (T)c->dc.rnu;
+    A.rad = c->rad;
+    c->vnew = (c->vcur + 3) % 4;
+    for (int k = 0; k < 3; k++) {
+        A.v0[k] = tp<T>(c->vel[c->vcur][k]);
+        A.v1[k] = tp<T>(c->vel[(c->vcur + 1) % 4][k]);
+        A.v2[k] = tp<T>(c->vel[(c->vcur + 2) % 4][k]);
+        A.d0[k] = tp<T>(c->flu[c->fnew][k]);
+        A.d1[k] = tp<T>(c->flu[c->fcur][k]);
+        A.d2[k] = tp<T>(c->flu[(c->fcur + 1) % 4][k]);
+        A.d3[k] = tp<T>(c->flu[(c->fcur + 2) % 4][k]);
+        A.u[k] = tp<T>(c->vpv[k]);
+        A.pert[k] = c->pert[k] ? tp<T>(c->pert[k]) : nullptr;
+        A.vn[k] = tp<T>(c->vel[c->vnew][k]);
+        A.dm[k] = tp<T>(c->dmv[k]);
+    }
+    k_advance<T><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(A);
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}
+
+int launch_advance(dl_ctx *c)
+{
+    if (c->nps == 0) { c->vnew = (c->vcur + 3) % 4; return 0; }
+    return c->mixed ? advance_t<float>(c) : advance_t<double>(c);
+}
+
+template <typename T>
+static int update_pos_t(dl_ctx *c)
+{
+    k_update_pos<T><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(
+        c->nps, c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2], tp<T>(c->dmv[0]), tp<T>(c->dmv[1]),
+        tp<T>(c->dmv[2]), c->pos[1 - c->pcur][0], c->pos[1 - c->pcur][1], c->pos[1 - c->pcur][2]);
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}
+
+int launch_update_position(dl_ctx *c, int)
+{
+    if (c->nps > 0) {
+        int r = c->mixed ? update_pos_t<float>(c) : update_pos_t<double>(c);
+        if (r) return r;
+    }
+    c->pcur = 1 - c->pcur;
+    return 0;
+}
+
+int launch_convert_field(dl_ctx *c, int icpt)
+{
+    const int n = c->dc.n, e = n + DL_PAD_LO + DL_PAD_HI;
+    int64_t tot = (int64_t)e * e * e;
+    float *out = c->f32 + (int64_t)(icpt - 1) * c->f32_comp;
+    k_convert_field<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->f64[icpt - 1], c->fpy[icpt - 1],
+                                                                          c->fpz[icpt - 1], n, out, c->f32_pitch,
+                                                                          c->f32_plane);
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}
+
+template <typename T>
+static int mean_vel_t(dl_ctx *c, double *host_out)
+{
+    const int nset = c->dc.nset;
+    DL_CUDA(c, cudaMemsetAsync(c->mv_acc, 0, sizeof(double) * 11 * nset, c->stream));
+    if (c->nps > 0) {
+        double *rad_d = c->mv_acc + 11 * 10;
+        DL_CUDA(c, cudaMemcpyAsync(rad_d, c->dc.radius, sizeof(double) * 10, cudaMemcpyHostToDevice, c->stream));
+        k_mean_vel<T><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(
+            c->nps, tp<T>(c->vel[c->vcur][0]), tp<T>(c->vel[c->vcur][1]), tp<T>(c->vel[c->vcur][2]), c->rad, nset,
+            rad_d, c->mv_acc);
+        DL_CHECK_LAUNCH(c);
+    }
+    DL_CUDA(c, cudaMemcpyAsync(host_out, c->mv_acc, sizeof(double) * 11 * nset, cudaMemcpyDeviceToHost, c->stream));
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < 11 * nset; i++) host_out[i] = host_out[i] / (double)c->p.npart * (double)nset;
+    return 0;
+}
+
+int launch_mean_vel(dl_ctx *c, double *host_out)
+{
+    return c->mixed ? mean_vel_t<float>(c, host_out) : mean_vel_t<double>(c, host_out);
+}
