@@ -1,0 +1,316 @@
+"""Benchmark of the droplet update path (particle-updates/s) on B200.
+
+Workload (N = 1): the headline configuration's shape -- a 256^3 periodic field and
+1,000,000 droplets with radii uniform in [10, 40] um -- with the mixed-precision path as
+the measured value and the FP64 path beside it.  One "step" is one droplet substep of the
+update path: interpolation of the three velocity components, history, drag advance,
+position update, periodic wrap and the PERIODIC reorder (plus the amortised spatial
+re-sort of the device order).  Inputs (field, droplet state) are resident in HBM when the
+timed region starts and are larger than L2 (field 218 MB FP32 / 441 MB FP64, droplet
+state ~0.2 GB), so no L2 flush is needed.  N > 1 runs independent replicas, one per GPU
+(the path does not shard on one node; weak scaling).
+
+``--impl reference`` times the CPU restatement of the reference's path (the reference
+itself cannot be built here) on this host's cores on a bounded sample of droplets.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_GRID = 256
+N_PART = 1_000_000
+SETS_UM = [10.0, 20.0, 30.0, 40.0]
+PHYS = dict(dt=5e-4, rnu=8e-4, etk_dns=0.0079, tauk_dns=0.078)
+CONFIG = {"workload": "256^3 field, 1,000,000 droplets, radii U[10,40] um, update substep",
+          "grid": N_GRID, "droplets": N_PART, "precision": "mixed (FP32 arithmetic, FP64 positions)",
+          "l2": "no flush: inputs larger than L2 (FP32 field 218 MB + droplet state ~0.2 GB)",
+          "parallelism": "replicas"}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _clock_sampler(dev: int):
+    cmd = ["nvidia-smi", f"--id={dev}",
+           "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+           "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+           "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"]
+    try:
+        return subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except OSError:
+        return None
+
+
+def _clock_summary(proc):
+    if proc is None:
+        return None
+    proc.terminate()
+    try:
+        out, _ = proc.communicate(timeout=5)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+        out, _ = proc.communicate()
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in out.strip().splitlines():
+        f = [x.strip() for x in line.split(",")]
+        if len(f) < 6:
+            continue
+        try:
+            sm.append(float(f[0])); mx.append(float(f[1]))
+        except ValueError:
+            continue
+        for nm, v in zip(names, f[2:6]):
+            if v.lower().startswith("active"):
+                reasons.add(nm)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _profile_traffic():
+    """DRAM bytes per update step of the two update kernels from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "update_kernels_mixed_256_1M.md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"traffic_bytes_per_step:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+def _make(precision, dev, npart=N_PART, n=N_GRID):
+    import numpy as np
+    from mpi_2d_domain_decomp_turb_particles_b200 import Partlib, ParticleParams
+    from mpi_2d_domain_decomp_turb_particles_b200.synthetic import droplets
+    p = ParticleParams(nx=n, npart=npart, radius_um=SETS_UM, precision=precision, device=dev,
+                       new_particle=True, **PHYS)
+    g = Partlib(p)
+    g.part_init()
+    s = g.scalars()
+    scale = s.radius[0] / SETS_UM[0]
+    yp = droplets(npart, scale, radius_um=(10.0, 40.0), seed=290710 + 17 * dev)
+    g.set_particles(yp)
+    return g
+
+
+def _time_update(g, stream, steps, warmup, torch):
+    for _ in range(warmup):
+        g.update_step()
+    g.sync()
+    g.timing(reset=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        g.update_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    kms, nk, launches = g.timing(reset=True)
+    return ms / steps, kms, launches
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from mpi_2d_domain_decomp_turb_particles_b200.bytes_model import update_bytes
+
+    ws, rank, local = _dist()
+    if ws > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = local
+    from mpi_2d_domain_decomp_turb_particles_b200.synthetic import spectral_field
+    field = spectral_field(N_GRID, seed=1234, device=f"cuda:{dev}")
+    stream = torch.cuda.Stream(device=dev)
+
+    # ---- mixed path (the measured value) ----
+    g = _make("mixed", dev)
+    g.set_stream(stream)
+    g.set_fields(*field)
+    g.sync()
+    clk = _clock_sampler(dev) if rank == 0 else None
+    time.sleep(0.4)   # the sampler's first reading lands before the timed region
+    if ws > 1:
+        dist.barrier()
+    ms_step, kernel_ms, launches = _time_update(g, stream, args.steps, args.warmup, torch)
+    clocks = _clock_summary(clk)
+    t = torch.tensor([ms_step, kernel_ms], device=f"cuda:{dev}", dtype=torch.float64)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_step, kernel_ms = float(t[0]), float(t[1])
+    value = ws * N_PART / (ms_step * 1e-3)
+
+    # ---- full particle substep (cell lists, collision detection and statistics) ----
+    full = []
+    cand = 0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        c, _gm = g.particle_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        full.append(e0.elapsed_time(e1))
+        cand = c.candidate_pairs
+    full_ms = statistics.median(full)
+    coll_ms = g.phase_times()[2]
+
+    # ---- end to end through the C ABI with host buffers (pinned) ----
+    import numpy as np
+    host = [f.cpu().pin_memory() for f in field]
+    e2e_steps = max(1, min(args.steps, 5))
+    for _ in range(2):
+        g.set_fields(*[h.numpy() for h in host]); g.update_step(); g.mean_vel()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        g.set_fields(*[h.numpy() for h in host])    # H2D of the step's field (INTERPOLATE(v, icpt))
+        g.update_step()
+        mv = g.mean_vel()                            # D2H of the step's statistic (MEAN_VEL)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    h2d = sum(h.numel() * h.element_size() for h in host)
+    d2h = mv.nbytes
+    g.close()
+    del g
+
+    # ---- FP64 path, same workload ----
+    g64 = _make("fp64", dev)
+    g64.set_stream(stream)
+    g64.set_fields(*field)
+    g64.sync()
+    ms64, kms64, _ = _time_update(g64, stream, max(3, args.steps // 2), args.warmup, torch)
+    g64.close()
+    t64 = torch.tensor([ms64], device=f"cuda:{dev}", dtype=torch.float64)
+    if ws > 1:
+        dist.all_reduce(t64, op=dist.ReduceOp.MAX)
+    value64 = ws * N_PART / (float(t64[0]) * 1e-3)
+
+    if rank == 0:
+        peak, kind = _peaks()
+        alg = update_bytes("mixed", N_GRID, N_PART)
+        achieved = alg / (kernel_ms * 1e-3) / 1e9
+        traffic = _profile_traffic()
+        line = {
+            "metric": "particle-updates/s (256^3, 1M droplets, mixed precision)",
+            "value": value, "unit": "particle-updates/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (positions f64)", "data": "synthetic (seeded spectrum field, uniform droplets)",
+            "config": CONFIG,
+            "fp64_value": value64, "fp64_ms_per_step": float(t64[0]), "mixed_over_fp64": value / value64,
+            "full_step_ms": full_ms, "collision_ms": coll_ms,
+            "collision_candidate_pairs_per_s": cand / (coll_ms * 1e-3) if coll_ms > 0 else None,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{kind} (burst copy)",
+                         "kernel": "k_interp + k_advance_fused, per update step",
+                         "algorithmic_bytes": alg, "kernel_ms": kernel_ms},
+            "e2e": {"value": N_PART / (e2e_ms * 1e-3), "unit": "particle-updates/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "path": "dl_set_field (host FP64 field, pinned) + dl_update_step + dl_mean_vel"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "cpu_baseline": cpu_baseline(),
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _oracle_sample(npart, n, steps, min_seconds=0.0):
+    """Oracle (CPU restatement) update steps on a sample: returns (updates/s, threads)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    orc.build()
+    o = orc.Oracle(nx=n, ny=n, nz=n, npart=npart, radius_um=SETS_UM, **PHYS)
+    o.part_init()
+    rng = np.random.default_rng(7)
+    x = np.arange(n) * 2 * np.pi / n
+    f = []
+    for c in range(3):
+        a = np.zeros((n, n, n + 2))
+        a[:, :, :n] = (np.sin(x)[None, None, :] * np.cos(2 * x)[None, :, None] +
+                       np.cos(x + c)[:, None, None])
+        f.append(np.ascontiguousarray(a))
+    o.update_step(*f)
+    t = time.perf_counter()
+    done = 0
+    while done < steps or (time.perf_counter() - t) < min_seconds:
+        o.update_step(*f)
+        done += 1
+        if done >= 200:
+            break
+    dt = (time.perf_counter() - t) / done
+    return npart / dt, orc.num_threads(), dt
+
+
+def cpu_baseline():
+    npart = 200_000
+    v, th, dt = _oracle_sample(npart, N_GRID, 3, min_seconds=10.0)
+    return {"value": v, "unit": "particle-updates/s", "cores": th, "kind": "port",
+            "sample": f"{npart} droplets on the 256^3 FP64 field, >= 10 s of update steps "
+                      f"(interpolation + history + advance + position), OpenMP over droplets; {dt:.3f} s/step"}
+
+
+def run_reference(args):
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    npart = 200_000
+    for _ in range(args.warmup):
+        pass
+    v, th, dt = _oracle_sample(npart, N_GRID, args.steps)
+    line = {
+        "metric": "particle-updates/s (256^3, 1M droplets, mixed precision)", "impl": "reference",
+        "value": v, "unit": "particle-updates/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3 * N_PART / npart, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": CONFIG,
+        "cpu_baseline": {"value": v, "unit": "particle-updates/s", "cores": th, "kind": "port",
+                         "sample": f"{npart} droplets per step on the 256^3 field (FP64 CPU restatement "
+                                   f"of partlib.f90; the Fortran/MPI reference cannot be built here)"},
+        "e2e": {"value": v, "unit": "particle-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

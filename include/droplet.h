@@ -139,15 +139,19 @@ int dl_set_pertvel(dl_ctx *ctx, const double *pertvel);
 /* Sets component icpt (1..3) of the physical-space field that INTERPOLATE reads:
  * element (ix, iy, iz) (0-based) is v[ix + pitch_y*iy + pitch_z*iz]; pitch_y = llx = nx+2
  * and pitch_z = llx*lly for the reference's v(llx, lly, lz).  on_device != 0 means v is
- * a device pointer that stays valid until the next call; otherwise it is copied.  The
- * mixed path converts it to its FP32 periodic-halo copy. */
+ * a device pointer that stays valid until the next call; otherwise it is copied.  It is
+ * converted into the halo-padded copy described at dl_set_field_padded. */
 int dl_set_field(dl_ctx *ctx, int icpt, const double *v, int64_t pitch_y, int64_t pitch_z, int on_device);
-/* Mixed path only: the FP32 periodic-halo field produced on the device by a flow solver,
- * layout [3][nz+7][ny+7][dl_field_f32_pitch()] with 3 halo planes below and 4 above in
- * every direction.  Used in place of dl_set_field. */
-int dl_set_field_f32(dl_ctx *ctx, const float *dev_ptr);
-int64_t dl_field_f32_pitch(const dl_ctx *ctx);
-int64_t dl_field_f32_elems(const dl_ctx *ctx);
+/* The field as the kernels read it: a halo-padded copy in the context's precision (float
+ * for DL_MIXED, double for DL_FP64), layout [3][n+8][n+8][dl_field_padded_pitch()] with 4
+ * periodic-image planes below and above the grid in every direction; element (x, y, z)
+ * of component c is at ((c*(n+8) + z+4)*(n+8) + y+4)*pitch + x+4.  A flow solver on the
+ * same device can write this layout directly and pass it here in place of dl_set_field
+ * (no counterpart in the reference, whose INTERPOLATE builds its halo with MPI,
+ * partlib.f90:394-452).  The pointer must stay valid and 16-byte aligned. */
+int dl_set_field_padded(dl_ctx *ctx, const void *dev_ptr);
+int64_t dl_field_padded_pitch(const dl_ctx *ctx);
+int64_t dl_field_padded_elems(const dl_ctx *ctx);
 
 /* ---------------------------------------------------------------------------------------
  * The particle subroutines, in the order turb.f90:553-610 calls them
@@ -218,6 +222,14 @@ int dl_get_nei(dl_ctx *ctx, int *nei_num, int *pairs2, double *coef6, int cap, i
 /* Device timing of the phases of the last dl_particle_step (ms): interpolation+advance,
  * cell list, collision detection, HDI, periodic/relocate, overlap detection. */
 int dl_get_phase_times(dl_ctx *ctx, double *ms6);
+
+/* Runs every later call of the context on the caller's CUDA stream (a cudaStream_t passed
+ * as void*; NULL restores the context's own stream).  No reference counterpart. */
+int dl_set_stream(dl_ctx *ctx, void *stream);
+/* Device time of the interpolation+advance kernels of dl_update_step/dl_particle_step,
+ * averaged over the steps since the last reset (CUDA events on the context's stream),
+ * and the number of kernels the library launched in that span.  Synchronises. */
+int dl_timing(dl_ctx *ctx, int reset, double *avg_update_ms, int *nsteps, int64_t *kernel_launches);
 
 #ifdef __cplusplus
 }

@@ -85,9 +85,9 @@ SIGNATURES = {
     "dl_get_pertvel": (C.c_int, [_vp, _dp]),
     "dl_set_pertvel": (C.c_int, [_vp, _dp]),
     "dl_set_field": (C.c_int, [_vp, C.c_int, C.c_void_p, C.c_int64, C.c_int64, C.c_int]),
-    "dl_set_field_f32": (C.c_int, [_vp, C.c_void_p]),
-    "dl_field_f32_pitch": (C.c_int64, [_vp]),
-    "dl_field_f32_elems": (C.c_int64, [_vp]),
+    "dl_set_field_padded": (C.c_int, [_vp, C.c_void_p]),
+    "dl_field_padded_pitch": (C.c_int64, [_vp]),
+    "dl_field_padded_elems": (C.c_int64, [_vp]),
     "dl_prepare_interp": (C.c_int, [_vp]),
     "dl_get_interp_weights": (C.c_int, [_vp, _ip, _dp]),
     "dl_interpolate": (C.c_int, [_vp, C.c_int]),
@@ -115,6 +115,8 @@ SIGNATURES = {
     "dl_get_collist": (C.c_int, [_vp, _dp, C.c_int, _ip]),
     "dl_get_nei": (C.c_int, [_vp, _ip, _ip, _dp, C.c_int, _ip]),
     "dl_get_phase_times": (C.c_int, [_vp, _dp]),
+    "dl_set_stream": (C.c_int, [_vp, C.c_void_p]),
+    "dl_timing": (C.c_int, [_vp, C.c_int, _dp, _ip, C.POINTER(C.c_int64)]),
 }
 
 _lib = None

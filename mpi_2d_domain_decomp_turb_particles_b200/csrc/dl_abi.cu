@@ -310,7 +310,9 @@ extern "C" int dl_create(const dl_params *p, dl_ctx **out)
     cudaError_t e = cudaSetDevice(p->device);
     if (e != cudaSuccess) return dl_fail(c, DL_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
     DL_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->own_stream = c->stream;
     for (int i = 0; i < 8; i++) DL_CUDA(c, cudaEventCreate(&c->ev[i]));
+    for (int i = 0; i < 2 * dl_ctx::NTEV; i++) DL_CUDA(c, cudaEventCreate(&c->tev[i]));
     // defaults for capacities (single GPU: no MPI load imbalance to absorb)
     if (c->p.msize <= 0) c->p.msize = std::max(16, p->npart);
     if (c->p.ncollmax <= 0) c->p.ncollmax = std::max(100, p->npart / 100);
@@ -349,8 +351,9 @@ static int allocate_state(dl_ctx *c)
     ALLOC(c->dev_of_ref, m * 4);
     ALLOC(c->keys, m * 4);
     ALLOC(c->perm, m * 4);
-    ALLOC(c->scratch8, m * 8);
-    ALLOC(c->scratch4, m * 4);
+    // re-sort scratch: positions, radius, id (8 bytes), 3x3 + 3x3 + 3 + 3 + 3 history/state arrays
+    // (element size of the precision) and the reference index (4 bytes)
+    ALLOC(c->perm_scratch, m * (5 * 8 + 27 * c->esz + 4 + 8));
     dl_brick_dims(c->mixed, &c->bx, &c->by, &c->bz);
     const int n = c->dc.n;
     c->nbx = (n + c->bx - 1) / c->bx;
@@ -407,10 +410,11 @@ static int allocate_state(dl_ctx *c)
     ALLOC(c->ovl_cnt, sizeof(int));
     // field: FP32 halo copy
     const int64_t e = n + DL_PAD_LO + DL_PAD_HI;
-    c->f32_pitch = (e + 3) / 4 * 4;
-    c->f32_ny = e;
-    c->f32_plane = c->f32_pitch * e;
-    c->f32_comp = c->f32_plane * e;
+    c->fp_pitch = (e + 3) / 4 * 4;   // 16-byte rows in both precisions (TMA strides)
+    c->fp_plane = c->fp_pitch * e;
+    c->fp_comp = c->fp_plane * e;
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
+    if (c->num_sms <= 0) c->num_sms = 148;
     return 0;
 }
 
@@ -425,19 +429,21 @@ extern "C" int dl_destroy(dl_ctx *c)
     for (int s = 0; s < 4; s++)
         for (int k = 0; k < 3; k++) { F(c->vel[s][k]); F(c->flu[s][k]); }
     for (int k = 0; k < 3; k++) { F(c->vpv[k]); F(c->dmv[k]); F(c->pert[k]); F(c->f64_own[k]); }
-    F(c->rad); F(c->gid); F(c->ref_of_dev); F(c->dev_of_ref); F(c->keys); F(c->perm); F(c->scratch8); F(c->scratch4);
+    F(c->rad); F(c->gid); F(c->ref_of_dev); F(c->dev_of_ref); F(c->keys); F(c->perm); F(c->perm_scratch);
     F(c->long_rows); F(c->n_long);
     F(c->brick_start); F(c->brick_cnt); F(c->lhnode); F(c->bg); F(c->ghosts); F(c->d_nghost);
     F(c->ent_row); F(c->ent_ix); F(c->row_start); F(c->row_fill); F(c->row_ent); F(c->leave_nid);
     F(c->lv_blk); F(c->lv_refs); F(c->lv_old); F(c->lv_new); F(c->lv_dev); F(c->lv_dep); F(c->d_err);
     F(c->xfer64); F(c->xfer_i); F(c->hist_i); F(c->hist_d); F(c->acc_i); F(c->acc_d); F(c->out_i); F(c->out_d);
     F(c->counts); F(c->cand); F(c->pairs); F(c->contacts); F(c->remove_dev); F(c->pair_buf); F(c->pair_ibuf); F(c->mv_acc);
-    F(c->ovl_list); F(c->ovl_cnt); F(c->f32_own);
+    F(c->ovl_list); F(c->ovl_cnt); F(c->fpad_own);
     F(c->nei_cnt); F(c->nei_start); F(c->nei_idx); F(c->nei_coef); F(c->nei_coef64); F(c->overlap_flag);
     F(c->kry); F(c->xg); F(c->rg); F(c->bg64); F(c->tmp64); F(c->wv); F(c->xt); F(c->dots);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    for (int i = 0; i < 2 * dl_ctx::NTEV; i++)
+        if (c->tev[i]) cudaEventDestroy(c->tev[i]);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return 0;
 }
@@ -741,8 +747,8 @@ extern "C" int dl_set_pertvel(dl_ctx *c, const double *pertvel)
 // ---------------------------------------------------------------------------------------
 // Field
 // ---------------------------------------------------------------------------------------
-extern "C" int64_t dl_field_f32_pitch(const dl_ctx *c) { return c ? c->f32_pitch : 0; }
-extern "C" int64_t dl_field_f32_elems(const dl_ctx *c) { return c ? 3 * c->f32_comp : 0; }
+extern "C" int64_t dl_field_padded_pitch(const dl_ctx *c) { return c ? c->fp_pitch : 0; }
+extern "C" int64_t dl_field_padded_elems(const dl_ctx *c) { return c ? 3 * c->fp_comp : 0; }
 
 extern "C" int dl_set_field(dl_ctx *c, int icpt, const double *v, int64_t pitch_y, int64_t pitch_z, int on_device)
 {
@@ -766,22 +772,22 @@ extern "C" int dl_set_field(dl_ctx *c, int icpt, const double *v, int64_t pitch_
     c->fpy[k] = pitch_y;
     c->fpz[k] = pitch_z;
     c->field_set[k] = 1;
-    if (c->mixed) {
-        if (!c->f32_own) ALLOC(c->f32_own, sizeof(float) * 3 * c->f32_comp);
-        c->f32 = c->f32_own;
-        int r = launch_convert_field(c, icpt);
-        if (r) return r;
-        c->f32_valid |= 1 << k;
-    }
+    if (!c->fpad_own) ALLOC(c->fpad_own, c->esz * 3 * c->fp_comp);
+    if (c->fpad != c->fpad_own) c->fpad_valid = 0;
+    c->fpad = c->fpad_own;
+    int r = launch_convert_field(c, icpt);
+    if (r) return r;
+    c->fpad_valid |= 1 << k;
     return 0;
 }
 
-extern "C" int dl_set_field_f32(dl_ctx *c, const float *dev_ptr)
+extern "C" int dl_set_field_padded(dl_ctx *c, const void *dev_ptr)
 {
     if (!c || !dev_ptr) return DL_E_ARG;
-    if (!c->mixed) return dl_fail(c, DL_E_STATE, "dl_set_field_f32: FP64 context");
-    c->f32 = const_cast<float *>(dev_ptr);
-    c->f32_valid = 7;
+    if (!c->initialized) return dl_fail(c, DL_E_STATE, "dl_set_field_padded: call dl_part_init first");
+    if (((uintptr_t)dev_ptr & 15) != 0) return dl_fail(c, DL_E_ARG, "dl_set_field_padded: pointer not 16-byte aligned");
+    c->fpad = const_cast<void *>(dev_ptr);
+    c->fpad_valid = 7;
     return 0;
 }
 
@@ -789,7 +795,7 @@ static int need_field(dl_ctx *c, int icpt)
 {
     int lo = icpt > 0 ? icpt - 1 : 0, hi = icpt > 0 ? icpt - 1 : 2;
     for (int k = lo; k <= hi; k++) {
-        if (c->mixed ? !(c->f32_valid >> k & 1) : !c->field_set[k])
+        if (!(c->fpad_valid >> k & 1))
             return dl_fail(c, DL_E_STATE, "velocity field component not set (dl_set_field)");
     }
     return 0;
@@ -1158,6 +1164,43 @@ extern "C" int dl_get_collist(dl_ctx *c, double *collist20, int cap, int *ntotpa
     return n > cap && collist20 ? dl_fail(c, DL_E_CAPACITY, "dl_get_collist: buffer too small") : 0;
 }
 
+extern "C" int dl_set_stream(dl_ctx *c, void *stream)
+{
+    if (!c) return DL_E_ARG;
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return 0;
+}
+
+extern "C" int dl_timing(dl_ctx *c, int reset, double *avg_ms, int *nsteps, int64_t *launches)
+{
+    if (!c) return DL_E_ARG;
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    const int m = std::min(c->ntev, (int)dl_ctx::NTEV);
+    double tot = 0.0;
+    for (int i = 0; i < m; i++) {
+        float ms = 0.f;
+        DL_CUDA(c, cudaEventElapsedTime(&ms, c->tev[2 * i], c->tev[2 * i + 1]));
+        tot += ms;
+    }
+    if (avg_ms) *avg_ms = m ? tot / m : 0.0;
+    if (nsteps) *nsteps = c->ntev;
+    if (launches) *launches = c->launches;
+    if (reset) { c->ntev = 0; c->launches = 0; }
+    return 0;
+}
+
+// brackets the update kernels of one step with a pair of timing events
+static void timing_begin(dl_ctx *c)
+{
+    cudaEventRecord(c->tev[2 * (c->ntev % dl_ctx::NTEV)], c->stream);
+}
+static void timing_end(dl_ctx *c)
+{
+    cudaEventRecord(c->tev[2 * (c->ntev % dl_ctx::NTEV) + 1], c->stream);
+    c->ntev++;
+}
+
 extern "C" int dl_get_phase_times(dl_ctx *c, double *ms6)
 {
     if (!c || !ms6) return DL_E_ARG;
@@ -1241,8 +1284,10 @@ extern "C" int dl_update_step(dl_ctx *c)
     if (r) return r;
     r = maybe_resort(c);
     if (r) return r;
+    timing_begin(c);
     r = launch_interp(c, 0, 1);
     if (r) return r;
+    timing_end(c);
     c->vp_slot = c->fnew;
     c->new_particle = 0;
     c->pcur = 1 - c->pcur;
@@ -1268,8 +1313,10 @@ extern "C" int dl_particle_step(dl_ctx *c, dl_coll_report *coll, dl_gmres_report
     cudaEventRecord(c->ev[0], c->stream);
     bool fused = !hdi;
     if (fused) {
+        timing_begin(c);
         r = launch_interp(c, 0, 1);   // PREPARE_INTERP..PART_ADVANCE + position update + wrap
         if (r) return r;
+        timing_end(c);
         c->vp_slot = c->fnew;   // vp = fdp(:,0): the fused kernel wrote it into the fluid ring
         c->have_vnew = c->have_fnew = c->have_dmove = 1;
         c->new_particle = 0;

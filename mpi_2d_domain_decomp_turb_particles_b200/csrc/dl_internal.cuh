@@ -2,6 +2,7 @@
 // Reference: thenumer8or/MPI_2D_domain_decomp_turb_particles partlib.f90 (single rank).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
@@ -10,7 +11,7 @@
 #include "../../include/droplet.h"
 
 #define DL_NBIN 180
-#define DL_PAD_LO 3   // FP32 halo field: planes below the grid in every direction
+#define DL_PAD_LO 4   // halo-padded field: planes below the grid in every direction
 #define DL_PAD_HI 4   // planes above
 
 // ---------------------------------------------------------------------------------------
@@ -101,21 +102,26 @@ struct dl_ctx {
     int *brick_start;            // nbricks + 1
     int *brick_cnt;              // nbricks
     int *keys, *perm;            // per droplet
-    void *scratch8;              // permutation scratch for 8-byte arrays (msize * 8 bytes)
-    void *scratch4;              // permutation scratch for 4-byte arrays (msize * 4 bytes)
+    void *perm_scratch;          // re-sort scratch: every permuted array once (msize each)
     int steps_since_sort;
     int resort_interval;
     int sorted;
 
     // ---- velocity field ----
-    const double *f64[3];
+    // The kernels read a halo-padded copy in the context's precision, layout
+    // [3][n+8][n+8][fp_pitch] with DL_PAD_LO planes below and DL_PAD_HI above in every
+    // direction (periodic images).  dl_set_field fills it from the reference layout.
+    const double *f64[3];        // last reference-layout FP64 field (device)
     int64_t fpy[3], fpz[3];
     double *f64_own[3];
-    float *f32;                  // [3][nz+7][ny+7][pitch]
-    float *f32_own;
-    int64_t f32_pitch, f32_ny, f32_plane, f32_comp;
+    void *fpad;                  // padded field, T
+    void *fpad_own;
+    int64_t fp_pitch, fp_plane, fp_comp;   // elements
     int field_set[3];
-    int f32_valid;
+    int fpad_valid;              // bit k: component k present in fpad
+    CUtensorMap tmap;            // TMA descriptor of fpad
+    const void *tmap_base;       // fpad the descriptor was built for
+    int num_sms;
 
     // ---- PREPARE_INTERP outputs ----
     int *lhnode;                 // (nps, 3) in reference order on download
@@ -191,6 +197,11 @@ struct dl_ctx {
     // ---- timing ----
     cudaEvent_t ev[8];
     double phase_ms[6];
+    cudaStream_t own_stream;
+    static const int NTEV = 256;
+    cudaEvent_t tev[2 * NTEV];   // start/stop of the update kernels of the last NTEV steps
+    int ntev;                    // pairs recorded since the last reset
+    int64_t launches;            // kernels launched since the last reset
 };
 
 // ---------------------------------------------------------------------------------------
@@ -203,7 +214,11 @@ int dl_fail(dl_ctx *c, int code, const std::string &msg);
         if (e__ != cudaSuccess)                                                             \
             return dl_fail((ctx), DL_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)); \
     } while (0)
-#define DL_CHECK_LAUNCH(ctx) DL_CUDA(ctx, cudaGetLastError())
+#define DL_CHECK_LAUNCH(ctx)                 \
+    do {                                     \
+        (ctx)->launches++;                   \
+        DL_CUDA(ctx, cudaGetLastError());    \
+    } while (0)
 
 // ---------------------------------------------------------------------------------------
 // Kernel launchers implemented in the .cu files

@@ -19,10 +19,11 @@
 #include "dl_internal.cuh"
 
 #include <algorithm>
+#include <cudaTypedefs.h>
+#include <string>
 
 namespace {
 
-constexpr int kThreads = 256;
 
 // ---------------------------------------------------------------------------------------
 // 6-point Lagrange weights, partlib.f90:317-338 (FP64, exact source order)
@@ -61,19 +62,6 @@ __device__ __forceinline__ int wrapi(int i, int n)
 {
     int r = i % n;
     return r < 0 ? r + n : r;
-}
-
-// Ampere+ asynchronous global->shared copy of one 4- or 8-byte element (cp.async.ca).
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void *smem_dst, const void *gmem_src)
-{
-    unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem_src), "n"(BYTES) : "memory");
-}
-
-__device__ __forceinline__ void cp_async_wait_all()
-{
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 // ---------------------------------------------------------------------------------------
@@ -119,20 +107,11 @@ struct SmemLoader {
     __device__ __forceinline__ T operator()(int a, int b, int c) const { return base[c * sz + b * sy + a]; }
 };
 
-struct GlobalLoader64 {
-    const double *f;
+template <typename T>
+struct GlobalLoaderPad {
+    const T *f;   // points at padded element (x0, y0, z0) of the stencil corner
     int64_t py, pz;
-    int ix[6], iy[6], iz[6];
-    __device__ __forceinline__ double operator()(int a, int b, int c) const
-    {
-        return f[ix[a] + py * iy[b] + pz * iz[c]];
-    }
-};
-
-struct GlobalLoader32 {
-    const float *f;   // points at padded element (x0, y0, z0) of the stencil corner
-    int64_t py, pz;
-    __device__ __forceinline__ float operator()(int a, int b, int c) const { return f[a + py * b + pz * c]; }
+    __device__ __forceinline__ T operator()(int a, int b, int c) const { return f[a + py * b + pz * c]; }
 };
 
 // ---------------------------------------------------------------------------------------
@@ -144,12 +123,10 @@ struct InterpArgs {
     double dx, pi2;
     const double *px, *py, *pz;     // current positions
     const int *brick_start;
-    int nbx, nby;
-    // field
-    const double *f64[3];
-    int64_t f64py[3], f64pz[3];
-    const float *f32;               // padded FP32 field
-    int64_t f32py, f32pz, f32comp;
+    int nbx, nby, nbricks;
+    // halo-padded field (elements): x + 4 + fpy*(y + 4) + fpz*(z + 4) + fpc*c
+    const T *fpad;
+    int64_t fpy, fpz, fpc;
     int comp_lo, ncomp;             // components evaluated by this launch
     // outputs (non-fused): vp
     T *vp[3];
@@ -165,14 +142,17 @@ struct InterpArgs {
     double *qx, *qy, *qz;           // new positions (other buffer)
     const int *ref_of_dev;
     signed char *leave_nid;         // PERIODIC departure flags by reference index
+    int *err;                       // device error flags
 };
 
+// Shared-memory bank geometry of one stencil load: conflict-free groups are 32 lanes of
+// 4-byte words (FP32) or 16 lanes of 8-byte words (FP64, one half-warp per wavefront).
 template <typename T>
 struct Elems;
 template <>
 struct Elems<double> {
-    static constexpr int R = 16;      // residue modulus: 16 eight-byte words per half-warp
-    static constexpr int LANES = 16;  // lanes per conflict-free group
+    static constexpr int R = 16;
+    static constexpr int LANES = 16;
 };
 template <>
 struct Elems<float> {
@@ -180,17 +160,21 @@ struct Elems<float> {
     static constexpr int LANES = 32;
 };
 
-template <typename T, int BX, int BY, int BZ, int NCS>
-struct Tile {
-    static constexpr int EX = BX + 5, EY = BY + 5, EZ = BZ + 5;
+// Field tile of one component of one brick, as one TMA box.  Component c's box starts
+// XS*c cells lower in x and YS*c cells lower in y than component 0's, which moves the
+// three components' copies of a stencil into different banks (corner offset shift CSHIFT)
+// while keeping the TMA x coordinate 16-byte aligned.
+template <typename T, int BX, int BY, int BZ, int XS, int YS>
+struct Geo {
+    static constexpr int EX = BX + 8 + 2 * XS, EY = BY + 5 + 2 * YS, EZ = BZ + 5;
     static constexpr int PLANE = EX * EY;
     static constexpr int VOL = PLANE * EZ;
-    // component stride: >= VOL and congruent to 11 (FP32) / 5 (FP64) modulo R so that the
-    // three components of one droplet start in different banks
-    static constexpr int SHIFT = (sizeof(T) == 8) ? 5 : 11;
-    static constexpr int R = Elems<T>::R;
-    static constexpr int CS = VOL + ((SHIFT - VOL % R) % R + R) % R;
-    static constexpr int FIELD = CS * NCS;
+    static constexpr int BOX_BYTES = VOL * (int)sizeof(T);
+    static constexpr int STAGE_BYTES = (BOX_BYTES + 127) / 128 * 128;
+    static constexpr int STAGE_ELEMS = STAGE_BYTES / (int)sizeof(T);
+    static constexpr int CSHIFT = YS * EX + XS;
+    static_assert((EX * sizeof(T)) % 16 == 0, "TMA box rows must be whole 16-byte units");
+    static_assert((XS * sizeof(T)) % 16 == 0, "component x shift must keep 16-byte alignment");
 };
 
 // PERIODIC's neighbour code of a droplet that left the single pencil (partlib.f90:874-1060)
@@ -284,7 +268,6 @@ __device__ __forceinline__ void epilogue_one(const InterpArgs<T> &A, int d, cons
     double xn[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        A.fnew[c][d] = u[c];
         A.vnew[c][d] = vn[c];
         A.dmv[c][d] = dm[c];
         xn[c] = xo[c] + (double)dm[c];
@@ -296,193 +279,314 @@ __device__ __forceinline__ void epilogue_one(const InterpArgs<T> &A, int d, cons
     if (nid) A.leave_nid[A.ref_of_dev[d]] = (signed char)nid;
 }
 
-// ---------------------------------------------------------------------------------------
-// The brick kernel
-// ---------------------------------------------------------------------------------------
-template <typename T, int BX, int BY, int BZ, int NCS, int MAXD>
-__global__ void __launch_bounds__(kThreads) k_interp(InterpArgs<T> A)
+// History, advance, position update, wrap and departure flags of every droplet, with the
+// interpolated velocity read from A.vp (the fluid-velocity ring slot F[fnew]).
+template <typename T>
+__global__ void __launch_bounds__(256) k_advance_fused(InterpArgs<T> A)
 {
-    using TL = Tile<T, BX, BY, BZ, NCS>;
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= A.nps) return;
+    T u[3] = {A.vp[0][d], A.vp[1][d], A.vp[2][d]};
+    epilogue_one<T>(A, d, u);
+}
+
+// ---------------------------------------------------------------------------------------
+// mbarrier / TMA primitives (inline PTX, sm_90+)
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: gives up after ~2^22 polls (each try_wait may itself suspend briefly).
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity)
+{
+    for (int i = 0; i < (1 << 22); i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, unsigned long long *bar, int x, int y,
+                                            int z, int c)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, "
+        "%6}], [%2];\n" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z), "r"(c)
+        : "memory");
+}
+
+#define DL_DERR_TMA_TIMEOUT 2
+
+// ---------------------------------------------------------------------------------------
+// The brick kernel: persistent, warp-specialised.  The last warp is the producer: it
+// streams the field tile of every component of every (non-empty) brick of this CTA into a
+// ring of S shared-memory stages with TMA.  NG consumer groups of GW warps take the CTA's
+// bricks in turn (brick k goes to group k % NG), so one group's serial phases overlap
+// another group's stencil phase and the producer's prefetch.  Per brick a group computes
+// weights and corners, groups the (droplet, component) stencil tasks by starting bank,
+// evaluates them from shared memory, releases the stages and runs the advance epilogue.
+// ---------------------------------------------------------------------------------------
+template <typename T, int MAXD>
+struct GroupAux {
+    static constexpr int R = Elems<T>::R;
+    static constexpr int NSW = (sizeof(T) == 8) ? 18 : 3;   // FP64 weights, FP32 fractions
+    static constexpr int CAP = 64;   // tasks per bank bucket; overflow goes to the slow list
+    static constexpr size_t BYTES =
+        ((sizeof(T) * (MAXD * NSW + MAXD * 3) + sizeof(int) * (MAXD + MAXD * 3 + R + 4) +
+          sizeof(unsigned short) * (R * CAP + MAXD * 3)) + 127) / 128 * 128;
+};
+
+template <typename T, int BX, int BY, int BZ, int XS, int YS, int S, int MAXD, int NG, int GW>
+__global__ void __launch_bounds__((NG * GW + 1) * 32, 1) k_interp(const __grid_constant__ CUtensorMap tmap,
+                                                                    InterpArgs<T> A)
+{
+    using G = Geo<T, BX, BY, BZ, XS, YS>;
+    using X = GroupAux<T, MAXD>;
     constexpr int R = Elems<T>::R;
-    constexpr int NW = kThreads / 32;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *sf = reinterpret_cast<T *>(smem_raw);                      // field tile [NCS][CS]
-    T *sw = sf + TL::FIELD;                                       // weights [MAXD][18]
-    T *sv = sw + MAXD * 18;                                       // results [MAXD][3]
-    int *scorner = reinterpret_cast<int *>(sv + MAXD * 3);        // corner offset or -1
-    int *snode = scorner + MAXD;                                  // [MAXD][3] nodes (fallback)
-    int *scnt = snode + MAXD * 3;                                 // [R]
-    int *sstart = scnt + R;                                       // [R]
-    int *sfill = sstart + R;                                      // [R]
-    int *sfb = sfill + R;                                         // fallback count
-    int *sg = sfb + 1;                                            // max bucket
-    unsigned short *stask = reinterpret_cast<unsigned short *>(sg + 1);   // [MAXD*NCS]
-    unsigned short *sfbt = stask + MAXD * NCS;                             // [MAXD*NCS]
+    constexpr int NSW = X::NSW;
+    constexpr int NT = GW * 32;   // threads per consumer group
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    T *stage = reinterpret_cast<T *>(smem_raw);
+    unsigned long long *full = reinterpret_cast<unsigned long long *>(smem_raw + S * G::STAGE_BYTES);
+    unsigned long long *empty = full + S;
+    int *sabort = reinterpret_cast<int *>(empty + S);
+    unsigned char *aux0 = smem_raw + S * G::STAGE_BYTES + 128;
 
-    const int b = blockIdx.x;
-    const int bxi = b % A.nbx, byi = (b / A.nbx) % A.nby, bzi = b / (A.nbx * A.nby);
-    const int d0 = A.brick_start[b], d1 = A.brick_start[b + 1];
-    if (d0 >= d1) return;
-    const int gx0 = bxi * BX - 2, gy0 = byi * BY - 2, gz0 = bzi * BZ - 2;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int n = A.n;
+    const int ncomp = A.ncomp, clo = A.comp_lo;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        *sabort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
 
-    for (int c0 = d0; c0 < d1; c0 += MAXD) {
-        const int nd = min(MAXD, d1 - c0);
-        // ---- Phase A: nodes, weights, corners ----
-        for (int i = tid; i < nd; i += kThreads) {
-            const int d = c0 + i;
-            double pos[3] = {A.px[d], A.py[d], A.pz[d]};
-            int node[3];
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                double z;
-                node[k] = node_frac(pos[k], A.dx, &z);
-                T w[6];
-                lagrange6((T)z, w);
-#pragma unroll
-                for (int q = 0; q < 6; q++) sw[i * 18 + k * 6 + q] = w[q];
-                snode[i * 3 + k] = node[k];
-            }
-            int lx = node[0] - 2 - gx0, ly = node[1] - 2 - gy0, lz = node[2] - 2 - gz0;
-            bool in = lx >= 0 && lx < BX && ly >= 0 && ly < BY && lz >= 0 && lz < BZ;
-            scorner[i] = in ? (lz * TL::EY + ly) * TL::EX + lx : -1;
-        }
-        for (int cg = A.comp_lo; cg < A.comp_lo + A.ncomp; cg += NCS) {
-            const int ncs = min(NCS, A.comp_lo + A.ncomp - cg);
-            if (tid < R) { scnt[tid] = 0; sfill[tid] = 0; }
-            if (tid == 0) *sfb = 0;
-            // ---- stage the field region of this brick: asynchronous copies, all in flight ----
-            for (int cc = 0; cc < ncs; cc++) {
-                T *dst = sf + cc * TL::CS;
-                const int comp = cg + cc;
-                for (int e = tid; e < TL::VOL; e += kThreads) {
-                    int x = e % TL::EX, yz = e / TL::EX, y = yz % TL::EY, z = yz / TL::EY;
-                    int gx = gx0 + x, gy = gy0 + y, gz = gz0 + z;
-                    const T *src;
-                    if constexpr (sizeof(T) == 8) {
-                        gx = gx < 0 ? gx + n : (gx >= n ? gx - n : gx);
-                        gy = gy < 0 ? gy + n : (gy >= n ? gy - n : gy);
-                        gz = gz < 0 ? gz + n : (gz >= n ? gz - n : gz);
-                        src = A.f64[comp] + gx + A.f64py[comp] * gy + A.f64pz[comp] * gz;
-                    } else {
-                        // bricks that overhang the grid (n not a multiple of the brick) wrap
-                        if (gx >= n + DL_PAD_HI) gx -= n;
-                        if (gy >= n + DL_PAD_HI) gy -= n;
-                        if (gz >= n + DL_PAD_HI) gz -= n;
-                        src = A.f32 + comp * A.f32comp + (int64_t)(gx + DL_PAD_LO) + A.f32py * (gy + DL_PAD_LO) +
-                              A.f32pz * (gz + DL_PAD_LO);
+    if (warp == NG * GW) {
+        // ================= producer =================
+        if (lane == 0) {
+            int it = 0;
+            bool ok = true;
+            for (int b = blockIdx.x; b < A.nbricks && ok; b += gridDim.x) {
+                if (A.brick_start[b] == A.brick_start[b + 1]) continue;
+                const int bxi = b % A.nbx, byi = (b / A.nbx) % A.nby, bzi = b / (A.nbx * A.nby);
+                for (int cc = 0; cc < ncomp; cc++, it++) {
+                    const int s = it % S;
+                    if (it >= S && !mbar_wait(&empty[s], ((it / S) - 1) & 1)) {
+                        atomicOr(A.err, DL_DERR_TMA_TIMEOUT);
+                        *(volatile int *)sabort = 1;
+                        ok = false;
+                        break;
                     }
-                    cp_async<sizeof(T)>(dst + e, src);
+                    const int c = clo + cc;
+                    mbar_arrive_expect_tx(&full[s], (unsigned)G::BOX_BYTES);
+                    // padded coordinates of the box origin (grid origin + DL_PAD_LO)
+                    tma_load_4d(stage + s * G::STAGE_ELEMS, &tmap, &full[s], bxi * BX - XS * c,
+                                byi * BY + 2 - YS * c, bzi * BZ + 2, c);
                 }
             }
-            cp_async_wait_all();
-            __syncthreads();
-            // ---- bucket tasks by starting bank ----
-            for (int t = tid; t < nd * ncs; t += kThreads) {
-                int i = t / ncs, cc = t % ncs;
-                int cr = scorner[i];
-                if (cr >= 0) atomicAdd(&scnt[(cr + cc * TL::CS) % R], 1);
-                else sfbt[atomicAdd(sfb, 1)] = (unsigned short)t;
-            }
-            __syncthreads();
-            if (warp == 0) {
-                int v = lane < R ? scnt[lane] : 0;
-                int incl = v;
+            // wait (bounded) for the copies still in flight before leaving
+            for (int k = (it > S ? it - S : 0); k < it; k++) mbar_wait(&full[k % S], (k / S) & 1);
+        }
+        return;
+    }
+
+    // ================= consumer group gi =================
+    const int gi = warp / GW, gw = warp % GW, tid = threadIdx.x - gi * NT;
+    const int bar_id = 1 + gi;
+    unsigned char *aux = aux0 + gi * X::BYTES;
+    T *sw = reinterpret_cast<T *>(aux);                             // [MAXD][NSW]
+    T *sv = sw + MAXD * NSW;                                        // [MAXD][3] results
+    int *scorner = reinterpret_cast<int *>(sv + MAXD * 3);          // [MAXD] corner offset (comp 0) or -1
+    int *snode = scorner + MAXD;                                    // [MAXD][3]
+    int *scnt = snode + MAXD * 3;                                   // [R] tasks per bank bucket
+    int *smisc = scnt + R;                                          // [0] slow-list length
+    constexpr int CAP = X::CAP;
+    unsigned short *stask = reinterpret_cast<unsigned short *>(smisc + 4);   // [R][CAP] bucketed tasks
+    unsigned short *sfbt = stask + R * CAP;                                   // [MAXD*3] slow list
+    auto gsync = [&]() { asm volatile("bar.sync %0, %1;\n" ::"r"(bar_id), "r"(NT) : "memory"); };
+
+    if (tid < R) scnt[tid] = 0;
+    if (tid == 0) smisc[0] = 0;
+    gsync();
+    int k = 0;   // index of the brick among this CTA's non-empty bricks
+    for (int b = blockIdx.x; b < A.nbricks; b += gridDim.x) {
+        const int d0 = A.brick_start[b], d1 = A.brick_start[b + 1];
+        if (d0 == d1) continue;
+        const int mine = (k % NG) == gi;
+        const int it = k * ncomp;
+        k++;
+        if (!mine) continue;
+        const int bxi = b % A.nbx, byi = (b / A.nbx) % A.nby, bzi = b / (A.nbx * A.nby);
+        bool waited = false;
+        for (int c0 = d0; c0 < d1; c0 += MAXD) {
+            const int nd = min(MAXD, d1 - c0);
+            // ---- Phase A: nodes, weights (FP64) or fractions (FP32), corners ----
+            for (int i = tid; i < nd; i += NT) {
+                const int d = c0 + i;
+                double pos[3] = {A.px[d], A.py[d], A.pz[d]};
+                int node[3];
 #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    int y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += y;
-                }
-                int mx = v;
+                for (int q3 = 0; q3 < 3; q3++) {
+                    double z;
+                    node[q3] = node_frac(pos[q3], A.dx, &z);
+                    if constexpr (sizeof(T) == 8) {
+                        double w[6];
+                        lagrange6(z, w);
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-                if (lane < R) sstart[lane] = incl - v;
-                if (lane == 0) *sg = mx;
-            }
-            __syncthreads();
-            for (int t = tid; t < nd * ncs; t += kThreads) {
-                int i = t / ncs, cc = t % ncs;
-                int cr = scorner[i];
-                if (cr >= 0) {
-                    int r = (cr + cc * TL::CS) % R;
-                    stask[sstart[r] + atomicAdd(&sfill[r], 1)] = (unsigned short)t;
+                        for (int q = 0; q < 6; q++) sw[i * NSW + q3 * 6 + q] = w[q];
+                    } else {
+                        sw[i * NSW + q3] = (T)z;
+                    }
+                    snode[i * 3 + q3] = node[q3];
+                }
+                // stencil corner in component 0's tile (origin bxi*BX-4, byi*BY-2, bzi*BZ-2); in
+                // component c's tile the same stencil starts CSHIFT*c words further on
+                const int lx = node[0] - bxi * BX + 2, ly = node[1] - byi * BY, lz = node[2] - bzi * BZ;
+                const bool in = lx >= 0 && lx + 2 * XS + 5 < G::EX && ly >= 0 && ly < BY && lz >= 0 && lz < BZ;
+                const int cr = in ? (lz * G::EY + ly) * G::EX + lx : -1;
+                scorner[i] = cr;
+                // bucket this droplet's tasks by starting bank (stages start on 128-byte
+                // boundaries, so the bank is set by the offset alone)
+                // the slot a task gets in its bucket is the count before it: no scan needed
+                for (int cc = 0; cc < ncomp; cc++) {
+                    const int t = i * ncomp + cc;
+                    bool slow = cr < 0;
+                    if (!slow) {
+                        const int r = (cr + G::CSHIFT * (clo + cc)) % R;
+                        const int slot = atomicAdd(&scnt[r], 1);
+                        if (slot < CAP) stask[r * CAP + slot] = (unsigned short)t;
+                        else slow = true;
+                    }
+                    if (slow) sfbt[atomicAdd(&smisc[0], 1)] = (unsigned short)t;
                 }
             }
-            __syncthreads();
+            // ---- wait for this brick's tiles (once per brick) ----
+            if (!waited) {
+                for (int cc = 0; cc < ncomp; cc++) {
+                    const int q = it + cc;
+                    if (!mbar_wait(&full[q % S], (q / S) & 1)) {
+                        *(volatile int *)sabort = 1;
+                        atomicOr(A.err, DL_DERR_TMA_TIMEOUT);
+                    }
+                }
+                waited = true;
+            }
+            gsync();
+            if (*(volatile int *)sabort) return;   // uniform within the group after the barrier
             // ---- conflict-free groups: lane r of group g takes the g-th task of bucket r ----
             {
-                const int G = *sg;
-                constexpr int GPW = 32 / Elems<T>::LANES;   // groups per warp instruction
+                constexpr int GPW = 32 / Elems<T>::LANES;
                 const int sub = lane / Elems<T>::LANES, r = lane % Elems<T>::LANES;
-                for (int g = warp * GPW + sub; g < G; g += NW * GPW) {
-                    if (g < scnt[r]) {
-                        int t = stask[sstart[r] + g];
-                        int i = t / ncs, cc = t % ncs;
-                        SmemLoader<T> ld{sf + cc * TL::CS + scorner[i], TL::EX, TL::PLANE};
-                        const T *w = sw + i * 18;
+                const int mycnt = min(scnt[r], CAP);
+                int Gn = mycnt;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) Gn = max(Gn, __shfl_xor_sync(0xffffffffu, Gn, o));
+                for (int g = gw * GPW + sub; g < Gn; g += GW * GPW) {
+                    if (g < mycnt) {
+                        const int t = stask[r * CAP + g];
+                        const int i = t / ncomp, cc = t - i * ncomp;
+                        const T *base = stage + ((it + cc) % S) * G::STAGE_ELEMS + scorner[i] + G::CSHIFT * (clo + cc);
+                        SmemLoader<T> ld{base, G::EX, G::PLANE};
                         T bx[6], by[6], bz[6];
+                        if constexpr (sizeof(T) == 8) {
+                            const T *w = sw + i * NSW;
 #pragma unroll
-                        for (int q = 0; q < 6; q++) { bx[q] = w[q]; by[q] = w[6 + q]; bz[q] = w[12 + q]; }
-                        sv[i * 3 + cg + cc] = stencil(ld, bx, by, bz);
+                            for (int q = 0; q < 6; q++) { bx[q] = w[q]; by[q] = w[6 + q]; bz[q] = w[12 + q]; }
+                        } else {
+                            lagrange6(sw[i * NSW + 0], bx);
+                            lagrange6(sw[i * NSW + 1], by);
+                            lagrange6(sw[i * NSW + 2], bz);
+                        }
+                        sv[i * 3 + clo + cc] = stencil(ld, bx, by, bz);
                     }
                 }
             }
-            // ---- droplets outside the staged region: global memory, same arithmetic ----
-            for (int q = tid; q < *sfb; q += kThreads) {
-                int t = sfbt[q];
-                int i = t / ncs, cc = t % ncs, comp = cg + cc;
-                const T *w = sw + i * 18;
+            // ---- slow list: bucket overflow (shared memory, bank conflicts possible) and
+            //      droplets outside the staged tile (padded field in global memory) ----
+            for (int q = tid; q < smisc[0]; q += NT) {
+                const int t = sfbt[q];
+                const int i = t / ncomp, cc = t - i * ncomp, comp = clo + cc;
+                if (scorner[i] >= 0) {
+                    const T *base = stage + ((it + cc) % S) * G::STAGE_ELEMS + scorner[i] + G::CSHIFT * comp;
+                    SmemLoader<T> ld{base, G::EX, G::PLANE};
+                    T bx[6], by[6], bz[6];
+                    if constexpr (sizeof(T) == 8) {
+                        const T *w = sw + i * NSW;
+#pragma unroll
+                        for (int q6 = 0; q6 < 6; q6++) { bx[q6] = w[q6]; by[q6] = w[6 + q6]; bz[q6] = w[12 + q6]; }
+                    } else {
+                        lagrange6(sw[i * NSW + 0], bx);
+                        lagrange6(sw[i * NSW + 1], by);
+                        lagrange6(sw[i * NSW + 2], bz);
+                    }
+                    sv[i * 3 + comp] = stencil(ld, bx, by, bz);
+                    continue;
+                }
                 T bx[6], by[6], bz[6];
-#pragma unroll
-                for (int k = 0; k < 6; k++) { bx[k] = w[k]; by[k] = w[6 + k]; bz[k] = w[12 + k]; }
-                T r;
                 if constexpr (sizeof(T) == 8) {
-                    GlobalLoader64 ld;
-                    ld.f = A.f64[comp]; ld.py = A.f64py[comp]; ld.pz = A.f64pz[comp];
+                    const T *w = sw + i * NSW;
 #pragma unroll
-                    for (int k = 0; k < 6; k++) {
-                        ld.ix[k] = wrapi(snode[i * 3 + 0] - 2 + k, n);
-                        ld.iy[k] = wrapi(snode[i * 3 + 1] - 2 + k, n);
-                        ld.iz[k] = wrapi(snode[i * 3 + 2] - 2 + k, n);
-                    }
-                    r = stencil(ld, bx, by, bz);
+                    for (int q6 = 0; q6 < 6; q6++) { bx[q6] = w[q6]; by[q6] = w[6 + q6]; bz[q6] = w[12 + q6]; }
                 } else {
-                    GlobalLoader32 ld;
-                    int x0 = wrapi(snode[i * 3 + 0], n) - 2 + DL_PAD_LO;
-                    int y0 = wrapi(snode[i * 3 + 1], n) - 2 + DL_PAD_LO;
-                    int z0 = wrapi(snode[i * 3 + 2], n) - 2 + DL_PAD_LO;
-                    ld.f = A.f32 + comp * A.f32comp + x0 + A.f32py * y0 + A.f32pz * z0;
-                    ld.py = A.f32py; ld.pz = A.f32pz;
-                    r = stencil(ld, bx, by, bz);
+                    lagrange6(sw[i * NSW + 0], bx);
+                    lagrange6(sw[i * NSW + 1], by);
+                    lagrange6(sw[i * NSW + 2], bz);
                 }
-                sv[i * 3 + comp] = r;
+                GlobalLoaderPad<T> ld;
+                const int x0 = wrapi(snode[i * 3 + 0], n) - 2 + DL_PAD_LO;
+                const int y0 = wrapi(snode[i * 3 + 1], n) - 2 + DL_PAD_LO;
+                const int z0 = wrapi(snode[i * 3 + 2], n) - 2 + DL_PAD_LO;
+                ld.f = A.fpad + comp * A.fpc + x0 + A.fpy * y0 + A.fpz * z0;
+                ld.py = A.fpy;
+                ld.pz = A.fpz;
+                sv[i * 3 + comp] = stencil(ld, bx, by, bz);
             }
-            __syncthreads();
-        }
-        // ---- epilogue ----
-        for (int i = tid; i < nd; i += kThreads) {
-            const int d = c0 + i;
-            if (A.fused) {
-                T u[3] = {sv[i * 3 + 0], sv[i * 3 + 1], sv[i * 3 + 2]};
-                epilogue_one<T>(A, d, u);
-            } else {
-                for (int comp = A.comp_lo; comp < A.comp_lo + A.ncomp; comp++) A.vp[comp][d] = sv[i * 3 + comp];
+            gsync();
+            if (c0 + MAXD >= d1 && tid == 0) {
+                // last chunk of this brick: hand the stages back to the producer
+                for (int cc = 0; cc < ncomp; cc++) mbar_arrive(&empty[(it + cc) % S]);
             }
+            // ---- write the interpolated velocity (coalesced); reset the bucket counters ----
+            for (int i = tid; i < nd; i += NT)
+                for (int comp = clo; comp < clo + ncomp; comp++) A.vp[comp][c0 + i] = sv[i * 3 + comp];
+            if (tid < R) scnt[tid] = 0;
+            if (tid == 0) smisc[0] = 0;
+            gsync();
         }
-        __syncthreads();
     }
 }
 
-template <typename T, int BX, int BY, int BZ, int NCS, int MAXD>
-size_t interp_smem()
+template <typename T, int BX, int BY, int BZ, int XS, int YS, int S, int MAXD, int NG>
+constexpr size_t interp_smem()
 {
-    using TL = Tile<T, BX, BY, BZ, NCS>;
-    constexpr int R = Elems<T>::R;
-    size_t s = sizeof(T) * (TL::FIELD + MAXD * 18 + MAXD * 3);
-    s += sizeof(int) * (MAXD + MAXD * 3 + 3 * R + 2);
-    s += sizeof(unsigned short) * 2 * MAXD * NCS;
-    return (s + 15) & ~size_t(15);
+    using G = Geo<T, BX, BY, BZ, XS, YS>;
+    return (size_t)S * G::STAGE_BYTES + 128 + NG * GroupAux<T, MAXD>::BYTES;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -560,6 +664,32 @@ __global__ void k_gather(int nps, const int *perm, const E *in, E *out)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < nps) out[i] = in[perm[i]];
+}
+
+struct PermTable {
+    int n8, n4;
+    long long m;                         // stride of the scratch slices (msize)
+    unsigned long long *a8[40];
+    unsigned int *a4[40];
+    unsigned long long *s8;
+    unsigned int *s4;
+};
+
+__global__ void __launch_bounds__(256) k_permute_gather(int nps, const int *perm, PermTable t)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nps) return;
+    const int j = perm[i];
+    for (int a = 0; a < t.n8; a++) t.s8[a * t.m + i] = t.a8[a][j];
+    for (int a = 0; a < t.n4; a++) t.s4[a * t.m + i] = t.a4[a][j];
+}
+
+__global__ void __launch_bounds__(256) k_permute_copyback(int nps, PermTable t)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nps) return;
+    for (int a = 0; a < t.n8; a++) t.a8[a][i] = t.s8[a * t.m + i];
+    for (int a = 0; a < t.n4; a++) t.a4[a][i] = t.s4[a * t.m + i];
 }
 
 __global__ void k_inverse(int nps, const int *ref_of_dev, int *dev_of_ref)
@@ -665,9 +795,9 @@ __global__ void k_update_pos(int nps, const double *px, const double *py, const 
     qz[d] = pz[d] + (double)dz[d];
 }
 
-// FP64 field -> FP32 periodic-halo copy (mixed path)
-__global__ void k_convert_field(const double *v, int64_t py, int64_t pz, int n, float *out, int64_t opy,
-                                int64_t opz)
+// FP64 reference-layout field -> halo-padded copy in precision T (periodic images)
+template <typename T>
+__global__ void k_convert_field(const double *v, int64_t py, int64_t pz, int n, T *out, int64_t opy, int64_t opz)
 {
     const int e = n + DL_PAD_LO + DL_PAD_HI;
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -677,7 +807,7 @@ __global__ void k_convert_field(const double *v, int64_t py, int64_t pz, int n, 
     int64_t yz = i / e;
     int y = (int)(yz % e), z = (int)(yz / e);
     int gx = wrapi(x - DL_PAD_LO, n), gy = wrapi(y - DL_PAD_LO, n), gz = wrapi(z - DL_PAD_LO, n);
-    out[x + opy * y + opz * z] = (float)v[gx + py * gy + pz * gz];
+    out[x + opy * y + opz * z] = (T)v[gx + py * gy + pz * gz];
 }
 
 // MEAN_VEL partial sums (partlib.f90:1910-1930) -> 11*nset doubles via FP64 atomics.
@@ -711,8 +841,12 @@ __global__ void k_mean_vel(int nps, const T *ux, const T *uy, const T *uz, const
 }
 
 // brick configurations (cells) per precision
-constexpr int F32_BX = 16, F32_BY = 16, F32_BZ = 8, F32_NCS = 3, F32_MAXD = 256;
-constexpr int F64_BX = 12, F64_BY = 12, F64_BZ = 8, F64_NCS = 3, F64_MAXD = 192;
+// brick / pipeline configuration per precision: brick cells, component shifts (bank
+// spreading), TMA stages, droplets per chunk, consumer groups x warps per group
+constexpr int F32_BX = 16, F32_BY = 16, F32_BZ = 8, F32_XS = 0, F32_YS = 1, F32_S = 6, F32_MAXD = 256;
+constexpr int F32_NG = 2, F32_GW = 6;
+constexpr int F64_BX = 16, F64_BY = 8, F64_BZ = 4, F64_XS = 2, F64_YS = 0, F64_S = 6, F64_MAXD = 64;
+constexpr int F64_NG = 2, F64_GW = 6;
 
 template <typename T>
 T *tp(void *p) { return reinterpret_cast<T *>(p); }
@@ -744,35 +878,31 @@ int launch_brick_sort(dl_ctx *c)
     DL_CUDA(c, cudaMemsetAsync(c->brick_cnt, 0, sizeof(int) * nkeys, c->stream));
     k_brick_scatter<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, c->keys, c->brick_start, c->brick_cnt, c->perm);
     DL_CHECK_LAUNCH(c);
-    // permute every live array through a scratch buffer of the same element size (pointer swap)
-    auto perm8 = [&](void *&arr) -> int {
-        k_gather<unsigned long long><<<dl_blocks(nps, t), t, 0, c->stream>>>(
-            nps, c->perm, (const unsigned long long *)arr, (unsigned long long *)c->scratch8);
-        std::swap(arr, c->scratch8);
-        return 0;
-    };
-    auto perm4 = [&](void *&arr) -> int {
-        k_gather<unsigned int><<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, c->perm, (const unsigned int *)arr,
-                                                                       (unsigned int *)c->scratch4);
-        std::swap(arr, c->scratch4);
-        return 0;
-    };
-    auto permT = [&](void *&arr) { return c->mixed ? perm4(arr) : perm8(arr); };
+    // permute every live array in two passes: gather all of them into the scratch region,
+    // then copy back (coalesced); one index load per droplet for ~30 arrays
+    PermTable tb;
+    memset(&tb, 0, sizeof(tb));
+    auto add8 = [&](void *a) { tb.a8[tb.n8++] = (unsigned long long *)a; };
+    auto add4 = [&](void *a) { tb.a4[tb.n4++] = (unsigned int *)a; };
+    auto addT = [&](void *a) { if (c->mixed) add4(a); else add8(a); };
     for (int k = 0; k < 3; k++) {
-        void *p = c->pos[c->pcur][k];
-        perm8(p);
-        c->pos[c->pcur][k] = (double *)p;
-        for (int l = 0; l < 3; l++) permT(c->vel[(c->vcur + l) % 4][k]);
-        for (int l = 0; l < 3; l++) permT(c->flu[(c->fcur + l) % 4][k]);
-        permT(c->vpv[k]);
-        permT(c->dmv[k]);
-        if (c->pert[k]) permT(c->pert[k]);
+        add8(c->pos[c->pcur][k]);
+        for (int l = 0; l < 3; l++) addT(c->vel[(c->vcur + l) % 4][k]);
+        for (int l = 0; l < 3; l++) addT(c->flu[(c->fcur + l) % 4][k]);
+        addT(c->vpv[k]);
+        addT(c->dmv[k]);
+        if (c->pert[k]) addT(c->pert[k]);
     }
-    {
-        void *p = c->rad; perm8(p); c->rad = (double *)p;
-        p = c->gid; perm8(p); c->gid = (double *)p;
-        p = c->ref_of_dev; perm4(p); c->ref_of_dev = (int *)p;
-    }
+    add8(c->rad);
+    add8(c->gid);
+    add4(c->ref_of_dev);
+    tb.s8 = (unsigned long long *)c->perm_scratch;
+    tb.s4 = (unsigned int *)((unsigned long long *)c->perm_scratch + (size_t)tb.n8 * c->msize);
+    tb.m = c->msize;
+    k_permute_gather<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, c->perm, tb);
+    DL_CHECK_LAUNCH(c);
+    k_permute_copyback<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, tb);
+    DL_CHECK_LAUNCH(c);
     if (c->has_dead) {
         int live = 0;
         DL_CUDA(c, cudaMemcpyAsync(&live, c->brick_start + c->nbricks, sizeof(int), cudaMemcpyDeviceToHost,
@@ -787,9 +917,41 @@ int launch_brick_sort(dl_ctx *c)
     return 0;
 }
 
-template <typename T, int BX, int BY, int BZ, int NCS, int MAXD>
+// TMA descriptor of the halo-padded field: 4D (x, y, z, component), box = one component tile
+static int make_tmap(dl_ctx *c, int box_x, int box_y, int box_z)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        DL_CUDA(c, cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess)
+            return dl_fail(c, DL_E_CUDA, "cuTensorMapEncodeTiled not available");
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    const cuuint64_t e = (cuuint64_t)c->dc.n + DL_PAD_LO + DL_PAD_HI;
+    const cuuint64_t es = c->esz;
+    cuuint64_t dims[4] = {(cuuint64_t)c->fp_pitch, e, e, 3};
+    cuuint64_t strides[3] = {(cuuint64_t)c->fp_pitch * es, (cuuint64_t)c->fp_plane * es, (cuuint64_t)c->fp_comp * es};
+    cuuint32_t box[4] = {(cuuint32_t)box_x, (cuuint32_t)box_y, (cuuint32_t)box_z, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = encode(&c->tmap, c->mixed ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
+                        c->fpad, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return dl_fail(c, DL_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    c->tmap_base = c->fpad;
+    return 0;
+}
+
+template <typename T, int BX, int BY, int BZ, int XS, int YS, int S, int MAXD, int NG, int GW>
 static int launch_interp_t(dl_ctx *c, int comp_lo, int ncomp, int fused)
 {
+    using G = Geo<T, BX, BY, BZ, XS, YS>;
+    if (c->tmap_base != c->fpad) {
+        int r = make_tmap(c, G::EX, G::EY, G::EZ);
+        if (r) return r;
+    }
     InterpArgs<T> A;
     memset(&A, 0, sizeof(A));
     A.n = c->dc.n;
@@ -798,20 +960,18 @@ static int launch_interp_t(dl_ctx *c, int comp_lo, int ncomp, int fused)
     A.pi2 = c->dc.pi2;
     A.px = c->pos[c->pcur][0]; A.py = c->pos[c->pcur][1]; A.pz = c->pos[c->pcur][2];
     A.brick_start = c->brick_start;
-    A.nbx = c->nbx; A.nby = c->nby;
-    for (int k = 0; k < 3; k++) {
-        A.f64[k] = c->f64[k];
-        A.f64py[k] = c->fpy[k];
-        A.f64pz[k] = c->fpz[k];
-        A.vp[k] = tp<T>(c->vpv[k]);
-    }
-    A.f32 = c->f32;
-    A.f32py = c->f32_pitch;
-    A.f32pz = c->f32_plane;
-    A.f32comp = c->f32_comp;
+    A.nbx = c->nbx; A.nby = c->nby; A.nbricks = c->nbricks;
+    A.fpad = tp<T>(c->fpad);
+    A.fpy = c->fp_pitch;
+    A.fpz = c->fp_plane;
+    A.fpc = c->fp_comp;
+    for (int k = 0; k < 3; k++) A.vp[k] = tp<T>(c->vpv[k]);
+    if (fused)   // the interpolated velocity goes straight into fdp(:,0) = F[fnew]
+        for (int k = 0; k < 3; k++) A.vp[k] = tp<T>(c->flu[(c->fcur + 3) % 4][k]);
     A.comp_lo = comp_lo;
     A.ncomp = ncomp;
     A.fused = fused;
+    A.err = c->d_err;
     if (fused) {
         A.first = c->new_particle;
         A.init_mode = c->p.init_velocity;
@@ -835,11 +995,17 @@ static int launch_interp_t(dl_ctx *c, int comp_lo, int ncomp, int fused)
         A.ref_of_dev = c->ref_of_dev;
         A.leave_nid = c->leave_nid;
     }
-    size_t sm = interp_smem<T, BX, BY, BZ, NCS, MAXD>();
-    auto kern = k_interp<T, BX, BY, BZ, NCS, MAXD>;
+    constexpr size_t sm = interp_smem<T, BX, BY, BZ, XS, YS, S, MAXD, NG>();
+    static_assert(sm <= 227 * 1024, "shared memory budget");
+    auto kern = k_interp<T, BX, BY, BZ, XS, YS, S, MAXD, NG, GW>;
     DL_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    kern<<<c->nbricks, kThreads, sm, c->stream>>>(A);
+    const int grid = std::min(c->nbricks, c->num_sms);
+    kern<<<grid, (NG * GW + 1) * 32, sm, c->stream>>>(c->tmap, A);
     DL_CHECK_LAUNCH(c);
+    if (fused) {
+        k_advance_fused<T><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(A);
+        DL_CHECK_LAUNCH(c);
+    }
     return 0;
 }
 
@@ -847,8 +1013,11 @@ int launch_interp(dl_ctx *c, int icpt, int fused)
 {
     if (c->nps == 0) return 0;
     int lo = icpt > 0 ? icpt - 1 : 0, nc = icpt > 0 ? 1 : 3;
-    if (c->mixed) return launch_interp_t<float, F32_BX, F32_BY, F32_BZ, F32_NCS, F32_MAXD>(c, lo, nc, fused);
-    return launch_interp_t<double, F64_BX, F64_BY, F64_BZ, F64_NCS, F64_MAXD>(c, lo, nc, fused);
+    if (c->mixed)
+        return launch_interp_t<float, F32_BX, F32_BY, F32_BZ, F32_XS, F32_YS, F32_S, F32_MAXD, F32_NG, F32_GW>(
+            c, lo, nc, fused);
+    return launch_interp_t<double, F64_BX, F64_BY, F64_BZ, F64_XS, F64_YS, F64_S, F64_MAXD, F64_NG, F64_GW>(
+        c, lo, nc, fused);
 }
 
 void dl_brick_dims(int mixed, int *bx, int *by, int *bz)
@@ -965,10 +1134,16 @@ int launch_convert_field(dl_ctx *c, int icpt)
 {
     const int n = c->dc.n, e = n + DL_PAD_LO + DL_PAD_HI;
     int64_t tot = (int64_t)e * e * e;
-    float *out = c->f32 + (int64_t)(icpt - 1) * c->f32_comp;
-    k_convert_field<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(c->f64[icpt - 1], c->fpy[icpt - 1],
-                                                                          c->fpz[icpt - 1], n, out, c->f32_pitch,
-                                                                          c->f32_plane);
+    const unsigned blocks = (unsigned)((tot + 255) / 256);
+    const int k = icpt - 1;
+    if (c->mixed)
+        k_convert_field<float><<<blocks, 256, 0, c->stream>>>(c->f64[k], c->fpy[k], c->fpz[k], n,
+                                                              (float *)c->fpad + (int64_t)k * c->fp_comp,
+                                                              c->fp_pitch, c->fp_plane);
+    else
+        k_convert_field<double><<<blocks, 256, 0, c->stream>>>(c->f64[k], c->fpy[k], c->fpz[k], n,
+                                                               (double *)c->fpad + (int64_t)k * c->fp_comp,
+                                                               c->fp_pitch, c->fp_plane);
     DL_CHECK_LAUNCH(c);
     return 0;
 }

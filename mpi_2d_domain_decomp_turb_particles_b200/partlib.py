@@ -195,16 +195,17 @@ class Partlib:
         for k, v in enumerate((vx, vy, vz)):
             self.set_field(k + 1, v)
 
-    def set_field_f32(self, t):
-        """Mixed path: a CUDA float32 tensor in the padded layout of ``field_f32_shape``."""
-        assert t.is_cuda and t.element_size() == 4 and t.is_contiguous()
+    def set_field_padded(self, t):
+        """A CUDA tensor in the halo-padded layout of ``field_padded_shape`` (float32 for the
+        mixed path, float64 for FP64), e.g. written by the on-device flow solver."""
+        assert t.is_cuda and t.is_contiguous()
+        assert t.element_size() == (4 if self.params.precision == "mixed" else 8)
         self._fields[0] = t
-        self._chk(self.lib.dl_set_field_f32(self.h, C.c_void_p(t.data_ptr())))
+        self._chk(self.lib.dl_set_field_padded(self.h, C.c_void_p(t.data_ptr())))
 
-    def field_f32_shape(self):
-        n = self.params.nx
-        e = n + 7
-        return (3, e, e, int(self.lib.dl_field_f32_pitch(self.h)))
+    def field_padded_shape(self):
+        e = self.params.nx + 8
+        return (3, e, e, int(self.lib.dl_field_padded_pitch(self.h)))
 
     # -- subroutines (turb.f90:553-610 order) --------------------------------------------
     def prepare_interp(self):
@@ -335,6 +336,17 @@ class Partlib:
         out = np.zeros((n.value, 20))
         self._chk(self.lib.dl_get_collist(self.h, _dptr(out), n.value, C.byref(n)))
         return out
+
+    def set_stream(self, stream):
+        """Run on a torch.cuda.Stream (or raw cudaStream_t int); None restores the own stream."""
+        h = None if stream is None else int(getattr(stream, "cuda_stream", stream))
+        self._chk(self.lib.dl_set_stream(self.h, C.c_void_p(h) if h else None))
+
+    def timing(self, reset: bool = True):
+        """(average device ms of the update kernels per step, steps, kernel launches)."""
+        ms, n, l = C.c_double(0), C.c_int(0), C.c_int64(0)
+        self._chk(self.lib.dl_timing(self.h, int(reset), C.byref(ms), C.byref(n), C.byref(l)))
+        return ms.value, n.value, l.value
 
     def phase_times(self) -> np.ndarray:
         out = np.zeros(6)
