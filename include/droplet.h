@@ -231,6 +231,23 @@ int dl_set_stream(dl_ctx *ctx, void *stream);
  * and the number of kernels the library launched in that span.  Synchronises. */
 int dl_timing(dl_ctx *ctx, int reset, double *avg_update_ms, int *nsteps, int64_t *kernel_launches);
 
+/* ---------------------------------------------------------------------------------------
+ * Allocation-free entry point (no counterpart in the reference)
+ * ------------------------------------------------------------------------------------- */
+/* The PERIODIC reorder permutation (partlib.f90:866-1133, single rank) for callers that
+ * cannot allocate device memory inside their time loop: a host code that runs on a fixed
+ * device-memory budget it manages itself, or a loop that must not take the implicit device
+ * synchronisation of cudaMalloc/cudaFree.  No context and no allocation: y and z are the
+ * device arrays yp(2,:) and yp(3,:) (reference order, after UPDATE_PART_POSITION and before
+ * the wrap); new_of_old (device, n ints) receives the new reference index of every droplet
+ * (0-based).  Scratch is a fixed 1.3 MB file-scope device array shared by every call: at
+ * most 2^26 droplets and 2^17 departing droplets per call (DL_E_ARG / DL_E_CAPACITY beyond,
+ * with new_of_old left as the identity in the latter case).  Calls that overlap on the GPU
+ * race on the shared scratch.  The first call on a device looks up the scratch address
+ * (cudaGetSymbolAddress) and should come before any stream capture on that device.
+ * Runs on `stream` (a cudaStream_t, NULL = default stream) and synchronises it. */
+int dl_periodic_order_noalloc(const double *y, const double *z, int n, int *new_of_old, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -117,6 +117,7 @@ SIGNATURES = {
     "dl_get_phase_times": (C.c_int, [_vp, _dp]),
     "dl_set_stream": (C.c_int, [_vp, C.c_void_p]),
     "dl_timing": (C.c_int, [_vp, C.c_int, _dp, _ip, C.POINTER(C.c_int64)]),
+    "dl_periodic_order_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None
