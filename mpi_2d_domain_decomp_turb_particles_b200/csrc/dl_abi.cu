@@ -345,6 +345,10 @@ static int allocate_state(dl_ctx *c)
         ALLOC(c->dmv[k], m * es);
         if (c->dc.hdi) ALLOC(c->pert[k], m * es);
     }
+    if (c->dc.hdi) {
+        ALLOC(c->pert_tmp, 3 * m * es);
+        ALLOC(c->lv_src, m * 4);
+    }
     ALLOC(c->rad, m * 8);
     ALLOC(c->gid, m * 8);
     ALLOC(c->ref_of_dev, m * 4);
@@ -368,6 +372,8 @@ static int allocate_state(dl_ctx *c)
     c->gcap = std::max(4096, (int)std::min<size_t>(m, (size_t)1 << 30));
     ALLOC(c->ghosts, sizeof(Ghost) * c->gcap);
     ALLOC(c->d_nghost, sizeof(int));
+    ALLOC(c->gh_blk, sizeof(int) * (8 * (m / 1024 + 1) + 8));
+    ALLOC(c->gh_start, sizeof(int) * (8 * (m / 1024 + 1) + 8));
     ALLOC(c->ent_row, sizeof(int) * (m + c->gcap));
     ALLOC(c->ent_ix, sizeof(int) * (m + c->gcap));
     c->nrows = c->dc.nyh * c->dc.nzh;
@@ -431,7 +437,7 @@ extern "C" int dl_destroy(dl_ctx *c)
     for (int k = 0; k < 3; k++) { F(c->vpv[k]); F(c->dmv[k]); F(c->pert[k]); F(c->f64_own[k]); }
     F(c->rad); F(c->gid); F(c->ref_of_dev); F(c->dev_of_ref); F(c->keys); F(c->perm); F(c->perm_scratch);
     F(c->long_rows); F(c->n_long);
-    F(c->brick_start); F(c->brick_cnt); F(c->lhnode); F(c->bg); F(c->ghosts); F(c->d_nghost);
+    F(c->brick_start); F(c->brick_cnt); F(c->lhnode); F(c->bg); F(c->ghosts); F(c->d_nghost); F(c->gh_blk); F(c->gh_start); F(c->pert_tmp); F(c->lv_src);
     F(c->ent_row); F(c->ent_ix); F(c->row_start); F(c->row_fill); F(c->row_ent); F(c->leave_nid);
     F(c->lv_blk); F(c->lv_refs); F(c->lv_old); F(c->lv_new); F(c->lv_dev); F(c->lv_dep); F(c->d_err);
     F(c->xfer64); F(c->xfer_i); F(c->hist_i); F(c->hist_d); F(c->acc_i); F(c->acc_d); F(c->out_i); F(c->out_d);
@@ -439,6 +445,7 @@ extern "C" int dl_destroy(dl_ctx *c)
     F(c->ovl_list); F(c->ovl_cnt); F(c->fpad_own);
     F(c->nei_cnt); F(c->nei_start); F(c->nei_idx); F(c->nei_coef); F(c->nei_coef64); F(c->overlap_flag);
     F(c->kry); F(c->xg); F(c->rg); F(c->bg64); F(c->tmp64); F(c->wv); F(c->xt); F(c->dots);
+    F(c->nei_fill); F(c->nei_blk); F(c->nei_key); F(c->rf32);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     for (int i = 0; i < 2 * dl_ctx::NTEV; i++)
@@ -1234,6 +1241,14 @@ extern "C" int dl_coalesce(dl_ctx *c)
     std::vector<int> dev_of_ref(n);
     DL_CUDA(c, cudaStreamSynchronize(c->stream));
     DL_CUDA(c, cudaMemcpy(dev_of_ref.data(), c->dev_of_ref, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    // pertvel stays at its reference index (COALESCE moves yp, vp, dmove, fvp, fdp only,
+    // partlib.f90:3676-3728)
+    std::vector<double> pert_by_ref;
+    if (c->pert[0]) {
+        pert_by_ref.resize((size_t)3 * n);
+        int rp = c->mixed ? pert_io_t<float>(c, pert_by_ref.data(), 0) : pert_io_t<double>(c, pert_by_ref.data(), 0);
+        if (rp) return rp;
+    }
     std::vector<int> slot(dev_of_ref);   // reference position -> device droplet (mutated by swaps)
     std::map<int, double> setrad;        // device droplet -> new radius (or -1 = deleted)
     int jj = 0;
@@ -1264,6 +1279,10 @@ extern "C" int dl_coalesce(dl_ctx *c)
     r = launch_brick_sort(c);
     if (r) return r;
     c->nps = newn;
+    if (c->pert[0]) {
+        r = c->mixed ? pert_io_t<float>(c, pert_by_ref.data(), 1) : pert_io_t<double>(c, pert_by_ref.data(), 1);
+        if (r) return r;
+    }
     return 0;
 }
 
@@ -1331,11 +1350,13 @@ extern "C" int dl_particle_step(dl_ctx *c, dl_coll_report *coll, dl_gmres_report
     r = launch_headlist(c, hdi ? c->sc.d_hdi : c->sc.d_coll);
     if (r) return r;
     cudaEventRecord(c->ev[2], c->stream);
+    int warn = 0;
     if (hdi) {
         r = launch_nei_list(c);
         if (r) return r;
         r = run_gmres(c, gm);
         if (r < 0) return r;
+        warn = r;   // GMRES not converged: the reference prints and carries on
         r = dl_part_history_fdp(c);
         if (r) return r;
         r = dl_part_advance(c);
@@ -1385,5 +1406,5 @@ extern "C" int dl_particle_step(dl_ctx *c, dl_coll_report *coll, dl_gmres_report
     c->phase_ms[5] = elapsed(c, 5, 6);
     c->time += c->dc.dt;
     c->steps_since_sort++;
-    return 0;
+    return warn;
 }

@@ -58,33 +58,85 @@ __device__ __forceinline__ int row_of(const DevConst &D, int iy, int iz)
 }
 
 // ---------------------------------------------------------------------------------------
-// Ghosts, partlib.f90:2211-2351 (single rank: every shift applies)
+// Ghosts, partlib.f90:2211-2394 (single rank: every shift applies).  The ghost array is
+// built in the reference's ypn order: slot jid = 1..8, inside a slot ascending source
+// reference index, so ghost g has ypn index nps + g + 1.  Threads run over reference
+// indices; one count pass per 1024 references, a scan over (slot, block), one scatter.
 // ---------------------------------------------------------------------------------------
-__global__ void k_ghosts(DevConst D, int nps, const double *py, const double *pz, double dist, Ghost *g, int cap,
-                         int *cnt)
+__device__ __forceinline__ unsigned ghost_tags(const DevConst &D, double y, double z, double dist)
 {
-    int d = blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= nps) return;
-    double y = py[d], z = pz[d];
-    double d_e = fabs(1.0 * D.hy - y);
-    double d_w = fabs(0.0 * D.hy - y);
-    double d_n = fabs(1.0 * D.hz - z);
-    double d_s = fabs(0.0 * D.hz - z);
-    bool tag[8];
-    tag[0] = d_e <= dist;
-    tag[1] = sqrt(d_e * d_e + d_n * d_n) <= dist;
-    tag[2] = d_n <= dist;
-    tag[3] = sqrt(d_w * d_w + d_n * d_n) <= dist;
-    tag[4] = d_w <= dist;
-    tag[5] = sqrt(d_w * d_w + d_s * d_s) <= dist;
-    tag[6] = d_s <= dist;
-    tag[7] = sqrt(d_e * d_e + d_s * d_s) <= dist;
-    const double p = D.pi2;
+    const double d_e = fabs(1.0 * D.hy - y);
+    const double d_w = fabs(0.0 * D.hy - y);
+    const double d_n = fabs(1.0 * D.hz - z);
+    const double d_s = fabs(0.0 * D.hz - z);
+    unsigned t = 0;
+    t |= (unsigned)(d_e <= dist) << 0;
+    t |= (unsigned)(sqrt(d_e * d_e + d_n * d_n) <= dist) << 1;
+    t |= (unsigned)(d_n <= dist) << 2;
+    t |= (unsigned)(sqrt(d_w * d_w + d_n * d_n) <= dist) << 3;
+    t |= (unsigned)(d_w <= dist) << 4;
+    t |= (unsigned)(sqrt(d_w * d_w + d_s * d_s) <= dist) << 5;
+    t |= (unsigned)(d_s <= dist) << 6;
+    t |= (unsigned)(sqrt(d_e * d_e + d_s * d_s) <= dist) << 7;
+    return t;
+}
+
+// per (slot, block of 1024 references) ghost counts, slot-major
+__global__ void __launch_bounds__(1024) k_ghost_count(DevConst D, int nps, const int *dev_of_ref, const double *py,
+                                                      const double *pz, double dist, int nblk, int *cnt)
+{
+    const int r = blockIdx.x * 1024 + threadIdx.x;
+    unsigned t = 0;
+    if (r < nps) {
+        const int d = dev_of_ref[r];
+        t = ghost_tags(D, py[d], pz[d], dist);
+    }
     for (int k = 0; k < 8; k++) {
-        if (!tag[k]) continue;
+        const int n = __syncthreads_count((t >> k) & 1u);
+        if (threadIdx.x == 0) cnt[k * nblk + blockIdx.x] = n;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_ghost_scatter(DevConst D, int nps, const int *dev_of_ref, const double *py,
+                                                        const double *pz, double dist, int nblk, const int *start,
+                                                        Ghost *g, int cap)
+{
+    __shared__ int woff[8][32];
+    const int r = blockIdx.x * 1024 + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned t = 0;
+    int d = 0;
+    double y = 0.0, z = 0.0;
+    if (r < nps) {
+        d = dev_of_ref[r];
+        y = py[d];
+        z = pz[d];
+        t = ghost_tags(D, y, z, dist);
+    }
+    unsigned bal[8];
+    for (int k = 0; k < 8; k++) {
+        bal[k] = __ballot_sync(0xffffffffu, (t >> k) & 1u);
+        if (lane == 0) woff[k][w] = __popc(bal[k]);
+    }
+    __syncthreads();
+    if (w < 8) {   // warp w scans the per-warp counts of slot w
+        const int v = woff[w][lane];
+        int incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int q = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += q;
+        }
+        __syncwarp();
+        woff[w][lane] = incl - v;
+    }
+    __syncthreads();
+    if (!t) return;
+    const double p = D.pi2;
+    const unsigned below = (1u << lane) - 1u;
+    for (int k = 0; k < 8; k++) {
+        if (!((t >> k) & 1u)) continue;
         Ghost gh;
         gh.y = y; gh.z = z; gh.src = d; gh.jid = k + 1;
-        switch (k + 1) {
+        switch (k + 1) {   // shifts applied by the sender, partlib.f90:2231-2348
         case 1: gh.y = y - p; break;
         case 2: gh.y = y - p; gh.z = z - p; break;
         case 3: gh.z = z - p; break;
@@ -94,7 +146,7 @@ __global__ void k_ghosts(DevConst D, int nps, const double *py, const double *pz
         case 7: gh.z = z + p; break;
         case 8: gh.y = y - p; gh.z = z + p; break;
         }
-        int s = atomicAdd(cnt, 1);
+        const int s = start[k * nblk + blockIdx.x] + woff[k][w] + __popc(bal[k] & below);
         if (s < cap) g[s] = gh;
     }
 }
@@ -579,9 +631,26 @@ __global__ void __launch_bounds__(1024) k_lv_compact(int n, const signed char *n
     if (f) refs[off[blockIdx.x] + wsum[w] + __popc(m & ((1u << lane) - 1))] = i;
 }
 
+// The HDI disturbance velocity pertvel is indexed by reference position and PERIODIC does
+// not move it with the droplets (partlib.f90:866-1133 moves yp, fvp, fdp only), so the
+// value at reference index R stays at R: pt[] (three components, element size pesz, or
+// none) is permuted against the droplets through ptmp / src_dev.
+template <typename E>
+__device__ void keep_by_reference(int m, const int *src_dev, const int *dev_tmp, E *p0, E *p1, E *p2, E *tmp,
+                                  bool gather)
+{
+    E *p[3] = {p0, p1, p2};
+    for (int j = threadIdx.x; j < m; j += blockDim.x)
+        for (int c = 0; c < 3; c++) {
+            if (gather) tmp[(int64_t)c * m + j] = p[c][src_dev[j]];
+            else p[c][dev_tmp[j]] = tmp[(int64_t)c * m + j];
+        }
+}
+
 __global__ void __launch_bounds__(1024) k_lv_reorder(int n, const int *ktot, const int *P, signed char *nid,
                                                      int *dep, int *old_ref, int *new_ref, int *dev_tmp,
-                                                     int *ref_of_dev, int *dev_of_ref, int *err)
+                                                     int *ref_of_dev, int *dev_of_ref, int *err, void *pt0,
+                                                     void *pt1, void *pt2, int pesz, void *ptmp, int *src_dev)
 {
     __shared__ int s_m, s_k;
     if (threadIdx.x == 0) {
@@ -618,13 +687,31 @@ __global__ void __launch_bounds__(1024) k_lv_reorder(int n, const int *ktot, con
     }
     __syncthreads();
     const int m = s_m, k = s_k;
-    for (int j = threadIdx.x; j < m; j += blockDim.x) dev_tmp[j] = dev_of_ref[old_ref[j]];
+    for (int j = threadIdx.x; j < m; j += blockDim.x) {
+        dev_tmp[j] = dev_of_ref[old_ref[j]];
+        if (pesz) src_dev[j] = dev_of_ref[new_ref[j]];   // device that holds reference new_ref[j] now
+    }
     __syncthreads();
+    if (pesz == 8)
+        keep_by_reference<unsigned long long>(m, src_dev, dev_tmp, (unsigned long long *)pt0,
+                                              (unsigned long long *)pt1, (unsigned long long *)pt2,
+                                              (unsigned long long *)ptmp, true);
+    else if (pesz == 4)
+        keep_by_reference<unsigned>(m, src_dev, dev_tmp, (unsigned *)pt0, (unsigned *)pt1, (unsigned *)pt2,
+                                    (unsigned *)ptmp, true);
     for (int j = threadIdx.x; j < m; j += blockDim.x) {
         ref_of_dev[dev_tmp[j]] = new_ref[j];
         dev_of_ref[new_ref[j]] = dev_tmp[j];
     }
     for (int j = threadIdx.x; j < k; j += blockDim.x) nid[P[j]] = 0;
+    __syncthreads();
+    if (pesz == 8)
+        keep_by_reference<unsigned long long>(m, src_dev, dev_tmp, (unsigned long long *)pt0,
+                                              (unsigned long long *)pt1, (unsigned long long *)pt2,
+                                              (unsigned long long *)ptmp, false);
+    else if (pesz == 4)
+        keep_by_reference<unsigned>(m, src_dev, dev_tmp, (unsigned *)pt0, (unsigned *)pt1, (unsigned *)pt2,
+                                    (unsigned *)ptmp, false);
 }
 
 // new reference indices for a set of droplets (old ref -> new ref, both 0-based)
@@ -659,14 +746,20 @@ int launch_headlist(dl_ctx *c, double dist)
     const DevConst &D = c->dc;
     const int nps = c->nps, t = 256;
     const double *P[3] = {c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2]};
-    DL_CUDA(c, cudaMemsetAsync(c->d_nghost, 0, sizeof(int), c->stream));
-    if (nps > 0) {
-        k_ghosts<<<dl_blocks(nps, t), t, 0, c->stream>>>(D, nps, P[1], P[2], dist, c->ghosts, c->gcap, c->d_nghost);
-        DL_CHECK_LAUNCH(c);
-    }
     int ng = 0;
-    DL_CUDA(c, cudaMemcpyAsync(&ng, c->d_nghost, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->nei_valid = 0;   // the neighbour lists index this cell list
+    if (nps > 0) {
+        const int nblk = dl_blocks(nps, 1024);
+        k_ghost_count<<<nblk, 1024, 0, c->stream>>>(D, nps, c->dev_of_ref, P[1], P[2], dist, nblk, c->gh_blk);
+        DL_CHECK_LAUNCH(c);
+        int r = dl_scan(c, c->gh_blk, c->gh_start, 8 * nblk);
+        if (r) return r;
+        k_ghost_scatter<<<nblk, 1024, 0, c->stream>>>(D, nps, c->dev_of_ref, P[1], P[2], dist, nblk, c->gh_start,
+                                                      c->ghosts, c->gcap);
+        DL_CHECK_LAUNCH(c);
+        DL_CUDA(c, cudaMemcpyAsync(&ng, c->gh_start + 8 * nblk, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
     if (ng > c->gcap) return dl_fail(c, DL_E_CAPACITY, "HEADLIST: halo droplet capacity exceeded");
     c->nghost = ng;
     const int ne = nps + ng;
@@ -862,8 +955,10 @@ int launch_periodic_reorder(dl_ctx *c)
     if (r) return r;
     k_lv_compact<<<nblk, 1024, 0, c->stream>>>(n, c->leave_nid, c->lv_blk, c->lv_refs);
     DL_CHECK_LAUNCH(c);
+    const int pesz = c->pert[0] ? (int)c->esz : 0;
     k_lv_reorder<<<1, 1024, 0, c->stream>>>(n, c->lv_blk + nblk, c->lv_refs, c->leave_nid, c->lv_dep, c->lv_old,
-                                            c->lv_new, c->lv_dev, c->ref_of_dev, c->dev_of_ref, c->d_err);
+                                            c->lv_new, c->lv_dev, c->ref_of_dev, c->dev_of_ref, c->d_err,
+                                            c->pert[0], c->pert[1], c->pert[2], pesz, c->pert_tmp, c->lv_src);
     DL_CHECK_LAUNCH(c);
     return 0;
 }

@@ -1,32 +1,958 @@
 // Hydrodynamic interaction: NEI_LIST_PRECOMP (partlib.f90:3218-3371), AFUN_PRECOMP
-// (3375-3510) and HDI_GMRES (2795-3005).
+// (3375-3510), EUC_NORM (2756-2791) and HDI_GMRES (2795-3005), single rank.
+//
+// Neighbour lists.  The reference walks, for every owned droplet ih1, the linked cell
+// lists of the (2 nx_max + 1)(2 ny_max + 1)(2 nz_max + 1) cells around it, visits the
+// droplets ih2 > ih1 (ypn order) and appends a Stokes-disturbance tensor to ih1's list
+// (partner radius) and, for an owned ih2, to ih2's list (own radius).  Here one thread per
+// owned droplet walks the row-sorted cell list twice (count, then fill into a CSR over
+// the device order) and each owner's entries are then sorted by a key that reproduces
+// the reference's append order:
+//   entries appended while an earlier ih1 was processed come first, by that ih1;
+//   then the owner's own walk: cell loop order (i, j, k), inside a cell descending ypn
+//   index (the head/list chain order).
+// The coefficients are computed in FP64 with the reference's operation order, so the
+// lists are bit-identical to the reference's (ghost partners are stored as their source
+// droplet, which is what AFUN_PRECOMP reads through ypn(16:18)).
+//
+// GMRES.  The Krylov vectors live in the device order, planar (x | y | z), as the
+// reference's x(1:3*nps).  Modified Gram-Schmidt runs as one kernel per projection, each
+// applying the previous projection and computing the next dot product (deterministic
+// two-stage reductions); the (maxiter+1) x maxiter Hessenberg least-squares update with
+// Givens rotations, the residual estimate and the tolerance schedule run on the host,
+// as in the reference.  Precision:
+//   FP64 context: the reference algorithm in FP64 (maxerr 1e-6, relaxed x10 at
+//     iteration 25 and at each iteration from 48, warm start pertvel).
+//   mixed context: FP32 Krylov vectors, FP32 tensors and FP32 accumulation for the
+//     iterations, wrapped in FP64 residual refinement: r = b - (I + N) x with FP64
+//     tensors and FP64 x, an FP32 GMRES solve for the correction, x += d, until the FP64
+//     relative residual ||b - (I + N) x|| / ||b|| is below 1e-6.
 #include "dl_internal.cuh"
 
-int launch_nei_list(dl_ctx *c)
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace {
+
+template <typename T>
+T *tp(void *p) { return reinterpret_cast<T *>(p); }
+
+constexpr int kMaxIter = 50;            // partlib.f90:2813
+constexpr double kMaxErr = 1.0e-6;      // partlib.f90:2814
+constexpr double kSmallRhs = 1.0e-5;    // partlib.f90:2853-2856: nothing to solve
+constexpr int kMaxRefine = 4;           // FP64 refinement sweeps of the mixed solve
+constexpr int kRedGrid = 296;           // reduction grid: 2 CTAs per SM
+constexpr int kRedThreads = 256;
+
+// ---------------------------------------------------------------------------------------
+// Cell walk (same cell formulas as the collision search, partlib.f90:3241-3260)
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void nei_cell(const DevConst &D, double x, double y, double z, int &ix, int &iy, int &iz)
 {
-    return dl_fail(c, DL_E_STATE, "NEI_LIST_PRECOMP: not available in this build");
+    ix = 1 + (int)(x / D.hx * (double)D.ncd);
+    iy = 1 + (int)((y - 0.0 * D.hy) / D.hy * (double)D.ncd);
+    iz = 1 + (int)((z - 0.0 * D.hz) / D.hz * (double)D.ncd);
+    if (ix > D.ncd) ix = D.ncd;
+    if (iy > D.ncd) iy = D.ncd;
+    if (iz > D.ncd) iz = D.ncd;
 }
 
-int run_gmres(dl_ctx *c, dl_gmres_report *)
+__device__ __forceinline__ int nei_row(const DevConst &D, int iy, int iz)
 {
-    return dl_fail(c, DL_E_STATE, "HDI_GMRES: not available in this build");
+    return (iz - (1 - D.nz_max)) * D.nyh + (iy - (1 - D.ny_max));
+}
+
+__device__ __forceinline__ int first_ix(const long long *re, int s, int e, int key)
+{
+    const long long k = (long long)key << 32;
+    while (s < e) {
+        const int m = (s + e) >> 1;
+        if (re[m] < k) s = m + 1;
+        else e = m;
+    }
+    return s;
+}
+
+// Stokes disturbance tensor of a sphere of radius arad at separation xd (partlib.f90:3318-3331)
+__device__ __forceinline__ void stokes_tensor(double arad, double dnij, const double *xd, double *c6)
+{
+    double fact1 = arad / dnij;
+    const double fact2 = fact1 * fact1 * fact1;
+    fact1 = 0.75 * fact1;
+    const double gamma = (fact1 - 0.75 * fact2) / (dnij * dnij);
+    const double beta = fact1 + 0.25 * fact2;
+    c6[0] = gamma * (xd[0] * xd[0]) + beta;
+    c6[1] = gamma * xd[0] * xd[1];
+    c6[2] = gamma * xd[0] * xd[2];
+    c6[3] = gamma * (xd[1] * xd[1]) + beta;
+    c6[4] = gamma * xd[1] * xd[2];
+    c6[5] = gamma * (xd[2] * xd[2]) + beta;
+}
+
+struct NeiArgs {
+    DevConst D;
+    int nps;
+    const double *px, *py, *pz, *rad;
+    const int *ref;
+    const Ghost *g;
+    const int *row_start;
+    const long long *row_ent;
+    int *cnt;                     // count pass: entries per owner
+    const int *start;             // fill pass: CSR offsets
+    int *fill;                    // fill pass: per-owner cursors
+    int *partner;                 // device index of the partner (its source droplet for ghosts)
+    unsigned long long *key;      // append-order key
+    double *coef;                 // 6 FP64 coefficients per entry
+    int *flag;                    // [0] overlapping owner + 1, [1] fill overflow
+};
+
+template <bool FILL>
+__device__ __forceinline__ void nei_emit(const NeiArgs &A, int owner, int partner, unsigned long long key,
+                                         double arad, double dnij, const double *xd)
+{
+    if (!FILL) {
+        atomicAdd(&A.cnt[owner], 1);
+        return;
+    }
+    const int slot = A.start[owner] + atomicAdd(&A.fill[owner], 1);
+    if (slot >= A.start[owner + 1]) {   // the count pass saw fewer: never expected
+        A.flag[1] = 1;
+        return;
+    }
+    A.partner[slot] = partner;
+    A.key[slot] = key;
+    stokes_tensor(arad, dnij, xd, A.coef + (int64_t)slot * 6);
+}
+
+template <bool FILL>
+__global__ void __launch_bounds__(128) k_nei_walk(NeiArgs A)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= A.nps) return;
+    const DevConst &D = A.D;
+    const double xa[3] = {A.px[a], A.py[a], A.pz[a]};
+    const double ra = A.rad[a];
+    const int refa = A.ref[a];
+    int ix, iy, iz;
+    nei_cell(D, xa[0], xa[1], xa[2], ix, iy, iz);
+    const int jlo = max(iy - D.ny_max, 1 - D.ny_max), jhi = min(iy + D.ny_max, D.ncd + D.ny_max);
+    const int klo = max(iz - D.nz_max, 1 - D.nz_max), khi = min(iz + D.nz_max, D.ncd + D.nz_max);
+    const int nj = 2 * D.ny_max + 1, nk = 2 * D.nz_max + 1;
+    const int lo_raw = ix - D.nx_max, hi_raw = ix + D.nx_max;
+    // x ranges: [lo, hi] of cell indices ii with the shift sx and the unwrapped i = ii + ish
+    int rlo[3], rhi[3], ish[3];
+    double rsx[3];
+    int nr = 0;
+    rlo[nr] = max(1, lo_raw); rhi[nr] = min(D.ncd, hi_raw); rsx[nr] = 0.0; ish[nr] = 0; nr++;
+    if (lo_raw < 1) { rlo[nr] = lo_raw + D.ncd; rhi[nr] = D.ncd; rsx[nr] = -1.0; ish[nr] = -D.ncd; nr++; }
+    if (hi_raw > D.ncd) { rlo[nr] = 1; rhi[nr] = hi_raw - D.ncd; rsx[nr] = 1.0; ish[nr] = D.ncd; nr++; }
+    const double trunc = D.hdi_trunc;
+    for (int j = jlo; j <= jhi; j++) {
+        for (int k = klo; k <= khi; k++) {
+            const int row = nei_row(D, j, k);
+            const int rs = A.row_start[row], re = A.row_start[row + 1];
+            if (rs == re) continue;
+            const int jrel = j - (iy - D.ny_max), krel = k - (iz - D.nz_max);
+            for (int q = 0; q < nr; q++) {
+                for (int s = first_ix(A.row_ent, rs, re, rlo[q]); s < re; s++) {
+                    const long long ke = A.row_ent[s];
+                    const int ix2 = (int)(ke >> 32);
+                    if (ix2 > rhi[q]) break;
+                    const int e = (int)(ke & 0xffffffffLL);
+                    int src, ypn2;
+                    double xb[3];
+                    bool ghost = e >= A.nps;
+                    if (!ghost) {
+                        src = e;
+                        if (A.ref[src] <= refa) continue;   // ih2 <= ih1
+                        ypn2 = A.ref[src] + 1;
+                        xb[1] = A.py[src];
+                        xb[2] = A.pz[src];
+                    } else {
+                        const Ghost &gh = A.g[e - A.nps];
+                        src = gh.src;
+                        ypn2 = e + 1;                     // ghosts are stored in ypn order
+                        xb[1] = gh.y;
+                        xb[2] = gh.z;
+                    }
+                    xb[0] = A.px[src] + rsx[q] * D.hx;
+                    double xd[3] = {xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2]};
+                    const double dnij = sqrt(xd[0] * xd[0] + xd[1] * xd[1] + xd[2] * xd[2]);
+                    const double rb = A.rad[src];
+                    if (dnij < ra + rb) {                 // partlib.f90:3294-3299
+                        atomicCAS(&A.flag[0], 0, a + 1);
+                        continue;
+                    }
+                    if (dnij < trunc * rb) {
+                        const int irel = ix2 + ish[q] - lo_raw;
+                        const unsigned cell = (unsigned)((irel * nj + jrel) * nk + krel);
+                        const unsigned long long key = (1ull << 62) | ((unsigned long long)cell << 32) |
+                                                       (unsigned long long)(0xffffffffu - (unsigned)ypn2);
+                        nei_emit<FILL>(A, a, src, key, rb, dnij, xd);
+                    }
+                    if (!ghost && dnij < trunc * ra) {
+                        const double nxd[3] = {-xd[0], -xd[1], -xd[2]};
+                        nei_emit<FILL>(A, src, a, (unsigned long long)(refa + 1), ra, dnij, nxd);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Append order inside each owner's segment (segments hold at most nei_max entries)
+__global__ void k_nei_sort(int nps, const int *start, unsigned long long *key, int *partner, double *coef)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nps) return;
+    const int s = start[a], e = start[a + 1];
+    for (int i = s + 1; i < e; i++) {
+        const unsigned long long kv = key[i];
+        const int pv = partner[i];
+        double cv[6];
+        for (int t = 0; t < 6; t++) cv[t] = coef[(int64_t)i * 6 + t];
+        int j = i - 1;
+        while (j >= s && key[j] > kv) {
+            key[j + 1] = key[j];
+            partner[j + 1] = partner[j];
+            for (int t = 0; t < 6; t++) coef[(int64_t)(j + 1) * 6 + t] = coef[(int64_t)j * 6 + t];
+            j--;
+        }
+        key[j + 1] = kv;
+        partner[j + 1] = pv;
+        for (int t = 0; t < 6; t++) coef[(int64_t)(j + 1) * 6 + t] = cv[t];
+    }
+}
+
+__global__ void k_coef_to_f32(int64_t n, const double *c, float *o)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) o[i] = (float)c[i];
+}
+
+// multi-block exclusive scan of per-owner counts: block sums (+ the largest count) ...
+__global__ void __launch_bounds__(1024) k_cnt_blocksum(int n, const int *cnt, int *bsum, int *maxcnt)
+{
+    __shared__ int ws[32];
+    const int i = blockIdx.x * 1024 + threadIdx.x;
+    const int v = i < n ? cnt[i] : 0;
+    int s = v, m = v;
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+    }
+    if ((threadIdx.x & 31) == 0) { ws[threadIdx.x >> 5] = s; atomicMax(maxcnt, m); }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int t = ws[threadIdx.x];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (threadIdx.x == 0) bsum[blockIdx.x] = t;
+    }
+}
+
+// ... then the in-block scan plus the block offset
+__global__ void __launch_bounds__(1024) k_cnt_apply(int n, const int *cnt, const int *boff, int nblk, int *start)
+{
+    __shared__ int ws[32];
+    const int i = blockIdx.x * 1024 + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int v = i < n ? cnt[i] : 0;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) ws[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        const int a = ws[lane];
+        int ai = a;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, ai, o);
+            if (lane >= o) ai += t;
+        }
+        ws[lane] = ai - a;
+    }
+    __syncthreads();
+    if (i < n) start[i] = boff[blockIdx.x] + ws[w] + incl - v;
+    if (blockIdx.x == 0 && threadIdx.x == 0) start[n] = boff[nblk];
+}
+
+// ---------------------------------------------------------------------------------------
+// AFUN_PRECOMP (partlib.f90:3466-3497): Ax = x + sum_j N_ij x_j, and b = sum_j N_ij (V_j - U_j)
+// ---------------------------------------------------------------------------------------
+template <typename T, typename C>
+__global__ void k_afun(int nps, const int *start, const int *partner, const C *coef, const T *x, int64_t ld, T *ax)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nps) return;
+    T r0 = (T)0, r1 = (T)0, r2 = (T)0;
+    const int e1 = start[a + 1];
+    for (int e = start[a]; e < e1; e++) {
+        const int p = partner[e];
+        const T x1 = x[p], x2 = x[ld + p], x3 = x[2 * ld + p];
+        const C *n = coef + (int64_t)e * 6;
+        const T n2 = (T)n[0], n3 = (T)n[1], n4 = (T)n[2], n5 = (T)n[3], n6 = (T)n[4], n7 = (T)n[5];
+        r0 = r0 + n2 * x1 + n3 * x2 + n4 * x3;
+        r1 = r1 + n3 * x1 + n5 * x2 + n6 * x3;
+        r2 = r2 + n4 * x1 + n6 * x2 + n7 * x3;
+    }
+    ax[a] = r0 + x[a];
+    ax[ld + a] = r1 + x[ld + a];
+    ax[2 * ld + a] = r2 + x[2 * ld + a];
+}
+
+template <typename V>
+__global__ void k_afun_rhs(int nps, const int *start, const int *partner, const double *coef, const V *vx,
+                           const V *vy, const V *vz, const V *ux, const V *uy, const V *uz, int64_t ld, double *b)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nps) return;
+    double b0 = 0.0, b1 = 0.0, b2 = 0.0;
+    const int e1 = start[a + 1];
+    for (int e = start[a]; e < e1; e++) {
+        const int p = partner[e];
+        const double w1 = (double)vx[p] - (double)ux[p];
+        const double w2 = (double)vy[p] - (double)uy[p];
+        const double w3 = (double)vz[p] - (double)uz[p];
+        const double *n = coef + (int64_t)e * 6;
+        b0 = b0 + n[0] * w1 + n[1] * w2 + n[2] * w3;
+        b1 = b1 + n[1] * w1 + n[3] * w2 + n[4] * w3;
+        b2 = b2 + n[2] * w1 + n[4] * w2 + n[5] * w3;
+    }
+    b[a] = b0;
+    b[ld + a] = b1;
+    b[2 * ld + a] = b2;
+}
+
+// ---------------------------------------------------------------------------------------
+// Vector kernels.  Reductions: fixed grid, per-thread strided partial sums in T, block
+// tree, then the last CTA to finish sums the CTA partials in order -> deterministic.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T *sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    v = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : (T)0;
+    if (w == 0)
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    return v;   // valid in thread 0
+}
+
+template <typename T>
+__device__ __forceinline__ void finish_reduction(T part, T *partials, T *out, unsigned *ticket, T *sh)
+{
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = part;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    T v = (T)0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) v += __ldcg(partials + i);
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) {
+        *out = v;
+        *ticket = 0u;
+    }
+}
+
+// One modified Gram-Schmidt step (partlib.f90:2870-2880): v -= h_prev * q_prev (when
+// q_prev is given, h_prev read from device memory), then out = <q_next, v>, or <v, v> when
+// q_next is null.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_mgs(int64_t n, T *v, const T *q_prev, const T *h_prev,
+                                                      const T *q_next, T *out, T *partials, unsigned *ticket)
+{
+    __shared__ T sh[32];
+    const T h = q_prev ? *h_prev : (T)0;
+    T s = (T)0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        T vi = v[i];
+        if (q_prev) {
+            vi = vi - h * q_prev[i];
+            v[i] = vi;
+        }
+        s += q_next ? q_next[i] * vi : vi * vi;
+    }
+    s = block_sum(s, sh);
+    finish_reduction(s, partials, out, ticket, sh);
+}
+
+// ||x||^2 of a vector in its own precision (EUC_NORM without the root)
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_sumsq(int64_t n, const T *x, T *out, T *partials, unsigned *ticket)
+{
+    __shared__ T sh[32];
+    T s = (T)0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        s += x[i] * x[i];
+    s = block_sum(s, sh);
+    finish_reduction(s, partials, out, ticket, sh);
+}
+
+template <typename T>
+__global__ void k_scale_div(int64_t n, const T *v, const T *h, T *q)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) q[i] = v[i] / *h;
+}
+
+template <typename T>
+__global__ void k_sub(int64_t n, const double *b, const T *ax, T *r)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] = (T)b[i] - ax[i];
+}
+
+// x = x0 + Q y (partlib.f90:2946-2950); x0 null = 0; accumulates in A
+template <typename T, typename A>
+__global__ void k_xupdate(int64_t n, int iters, const T *Q, int64_t qld, const double *y, const A *x0, A *x)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    A acc = (A)0;
+    for (int j = 0; j < iters; j++) acc = acc + (A)Q[(int64_t)j * qld + i] * (A)y[j];
+    x[i] = (x0 ? x0[i] : (A)0) + acc;
+}
+
+// FP64 residual of the mixed solve: r = b - ((I + N) x) with FP64 tensors; also r in FP32
+__global__ void k_residual64(int nps, const int *start, const int *partner, const double *coef, const double *x,
+                             int64_t ld, const double *b, double *r, float *rf)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nps) return;
+    double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+    const int e1 = start[a + 1];
+    for (int e = start[a]; e < e1; e++) {
+        const int p = partner[e];
+        const double x1 = x[p], x2 = x[ld + p], x3 = x[2 * ld + p];
+        const double *n = coef + (int64_t)e * 6;
+        r0 = r0 + n[0] * x1 + n[1] * x2 + n[2] * x3;
+        r1 = r1 + n[1] * x1 + n[3] * x2 + n[4] * x3;
+        r2 = r2 + n[2] * x1 + n[4] * x2 + n[5] * x3;
+    }
+    const double q0 = b[a] - (r0 + x[a]);
+    const double q1 = b[ld + a] - (r1 + x[ld + a]);
+    const double q2 = b[2 * ld + a] - (r2 + x[2 * ld + a]);
+    r[a] = q0; r[ld + a] = q1; r[2 * ld + a] = q2;
+    rf[a] = (float)q0; rf[ld + a] = (float)q1; rf[2 * ld + a] = (float)q2;
+}
+
+template <typename S, typename D>
+__global__ void k_copy3(int nps, const S *s0, const S *s1, const S *s2, int64_t ld, D *d)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nps) return;
+    d[a] = (D)s0[a];
+    d[ld + a] = (D)s1[a];
+    d[2 * ld + a] = (D)s2[a];
+}
+
+template <typename S, typename D>
+__global__ void k_uncopy3(int nps, const S *s, int64_t ld, D *d0, D *d1, D *d2)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nps) return;
+    d0[a] = (D)s[a];
+    d1[a] = (D)s[ld + a];
+    d2[a] = (D)s[2 * ld + a];
+}
+
+// ---------------------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------------------
+int grow(dl_ctx *c, void **p, size_t bytes, size_t *have)
+{
+    if (bytes <= *have && *p) return 0;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *have = 0;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return dl_fail(c, DL_E_ALLOC, std::string("HDI buffers: ") + cudaGetErrorString(e));
+    *have = bytes;
+    return 0;
+}
+
+// The Krylov space, the reduction scratch and the FP64 vectors (allocated on first use).
+int gmres_buffers(dl_ctx *c)
+{
+    const size_t v3 = 3 * (size_t)c->msize;
+    int r = grow(c, &c->kry, (size_t)(kMaxIter + 1) * v3 * c->esz, &c->hdi_kry_bytes);
+    if (r) return r;
+    if (!c->wv) {
+        void *p = nullptr;
+        if (cudaMalloc(&c->wv, v3 * c->esz) != cudaSuccess || cudaMalloc(&c->xt, v3 * c->esz) != cudaSuccess ||
+            cudaMalloc(&c->xg, v3 * 8) != cudaSuccess || cudaMalloc(&c->rg, v3 * 8) != cudaSuccess ||
+            cudaMalloc(&c->bg64, v3 * 8) != cudaSuccess ||
+            cudaMalloc(&c->tmp64, std::max(v3, (size_t)(kMaxIter + 8)) * 8) != cudaSuccess ||
+            cudaMalloc(&p, v3 * 4) != cudaSuccess ||
+            cudaMalloc(&c->dots, sizeof(double) * (kRedGrid + 2 * (kMaxIter + 4)) + 64) != cudaSuccess)
+            return dl_fail(c, DL_E_ALLOC, "HDI_GMRES: cudaMalloc failed");
+        c->rf32 = (float *)p;
+        DL_CUDA(c, cudaMemset(c->dots, 0, sizeof(double) * (kRedGrid + 2 * (kMaxIter + 4)) + 64));
+    }
+    return 0;
+}
+
+// Device scratch inside c->dots: [0, kRedGrid) partials, then h[kMaxIter + 2], then a
+// scalar slot, then the ticket (all in units of double so both precisions fit).
+template <typename T>
+struct Red {
+    T *partials, *h, *scalar;
+    unsigned *ticket;
+};
+template <typename T>
+Red<T> red_of(dl_ctx *c)
+{
+    Red<T> r;
+    double *base = c->dots;
+    r.partials = reinterpret_cast<T *>(base);
+    r.h = reinterpret_cast<T *>(base + kRedGrid);
+    r.scalar = reinterpret_cast<T *>(base + kRedGrid + kMaxIter + 2);
+    r.ticket = reinterpret_cast<unsigned *>(base + kRedGrid + kMaxIter + 3);
+    return r;
+}
+
+template <typename T>
+int sumsq(dl_ctx *c, const T *x, int64_t n, double *out)
+{
+    Red<T> R = red_of<T>(c);
+    k_sumsq<T><<<kRedGrid, kRedThreads, 0, c->stream>>>(n, x, R.scalar, R.partials, R.ticket);
+    DL_CHECK_LAUNCH(c);
+    T v;
+    DL_CUDA(c, cudaMemcpyAsync(&v, R.scalar, sizeof(T), cudaMemcpyDeviceToHost, c->stream));
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    *out = (double)v;
+    return 0;
+}
+
+template <typename T, typename C>
+int afun(dl_ctx *c, const C *coef, const T *x, T *ax)
+{
+    k_afun<T, C><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(c->nps, c->nei_start, c->nei_idx, coef, x,
+                                                                 (int64_t)c->nps, ax);
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}
+
+struct GmresResult {
+    int iters = 0;
+    double res = 0.0;
+    bool converged = false;
+    std::vector<double> y;
+};
+
+// The GMRES iteration of partlib.f90:2858-2976 on Krylov vectors of type T.  On entry Q0
+// holds the initial residual (not normalised) and norm_rhs its norm; norm_b scales the
+// residual estimate.  stop_abs > 0 also ends the iteration once the estimate falls
+// below it (the FP32 inner solve of the mixed path).
+template <typename T, typename C>
+int gmres_iterate(dl_ctx *c, const C *coef, double norm_b, double norm_rhs, double stop_abs, GmresResult &out)
+{
+    const int64_t n3 = 3 * (int64_t)c->nps;
+    const int64_t qld = 3 * (int64_t)c->msize;
+    T *Q = tp<T>(c->kry);
+    T *v = tp<T>(c->wv);
+    Red<T> R = red_of<T>(c);
+    const int M1 = kMaxIter + 1;
+    std::vector<double> H((size_t)M1 * kMaxIter, 0.0), Rn((size_t)M1 * M1, 0.0), Qn((size_t)M1 * M1, 0.0);
+    std::vector<double> bn(M1, 0.0), y(kMaxIter, 0.0), v1(M1, 0.0), v2(M1, 0.0), resv(M1, 0.0);
+    auto HH = [&](int r, int col) -> double & { return H[(size_t)(col - 1) * M1 + (r - 1)]; };
+    auto RN = [&](int r, int col) -> double & { return Rn[(size_t)(col - 1) * M1 + (r - 1)]; };
+    auto QN = [&](int r, int col) -> double & { return Qn[(size_t)(col - 1) * M1 + (r - 1)]; };
+    const int tb = 256;
+    const int nb = (int)((n3 + tb - 1) / tb);
+    // Q0 = r0 / norm_rhs
+    {
+        const T nr = (T)norm_rhs;
+        DL_CUDA(c, cudaMemcpyAsync(R.scalar, &nr, sizeof(T), cudaMemcpyHostToDevice, c->stream));
+        k_scale_div<T><<<nb, tb, 0, c->stream>>>(n3, Q, R.scalar, Q);
+        DL_CHECK_LAUNCH(c);
+    }
+    double maxerr = kMaxErr, res = 0.0;
+    int iter;
+    bool converged = false;
+    std::vector<T> hcol(kMaxIter + 2);
+    for (iter = 1; iter <= kMaxIter; iter++) {
+        int r = afun<T, C>(c, coef, Q + (int64_t)(iter - 1) * qld, v);
+        if (r) return r;
+        // modified Gram-Schmidt: h_j = <q_j, v>; v -= h_j q_j (j = 1..iter), then ||v||
+        for (int j = 1; j <= iter + 1; j++) {
+            const T *qprev = j > 1 ? Q + (int64_t)(j - 2) * qld : nullptr;
+            const T *hprev = j > 1 ? R.h + (j - 2) : nullptr;
+            const T *qnext = j <= iter ? Q + (int64_t)(j - 1) * qld : nullptr;
+            k_mgs<T><<<kRedGrid, kRedThreads, 0, c->stream>>>(n3, v, qprev, hprev, qnext, R.h + (j - 1), R.partials,
+                                                              R.ticket);
+            DL_CHECK_LAUNCH(c);
+        }
+        DL_CUDA(c, cudaMemcpyAsync(hcol.data(), R.h, sizeof(T) * (iter + 1), cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaStreamSynchronize(c->stream));
+        for (int j = 1; j <= iter; j++) HH(j, iter) = (double)hcol[j - 1];
+        HH(iter + 1, iter) = std::sqrt((double)hcol[iter]);
+        // q_{iter+1} = v / H(iter+1, iter)
+        {
+            const T hn = (T)HH(iter + 1, iter);
+            DL_CUDA(c, cudaMemcpyAsync(R.scalar, &hn, sizeof(T), cudaMemcpyHostToDevice, c->stream));
+            k_scale_div<T><<<nb, tb, 0, c->stream>>>(n3, v, R.scalar, Q + (int64_t)iter * qld);
+            DL_CHECK_LAUNCH(c);
+        }
+        // Givens update of the least-squares problem (partlib.f90:2888-2944)
+        if (iter == 1) {
+            const double nrm = std::sqrt(HH(1, 1) * HH(1, 1) + HH(2, 1) * HH(2, 1));
+            const double q1a = HH(1, 1) / nrm, q1b = HH(2, 1) / nrm;
+            QN(1, 1) = q1a; QN(2, 1) = q1b;
+            QN(1, 2) = q1b; QN(2, 2) = -q1a;
+            RN(1, 1) = std::sqrt(HH(1, 1) * HH(1, 1) + HH(2, 1) * HH(2, 1));
+            bn[0] = q1a * norm_rhs;
+            y[0] = bn[0] / RN(1, 1);
+        } else {
+            for (int i = 1; i <= iter; i++) {
+                double acc = 0.0;
+                for (int j = 1; j <= iter; j++) acc = acc + QN(i, j) * HH(j, iter);
+                RN(i, iter) = acc;
+            }
+            const double aa = RN(iter, iter), bb = HH(iter + 1, iter);
+            const double dd = std::sqrt(aa * aa + bb * bb);
+            const double cc = aa / dd, ss = bb / dd;
+            RN(iter, iter) = dd;
+            for (int j = 1; j <= iter; j++) {
+                v1[j - 1] = cc * QN(iter, j);
+                v2[j - 1] = -ss * QN(iter, j);
+            }
+            v1[iter] = ss;
+            v2[iter] = cc;
+            for (int j = 1; j <= iter + 1; j++) {
+                QN(iter, j) = v1[j - 1];
+                QN(iter + 1, j) = v2[j - 1];
+            }
+            bn[iter - 2] = QN(iter - 1, 1) * norm_rhs;
+            bn[iter - 1] = QN(iter, 1) * norm_rhs;
+            y[iter - 1] = bn[iter - 1] / RN(iter, iter);
+            for (int i = iter - 1; i >= 1; i--) {
+                double d = 0.0;
+                for (int j = i + 1; j <= iter; j++) d = d + y[j - 1] * RN(i, j);
+                y[i - 1] = (bn[i - 1] - d) / RN(i, i);
+            }
+        }
+        // residual estimate (partlib.f90:2958-2964)
+        for (int i = 1; i <= iter + 1; i++) {
+            double acc = 0.0;
+            for (int j = 1; j <= iter; j++) acc = acc + HH(i, j) * y[j - 1];
+            resv[i - 1] = acc;
+        }
+        resv[0] = resv[0] - norm_rhs;
+        double xc = 0.0;
+        for (int i = 0; i <= iter; i++) xc = xc + resv[i] * resv[i];
+        res = std::sqrt(xc) / norm_b;
+        out.iters = iter;
+        if (res < maxerr || (stop_abs > 0.0 && std::sqrt(xc) < stop_abs)) {
+            converged = true;
+            break;
+        }
+        if (iter == kMaxIter / 2) maxerr = maxerr * 10;
+        if (iter >= kMaxIter - 2) maxerr = maxerr * 10;
+    }
+    out.res = res;
+    out.converged = converged || !(res > maxerr);
+    out.y.assign(y.begin(), y.begin() + out.iters);
+    return 0;
+}
+
+template <typename T>
+int x_update(dl_ctx *c, const GmresResult &g, const double *x0, double *x)
+{
+    const int64_t n3 = 3 * (int64_t)c->nps;
+    if (g.iters == 0) return 0;
+    double *yd = c->tmp64;   // the solution coefficients (a few doubles) at the head of tmp64
+    DL_CUDA(c, cudaMemcpyAsync(yd, g.y.data(), sizeof(double) * g.iters, cudaMemcpyHostToDevice, c->stream));
+    k_xupdate<T, double><<<(int)((n3 + 255) / 256), 256, 0, c->stream>>>(n3, g.iters, tp<T>(c->kry),
+                                                                         3 * (int64_t)c->msize, yd, x0, x);
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}
+
+// HDI_GMRES of an FP64 context: the reference algorithm, Krylov vectors in FP64.
+int gmres_fp64(dl_ctx *c, dl_gmres_report *rep)
+{
+    const int nps = c->nps;
+    const int64_t ld = nps, n3 = 3 * (int64_t)nps;
+    const int bs = dl_blocks(nps, 256);
+    double *x0 = c->xg, *b = c->bg64, *ax = c->rg;
+    double *Q0 = tp<double>(c->kry);
+    // x0 = pertvel, b = AFUN(icall = 1), r0 = b - A x0 (partlib.f90:2842-2852)
+    k_copy3<double, double><<<bs, 256, 0, c->stream>>>(nps, tp<double>(c->pert[0]), tp<double>(c->pert[1]),
+                                                       tp<double>(c->pert[2]), ld, x0);
+    DL_CHECK_LAUNCH(c);
+    const int vs = c->vcur;
+    k_afun_rhs<double><<<bs, 256, 0, c->stream>>>(nps, c->nei_start, c->nei_idx, c->nei_coef64,
+                                                  tp<double>(c->vel[vs][0]), tp<double>(c->vel[vs][1]),
+                                                  tp<double>(c->vel[vs][2]), tp<double>(dl_vp_ptr(c, 0)),
+                                                  tp<double>(dl_vp_ptr(c, 1)), tp<double>(dl_vp_ptr(c, 2)), ld, b);
+    DL_CHECK_LAUNCH(c);
+    int r = afun<double, double>(c, c->nei_coef64, x0, ax);
+    if (r) return r;
+    k_sub<double><<<(int)((n3 + 255) / 256), 256, 0, c->stream>>>(n3, b, ax, Q0);
+    DL_CHECK_LAUNCH(c);
+    double nb2 = 0.0, nr2 = 0.0;
+    if ((r = sumsq<double>(c, b, n3, &nb2))) return r;
+    if ((r = sumsq<double>(c, Q0, n3, &nr2))) return r;
+    const double norm_b = std::sqrt(nb2), norm_rhs = std::sqrt(nr2);
+    rep->norm_rhs = norm_rhs;
+    rep->iterations = 0;
+    rep->refinements = 0;
+    rep->residual = 0.0;
+    if (norm_rhs < kSmallRhs) return 0;   // pertvel unchanged
+    GmresResult g;
+    if ((r = gmres_iterate<double, double>(c, c->nei_coef64, norm_b, norm_rhs, 0.0, g))) return r;
+    if ((r = x_update<double>(c, g, x0, tp<double>(c->xt)))) return r;
+    k_uncopy3<double, double><<<bs, 256, 0, c->stream>>>(nps, tp<double>(c->xt), ld, tp<double>(c->pert[0]),
+                                                         tp<double>(c->pert[1]), tp<double>(c->pert[2]));
+    DL_CHECK_LAUNCH(c);
+    rep->iterations = g.iters;
+    rep->residual = g.res;
+    return g.converged ? 0 : DL_W_GMRES_NOT_CONVERGED;
+}
+
+// HDI_GMRES of a mixed context: FP32 GMRES corrections inside FP64 residual refinement.
+int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
+{
+    const int nps = c->nps;
+    const int64_t ld = nps, n3 = 3 * (int64_t)nps;
+    const int bs = dl_blocks(nps, 256);
+    double *x = c->xg, *b = c->bg64, *r64 = c->rg;
+    float *Q0 = tp<float>(c->kry);
+    k_copy3<float, double><<<bs, 256, 0, c->stream>>>(nps, tp<float>(c->pert[0]), tp<float>(c->pert[1]),
+                                                      tp<float>(c->pert[2]), ld, x);
+    DL_CHECK_LAUNCH(c);
+    const int vs = c->vcur;
+    k_afun_rhs<float><<<bs, 256, 0, c->stream>>>(nps, c->nei_start, c->nei_idx, c->nei_coef64,
+                                                 tp<float>(c->vel[vs][0]), tp<float>(c->vel[vs][1]),
+                                                 tp<float>(c->vel[vs][2]), tp<float>(dl_vp_ptr(c, 0)),
+                                                 tp<float>(dl_vp_ptr(c, 1)), tp<float>(dl_vp_ptr(c, 2)), ld, b);
+    DL_CHECK_LAUNCH(c);
+    int r;
+    double nb2 = 0.0;
+    if ((r = sumsq<double>(c, b, n3, &nb2))) return r;
+    const double norm_b = std::sqrt(nb2);
+    rep->iterations = 0;
+    rep->refinements = 0;
+    rep->residual = 0.0;
+    rep->norm_rhs = 0.0;
+    bool converged = false;
+    for (int sweep = 0; sweep <= kMaxRefine; sweep++) {
+        // FP64 residual of the current x
+        k_residual64<<<bs, 256, 0, c->stream>>>(nps, c->nei_start, c->nei_idx, c->nei_coef64, x, ld, b, r64, c->rf32);
+        DL_CHECK_LAUNCH(c);
+        rep->refinements = sweep + 1;
+        double rr = 0.0;
+        if ((r = sumsq<double>(c, r64, n3, &rr))) return r;
+        const double nr = std::sqrt(rr);
+        if (sweep == 0) {
+            rep->norm_rhs = nr;
+            if (nr < kSmallRhs) {   // nothing to solve: pertvel unchanged (partlib.f90:2853-2856)
+                rep->residual = 0.0;
+                return 0;
+            }
+        }
+        rep->residual = norm_b > 0.0 ? nr / norm_b : 0.0;
+        if (sweep > 0 && rep->residual < kMaxErr) { converged = true; break; }
+        if (sweep == kMaxRefine) break;
+        // FP32 correction: (I + N) d = r, d0 = 0
+        DL_CUDA(c, cudaMemcpyAsync(Q0, c->rf32, sizeof(float) * n3, cudaMemcpyDeviceToDevice, c->stream));
+        double nf2 = 0.0;
+        if ((r = sumsq<float>(c, Q0, n3, &nf2))) return r;
+        const double nf = std::sqrt(nf2);
+        if (!(nf > 0.0)) { converged = true; break; }
+        GmresResult g;
+        // stop the FP32 solve at a tenth of the FP64 target, or at FP32 resolution of r
+        const double stop_abs = std::max(0.1 * kMaxErr * norm_b, 1.0e-5 * nf);
+        if ((r = gmres_iterate<float, float>(c, tp<float>(c->nei_coef), norm_b, nf, stop_abs, g))) return r;
+        rep->iterations += g.iters;
+        if ((r = x_update<float>(c, g, x, x))) return r;
+    }
+    k_uncopy3<double, float><<<bs, 256, 0, c->stream>>>(nps, x, ld, tp<float>(c->pert[0]), tp<float>(c->pert[1]),
+                                                        tp<float>(c->pert[2]));
+    DL_CHECK_LAUNCH(c);
+    return converged ? 0 : DL_W_GMRES_NOT_CONVERGED;
+}
+
+}  // namespace
+
+// NEI_LIST_PRECOMP: CSR neighbour lists over the device order in the reference's order.
+int launch_nei_list(dl_ctx *c)
+{
+    if (!c->dc.hdi) return dl_fail(c, DL_E_STATE, "NEI_LIST_PRECOMP: HDI is off");
+    if (!c->hl_valid) return dl_fail(c, DL_E_STATE, "NEI_LIST_PRECOMP: call HEADLIST first");
+    const int nps = c->nps;
+    const size_t m = (size_t)c->msize;
+    int r;
+    if (!c->nei_cnt) {
+        if (cudaMalloc(&c->nei_cnt, sizeof(int) * (m + 1)) != cudaSuccess ||
+            cudaMalloc(&c->nei_start, sizeof(int) * (m + 1)) != cudaSuccess ||
+            cudaMalloc(&c->nei_fill, sizeof(int) * (m + 1)) != cudaSuccess ||
+            cudaMalloc(&c->nei_blk, sizeof(int) * (m / 1024 + 4) * 2) != cudaSuccess ||
+            cudaMalloc(&c->overlap_flag, sizeof(int) * 4) != cudaSuccess)
+            return dl_fail(c, DL_E_ALLOC, "NEI_LIST_PRECOMP: cudaMalloc failed");
+    }
+    c->nei_valid = 0;
+    c->nnz = 0;
+    DL_CUDA(c, cudaMemsetAsync(c->nei_cnt, 0, sizeof(int) * (m + 1), c->stream));
+    DL_CUDA(c, cudaMemsetAsync(c->nei_fill, 0, sizeof(int) * (m + 1), c->stream));
+    DL_CUDA(c, cudaMemsetAsync(c->overlap_flag, 0, sizeof(int) * 4, c->stream));
+    if (nps == 0) {
+        DL_CUDA(c, cudaMemsetAsync(c->nei_start, 0, sizeof(int), c->stream));
+        c->nei_valid = 1;
+        return 0;
+    }
+    NeiArgs A;
+    A.D = c->dc;
+    A.nps = nps;
+    A.px = c->pos[c->pcur][0]; A.py = c->pos[c->pcur][1]; A.pz = c->pos[c->pcur][2];
+    A.rad = c->rad;
+    A.ref = c->ref_of_dev;
+    A.g = c->ghosts;
+    A.row_start = c->row_start;
+    A.row_ent = (const long long *)c->row_ent;
+    A.cnt = c->nei_cnt;
+    A.start = c->nei_start;
+    A.fill = c->nei_fill;
+    A.partner = c->nei_idx;
+    A.key = c->nei_key;
+    A.coef = c->nei_coef64;
+    A.flag = c->overlap_flag;
+    k_nei_walk<false><<<dl_blocks(nps, 128), 128, 0, c->stream>>>(A);
+    DL_CHECK_LAUNCH(c);
+    // CSR offsets and the capacity check (the reference allows nei_max = 100 per droplet)
+    const int nblk = dl_blocks(nps, 1024);
+    int *bsum = c->nei_blk, *boff = c->nei_blk + (m / 1024 + 4);
+    k_cnt_blocksum<<<nblk, 1024, 0, c->stream>>>(nps, c->nei_cnt, bsum, c->overlap_flag + 2);
+    DL_CHECK_LAUNCH(c);
+    r = dl_scan(c, bsum, boff, nblk);
+    if (r) return r;
+    k_cnt_apply<<<nblk, 1024, 0, c->stream>>>(nps, c->nei_cnt, boff, nblk, c->nei_start);
+    DL_CHECK_LAUNCH(c);
+    int hf[4] = {0, 0, 0, 0}, nnz = 0;
+    DL_CUDA(c, cudaMemcpyAsync(hf, c->overlap_flag, sizeof(int) * 4, cudaMemcpyDeviceToHost, c->stream));
+    DL_CUDA(c, cudaMemcpyAsync(&nnz, c->nei_start + nps, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (hf[0]) {
+        int ref = -1;
+        DL_CUDA(c, cudaMemcpy(&ref, c->ref_of_dev + (hf[0] - 1), sizeof(int), cudaMemcpyDeviceToHost));
+        return dl_fail(c, DL_E_OVERLAP_HDI, "NEI_LIST_PRECOMP: overlapping droplets (droplet " +
+                                                std::to_string(ref + 1) + ")");
+    }
+    if (hf[2] > c->p.nei_max)
+        return dl_fail(c, DL_E_NEI_CAPACITY, "NEI_LIST_PRECOMP: " + std::to_string(hf[2]) +
+                                                 " neighbours for one droplet exceed nei_max = " +
+                                                 std::to_string(c->p.nei_max));
+    // entry storage
+    const size_t ne = std::max<size_t>((size_t)nnz, 1);
+    if (ne > c->nei_cap) {
+        size_t cap = std::max(ne + ne / 4, (size_t)4096);
+        cudaFree(c->nei_idx); cudaFree(c->nei_key); cudaFree(c->nei_coef64); cudaFree(c->nei_coef);
+        c->nei_idx = nullptr; c->nei_key = nullptr; c->nei_coef64 = nullptr; c->nei_coef = nullptr;
+        c->nei_cap = 0;
+        if (cudaMalloc(&c->nei_idx, sizeof(int) * cap) != cudaSuccess ||
+            cudaMalloc(&c->nei_key, sizeof(unsigned long long) * cap) != cudaSuccess ||
+            cudaMalloc(&c->nei_coef64, sizeof(double) * 6 * cap) != cudaSuccess ||
+            (c->mixed && cudaMalloc(&c->nei_coef, sizeof(float) * 6 * cap) != cudaSuccess))
+            return dl_fail(c, DL_E_ALLOC, "NEI_LIST_PRECOMP: cudaMalloc of the neighbour lists failed");
+        c->nei_cap = cap;
+        A.partner = c->nei_idx;
+        A.key = c->nei_key;
+        A.coef = c->nei_coef64;
+    }
+    if (nnz > 0) {
+        k_nei_walk<true><<<dl_blocks(nps, 128), 128, 0, c->stream>>>(A);
+        DL_CHECK_LAUNCH(c);
+        k_nei_sort<<<dl_blocks(nps, 128), 128, 0, c->stream>>>(nps, c->nei_start, c->nei_key, c->nei_idx,
+                                                               c->nei_coef64);
+        DL_CHECK_LAUNCH(c);
+        if (c->mixed) {
+            k_coef_to_f32<<<(int)((6 * (int64_t)nnz + 255) / 256), 256, 0, c->stream>>>(6 * (int64_t)nnz,
+                                                                                         c->nei_coef64,
+                                                                                         tp<float>(c->nei_coef));
+            DL_CHECK_LAUNCH(c);
+        }
+        int ovf = 0;
+        DL_CUDA(c, cudaMemcpyAsync(&ovf, c->overlap_flag + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaStreamSynchronize(c->stream));
+        if (ovf) return dl_fail(c, DL_E_STATE, "NEI_LIST_PRECOMP: count and fill passes disagree");
+    }
+    c->nnz = nnz;
+    c->nei_valid = 1;
+    return 0;
+}
+
+int run_gmres(dl_ctx *c, dl_gmres_report *rep)
+{
+    dl_gmres_report local;
+    if (!rep) rep = &local;
+    *rep = dl_gmres_report{0, 0, 0.0, 0.0};
+    if (!c->dc.hdi) return dl_fail(c, DL_E_STATE, "HDI_GMRES: HDI is off");
+    if (!c->nei_valid) return dl_fail(c, DL_E_STATE, "HDI_GMRES: call NEI_LIST_PRECOMP first");
+    if (c->nps == 0) return 0;
+    int r = gmres_buffers(c);
+    if (r) return r;
+    r = c->mixed ? gmres_mixed(c, rep) : gmres_fp64(c, rep);
+    c->gmres_iters = rep->iterations;
+    c->gmres_refine = rep->refinements;
+    c->gmres_res = rep->residual;
+    c->gmres_norm_rhs = rep->norm_rhs;
+    if (r == DL_W_GMRES_NOT_CONVERGED) c->err = "HDI_GMRES: not converged";
+    return r;
 }
 
 extern "C" int dl_nei_list_precomp(dl_ctx *c)
 {
     if (!c) return DL_E_ARG;
+    if (!c->initialized) return dl_fail(c, DL_E_STATE, "call dl_part_init first");
     return launch_nei_list(c);
 }
 
 extern "C" int dl_hdi_gmres(dl_ctx *c, dl_gmres_report *rep)
 {
     if (!c) return DL_E_ARG;
+    if (!c->initialized) return dl_fail(c, DL_E_STATE, "call dl_part_init first");
     return run_gmres(c, rep);
 }
 
-extern "C" int dl_get_nei(dl_ctx *c, int *, int *, double *, int, int *nnz)
+// Neighbour lists in reference order: nei_num(nps); per entry (ih1, partner) 1-based
+// reference indices (the source droplet for ghost partners) and 6 FP64 coefficients.
+extern "C" int dl_get_nei(dl_ctx *c, int *nei_num, int *pairs2, double *coef6, int cap, int *nnz)
 {
     if (!c) return DL_E_ARG;
-    if (nnz) *nnz = 0;
-    return dl_fail(c, DL_E_STATE, "dl_get_nei: not available in this build");
+    if (nnz) *nnz = c->nei_valid ? c->nnz : 0;
+    if (!c->nei_valid) return dl_fail(c, DL_E_STATE, "dl_get_nei: no neighbour lists (call dl_nei_list_precomp)");
+    const int nps = c->nps, nz = c->nnz;
+    if ((pairs2 || coef6) && cap < nz) return dl_fail(c, DL_E_CAPACITY, "dl_get_nei: cap < nnz");
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    std::vector<int> start(nps + 1), rod(nps), dor(nps), part(nz);
+    std::vector<double> cf((size_t)6 * nz);
+    DL_CUDA(c, cudaMemcpy(start.data(), c->nei_start, sizeof(int) * (nps + 1), cudaMemcpyDeviceToHost));
+    DL_CUDA(c, cudaMemcpy(rod.data(), c->ref_of_dev, sizeof(int) * nps, cudaMemcpyDeviceToHost));
+    DL_CUDA(c, cudaMemcpy(dor.data(), c->dev_of_ref, sizeof(int) * nps, cudaMemcpyDeviceToHost));
+    if (nz) {
+        DL_CUDA(c, cudaMemcpy(part.data(), c->nei_idx, sizeof(int) * nz, cudaMemcpyDeviceToHost));
+        DL_CUDA(c, cudaMemcpy(cf.data(), c->nei_coef64, sizeof(double) * 6 * nz, cudaMemcpyDeviceToHost));
+    }
+    int o = 0;
+    for (int rf = 0; rf < nps; rf++) {
+        const int d = dor[rf];
+        if (nei_num) nei_num[rf] = start[d + 1] - start[d];
+        for (int e = start[d]; e < start[d + 1]; e++, o++) {
+            if (pairs2) { pairs2[2 * o] = rf + 1; pairs2[2 * o + 1] = rod[part[e]] + 1; }
+            if (coef6)
+                for (int t = 0; t < 6; t++) coef6[6 * (size_t)o + t] = cf[6 * (size_t)e + t];
+        }
+    }
+    return 0;
 }

@@ -130,8 +130,9 @@ struct dl_ctx {
     // ---- cell list (HEADLIST) ----
     double hl_dist;
     int hl_valid;
-    Ghost *ghosts;
+    Ghost *ghosts;               // in the reference's ypn order (slot, then source reference index)
     int gcap, nghost;
+    int *gh_blk, *gh_start;      // [8 * nblk + 1] ghost counts per (slot, 1024 references) and offsets
     int *d_nghost;
     int *ent_row;                // row of each entry (owned + ghosts)
     int *ent_ix;                 // ix of each entry
@@ -146,6 +147,8 @@ struct dl_ctx {
     int *lv_blk;                 // [nblk + 1] per-1024-block counts -> offsets
     int *lv_refs;                // [msize] leaving reference indices, ascending
     int *lv_old, *lv_new, *lv_dev, *lv_dep;   // [msize] remap scratch
+    int *lv_src;                 // [msize] (HDI) device holding each new reference index before the reorder
+    void *pert_tmp;              // [3 * msize] (HDI) pertvel values kept at their reference index
     int *d_err;                  // device error flags (see DL_DERR_*)
     double *xfer64;              // [3 * msize] host<->device transfer scratch
     int *xfer_i;                 // [4 * msize] host<->device transfer scratch
@@ -174,18 +177,24 @@ struct dl_ctx {
     // ---- MEAN_VEL ----
     double *mv_acc;
 
-    // ---- HDI ----
-    int *nei_cnt, *nei_start;    // CSR over owned droplets
-    int *nei_idx;                // partner entry
-    void *nei_coef;              // NeiCoef<T>
-    double *nei_coef64;          // FP64 coefficients for the residual (mixed)
-    int nei_cap, nnz;
-    int *overlap_flag;
+    // ---- HDI (allocated on first use) ----
+    int *nei_cnt, *nei_start;    // CSR over owned droplets (device order)
+    int *nei_fill;               // per-owner fill cursors
+    int *nei_blk;                // scan scratch
+    int *nei_idx;                // partner: device index of the source droplet
+    unsigned long long *nei_key; // reference append order of each entry
+    void *nei_coef;              // 6 FP32 coefficients per entry (mixed)
+    double *nei_coef64;          // 6 FP64 coefficients per entry (reference arithmetic)
+    size_t nei_cap;
+    int nnz, nei_valid;
+    int *overlap_flag;           // [0] overlapping owner + 1, [1] fill overflow, [2] largest count
     // GMRES work
     void *kry;                   // Krylov basis (maxiter+1) x 3*msize, T
+    size_t hdi_kry_bytes;
     double *xg, *rg, *bg64, *tmp64;   // FP64 vectors (3*msize)
-    void *wv, *xt;               // T vectors
-    double *dots;                // device scratch for dot products
+    void *wv, *xt;               // T vectors (3*msize)
+    float *rf32;                 // FP32 copy of the FP64 residual (mixed)
+    double *dots;                // reduction scratch
     int gmres_iters, gmres_refine;
     double gmres_res, gmres_norm_rhs;
 

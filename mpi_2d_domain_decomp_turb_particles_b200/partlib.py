@@ -238,6 +238,17 @@ class Partlib:
         self._chk(self.lib.dl_hdi_gmres(self.h, C.byref(r)))
         return r
 
+    def nei(self):
+        """NEI_LIST_PRECOMP output in reference order: (nei_num (nps,), pairs (nnz, 2) of
+        1-based (owner, partner source) reference indices, coefficients (nnz, 6))."""
+        n = C.c_int(0)
+        num = np.zeros(self.nps, np.int32)
+        self._chk(self.lib.dl_get_nei(self.h, _iptr(num), None, None, 0, C.byref(n)))
+        pairs = np.zeros((n.value, 2), np.int32)
+        coef = np.zeros((n.value, 6))
+        self._chk(self.lib.dl_get_nei(self.h, _iptr(num), _iptr(pairs), _dptr(coef), n.value, C.byref(n)))
+        return num, pairs, coef
+
     def part_history_fdp(self):
         self._chk(self.lib.dl_part_history_fdp(self.h))
 
