@@ -52,6 +52,12 @@ class _Contact(C.Structure):
     _fields_ = [("ih1", C.c_int), ("src2", C.c_int), ("jid2", C.c_int), ("rec", C.c_double * 12)]
 
 
+class _AdjParams(C.Structure):
+    _fields_ = [("n", C.c_int), ("np", C.c_int), ("nsteps", C.c_int), ("init_velocity", C.c_int),
+                ("dt", C.c_double), ("gravity", C.c_double), ("pair_factor", C.c_double),
+                ("w_wr", C.c_double), ("w_disp", C.c_double)]
+
+
 _lib = None
 
 
@@ -83,6 +89,12 @@ def _load():
     lib.orc_mean_vel.argtypes = [vp, dp]
     lib.orc_afun_precomp.argtypes = [vp, dp, C.c_int]
     lib.orc_findindex.argtypes = [vp, C.c_double, C.c_double, ip, ip]
+    lib.orc_adj_forward.restype = C.c_int
+    lib.orc_adj_forward.argtypes = [C.POINTER(_AdjParams), dp, C.c_long, C.c_long, C.c_long, dp, dp, dp, dp, ip,
+                                    dp, dp]
+    lib.orc_adj_gradient.restype = C.c_int
+    lib.orc_adj_gradient.argtypes = [C.POINTER(_AdjParams), dp, C.c_long, C.c_long, C.c_long, dp, dp, dp, dp, dp,
+                                     dp, dp]
     lib.orc_ranpp.restype = C.c_double
     lib.orc_ranpp.argtypes = [ip, ip, ip]
     lib.orc_ranff2.restype = C.c_double
@@ -382,3 +394,64 @@ class Oracle:
             out["overlap_sweeps"] = self.overlap_det(max_sweeps)
         self.setd("time", self.getd("time") + self.getd("dt"))
         return out
+
+
+# ------------------------------------------------------------------------------------
+# Droplet adjoint reference (adjoint_oracle.h)
+# ------------------------------------------------------------------------------------
+class AdjointOracle:
+    """FP64 forward loss and exact discrete adjoint of the droplet advance in a frozen
+    field (see adjoint_oracle.h).  ``u`` is (3, n, n, llx) float64 (x fastest, llx >= n),
+    ``x0`` (np, 3), ``tau`` and ``rad`` (np,)."""
+
+    def __init__(self, n, nsteps, dt, gravity, init_velocity=0, pair_factor=2.0, w_wr=1.0, w_disp=1.0):
+        self.kw = dict(n=n, nsteps=nsteps, dt=dt, gravity=gravity, init_velocity=init_velocity,
+                       pair_factor=pair_factor, w_wr=w_wr, w_disp=w_disp)
+        self.lib = _load()
+
+    def _params(self, np_):
+        p = _AdjParams()
+        for k, v in self.kw.items():
+            setattr(p, k, v)
+        p.np = np_
+        return p
+
+    @staticmethod
+    def _arrs(u, x0, tau, rad):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        x0 = np.ascontiguousarray(x0, dtype=np.float64)
+        tau = np.ascontiguousarray(tau, dtype=np.float64)
+        rad = np.ascontiguousarray(rad, dtype=np.float64)
+        return u, x0, tau, rad
+
+    def forward(self, u, x0, tau, rad):
+        u, x0, tau, rad = self._arrs(u, x0, tau, rad)
+        n, llx = u.shape[1], u.shape[3]
+        dp = C.POINTER(C.c_double)
+        loss = C.c_double(0)
+        npairs = C.c_int(0)
+        xN = np.zeros_like(x0)
+        vN = np.zeros_like(x0)
+        rc = self.lib.orc_adj_forward(C.byref(self._params(len(x0))), u.ctypes.data_as(dp), llx, llx * n,
+                                      llx * n * n, x0.ctypes.data_as(dp), tau.ctypes.data_as(dp),
+                                      rad.ctypes.data_as(dp), C.byref(loss), C.byref(npairs),
+                                      xN.ctypes.data_as(dp), vN.ctypes.data_as(dp))
+        if rc:
+            raise RuntimeError(f"orc_adj_forward: {rc}")
+        return loss.value, npairs.value, xN, vN
+
+    def gradient(self, u, x0, tau, rad):
+        u, x0, tau, rad = self._arrs(u, x0, tau, rad)
+        n, llx = u.shape[1], u.shape[3]
+        dp = C.POINTER(C.c_double)
+        loss = C.c_double(0)
+        dx0 = np.zeros_like(x0)
+        dtau = np.zeros_like(tau)
+        du = np.zeros_like(u)
+        rc = self.lib.orc_adj_gradient(C.byref(self._params(len(x0))), u.ctypes.data_as(dp), llx, llx * n,
+                                       llx * n * n, x0.ctypes.data_as(dp), tau.ctypes.data_as(dp),
+                                       rad.ctypes.data_as(dp), C.byref(loss), dx0.ctypes.data_as(dp),
+                                       dtau.ctypes.data_as(dp), du.ctypes.data_as(dp))
+        if rc:
+            raise RuntimeError(f"orc_adj_gradient: {rc}")
+        return loss.value, dx0, dtau, du
