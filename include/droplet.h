@@ -232,6 +232,50 @@ int dl_set_stream(dl_ctx *ctx, void *stream);
 int dl_timing(dl_ctx *ctx, int reset, double *avg_update_ms, int *nsteps, int64_t *kernel_launches);
 
 /* ---------------------------------------------------------------------------------------
+ * Droplet adjoint (no counterpart in the reference)
+ * ------------------------------------------------------------------------------------- */
+/* Gradients of a droplet statistic through nsteps substeps of the reference's
+ * interpolation + advance (partlib.f90:317-338, 462-510, 553-757; Stokes drag, no HDI) in
+ * a frozen periodic field, with respect to the field, the initial positions and the drag
+ * times tau_p.  The gravity term dt * W / tau_p of PART_ADVANCE is dt * gravity with
+ * gravity fixed; V_0 is the terminal velocity gravity * tau_p e_x (init_velocity = 0,
+ * partlib.f90:564-566) or the fluid velocity (1).  Positions are not wrapped.
+ * Loss = w_wr * mean over final pairs |r| < pair_factor * (a_i + a_j) (minimum image) of
+ * (v_i - v_j) . r / |r|  +  w_disp * mean over droplets of |x(T) - x(0)|^2.
+ * The forward pass keeps a checkpoint every checkpoint_every steps; the backward pass
+ * recomputes each segment from its checkpoint and runs the exact discrete adjoint. */
+typedef struct dl_adj_params {
+    int n;                       /* grid points per side */
+    int np;                      /* droplets */
+    int nsteps;                  /* substeps */
+    int checkpoint_every;        /* 0 -> 20 */
+    int precision;               /* DL_FP64, or DL_MIXED (FP32 velocities/field/weights, FP64 positions) */
+    int init_velocity;           /* 0 terminal velocity, 1 fluid velocity */
+    int device;
+    double dt, gravity;          /* DNS units; gravity along x */
+    double pair_factor, w_wr, w_disp;
+} dl_adj_params;
+
+typedef struct dl_adj dl_adj;
+int dl_adj_create(const dl_adj_params *p, dl_adj **out);
+int dl_adj_destroy(dl_adj *a);
+const char *dl_adj_last_error(const dl_adj *a);
+int dl_adj_set_stream(dl_adj *a, void *stream);
+/* one component (icpt 1..3) in the INTERPOLATE layout v(llx, ly, lz), host or device */
+int dl_adj_set_field(dl_adj *a, int icpt, const double *v, int64_t pitch_y, int64_t pitch_z, int on_device);
+/* x0 (np, 3) row-major, tau_p (np), radius (np) in DNS units, host or device */
+int dl_adj_set_droplets(dl_adj *a, const double *x0, const double *tau, const double *radius, int on_device);
+int dl_adj_forward(dl_adj *a, double *loss, int *npairs);
+/* dL/dx0 (np, 3), dL/dtau_p (np) (both required) and, when du is not NULL, dL/du: three
+ * components, component c at du + c * pitch_z * n, in the layout given by the pitches
+ * (padding columns x >= n are set to 0).  Host or device arrays. */
+int dl_adj_backward(dl_adj *a, double *dx0, double *dtau, double *du, int64_t pitch_y, int64_t pitch_z, int on_device);
+/* final positions and velocities (np, 3) of the last forward pass */
+int dl_adj_get_final(dl_adj *a, double *xN, double *vN);
+/* device ms of the last forward pass (steps only) and backward pass (recompute + reverse) */
+int dl_adj_timing(dl_adj *a, double *forward_ms, double *backward_ms);
+
+/* ---------------------------------------------------------------------------------------
  * Allocation-free entry point (no counterpart in the reference)
  * ------------------------------------------------------------------------------------- */
 /* The PERIODIC reorder permutation (partlib.f90:866-1133, single rank) for callers that

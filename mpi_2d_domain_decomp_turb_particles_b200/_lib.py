@@ -70,6 +70,15 @@ class GmresReport(C.Structure):
     ]
 
 
+class AdjParams(C.Structure):
+    _fields_ = [
+        ("n", C.c_int), ("np", C.c_int), ("nsteps", C.c_int), ("checkpoint_every", C.c_int),
+        ("precision", C.c_int), ("init_velocity", C.c_int), ("device", C.c_int),
+        ("dt", C.c_double), ("gravity", C.c_double),
+        ("pair_factor", C.c_double), ("w_wr", C.c_double), ("w_disp", C.c_double),
+    ]
+
+
 # name -> (restype, argtypes); the exported surface of include/droplet.h
 _vp, _ip, _dp, _fp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_float)
 SIGNATURES = {
@@ -117,6 +126,16 @@ SIGNATURES = {
     "dl_get_phase_times": (C.c_int, [_vp, _dp]),
     "dl_set_stream": (C.c_int, [_vp, C.c_void_p]),
     "dl_timing": (C.c_int, [_vp, C.c_int, _dp, _ip, C.POINTER(C.c_int64)]),
+    "dl_adj_create": (C.c_int, [C.POINTER(AdjParams), C.POINTER(C.c_void_p)]),
+    "dl_adj_destroy": (C.c_int, [_vp]),
+    "dl_adj_last_error": (C.c_char_p, [_vp]),
+    "dl_adj_set_stream": (C.c_int, [_vp, C.c_void_p]),
+    "dl_adj_set_field": (C.c_int, [_vp, C.c_int, C.c_void_p, C.c_int64, C.c_int64, C.c_int]),
+    "dl_adj_set_droplets": (C.c_int, [_vp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "dl_adj_forward": (C.c_int, [_vp, _dp, _ip]),
+    "dl_adj_backward": (C.c_int, [_vp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int]),
+    "dl_adj_get_final": (C.c_int, [_vp, _dp, _dp]),
+    "dl_adj_timing": (C.c_int, [_vp, _dp, _dp]),
     "dl_periodic_order_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
 }
 

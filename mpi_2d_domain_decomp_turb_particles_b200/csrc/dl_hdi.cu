@@ -28,6 +28,7 @@
 //     tensors and FP64 x, an FP32 GMRES solve for the correction, x += d, until the FP64
 //     relative residual ||b - (I + N) x|| / ||b|| is below 1e-6.
 #include "dl_internal.cuh"
+#include "dl_scan.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -229,53 +230,6 @@ __global__ void k_coef_to_f32(int64_t n, const double *c, float *o)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) o[i] = (float)c[i];
-}
-
-// multi-block exclusive scan of per-owner counts: block sums (+ the largest count) ...
-__global__ void __launch_bounds__(1024) k_cnt_blocksum(int n, const int *cnt, int *bsum, int *maxcnt)
-{
-    __shared__ int ws[32];
-    const int i = blockIdx.x * 1024 + threadIdx.x;
-    const int v = i < n ? cnt[i] : 0;
-    int s = v, m = v;
-    for (int o = 16; o > 0; o >>= 1) {
-        s += __shfl_down_sync(0xffffffffu, s, o);
-        m = max(m, __shfl_down_sync(0xffffffffu, m, o));
-    }
-    if ((threadIdx.x & 31) == 0) { ws[threadIdx.x >> 5] = s; atomicMax(maxcnt, m); }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        int t = ws[threadIdx.x];
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-        if (threadIdx.x == 0) bsum[blockIdx.x] = t;
-    }
-}
-
-// ... then the in-block scan plus the block offset
-__global__ void __launch_bounds__(1024) k_cnt_apply(int n, const int *cnt, const int *boff, int nblk, int *start)
-{
-    __shared__ int ws[32];
-    const int i = blockIdx.x * 1024 + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int v = i < n ? cnt[i] : 0;
-    int incl = v;
-    for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    if (lane == 31) ws[w] = incl;
-    __syncthreads();
-    if (w == 0) {
-        const int a = ws[lane];
-        int ai = a;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, ai, o);
-            if (lane >= o) ai += t;
-        }
-        ws[lane] = ai - a;
-    }
-    __syncthreads();
-    if (i < n) start[i] = boff[blockIdx.x] + ws[w] + incl - v;
-    if (blockIdx.x == 0 && threadIdx.x == 0) start[n] = boff[nblk];
 }
 
 // ---------------------------------------------------------------------------------------
@@ -831,14 +785,8 @@ int launch_nei_list(dl_ctx *c)
     k_nei_walk<false><<<dl_blocks(nps, 128), 128, 0, c->stream>>>(A);
     DL_CHECK_LAUNCH(c);
     // CSR offsets and the capacity check (the reference allows nei_max = 100 per droplet)
-    const int nblk = dl_blocks(nps, 1024);
-    int *bsum = c->nei_blk, *boff = c->nei_blk + (m / 1024 + 4);
-    k_cnt_blocksum<<<nblk, 1024, 0, c->stream>>>(nps, c->nei_cnt, bsum, c->overlap_flag + 2);
-    DL_CHECK_LAUNCH(c);
-    r = dl_scan(c, bsum, boff, nblk);
-    if (r) return r;
-    k_cnt_apply<<<nblk, 1024, 0, c->stream>>>(nps, c->nei_cnt, boff, nblk, c->nei_start);
-    DL_CHECK_LAUNCH(c);
+    DL_CUDA(c, dl_scan_counts(c->stream, c->nei_cnt, c->nei_start, nps, c->nei_blk, c->overlap_flag + 2));
+    c->launches += 3;
     int hf[4] = {0, 0, 0, 0}, nnz = 0;
     DL_CUDA(c, cudaMemcpyAsync(hf, c->overlap_flag, sizeof(int) * 4, cudaMemcpyDeviceToHost, c->stream));
     DL_CUDA(c, cudaMemcpyAsync(&nnz, c->nei_start + nps, sizeof(int), cudaMemcpyDeviceToHost, c->stream));

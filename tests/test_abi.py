@@ -38,7 +38,8 @@ def test_struct_layouts_match_the_c_header(tmp_path):
     """Compile a probe against include/droplet.h with gcc and compare sizes/offsets."""
     import subprocess
     structs = {"dl_params": _lib.Params, "dl_scalars": _lib.Scalars,
-               "dl_coll_report": _lib.CollReport, "dl_gmres_report": _lib.GmresReport}
+               "dl_coll_report": _lib.CollReport, "dl_gmres_report": _lib.GmresReport,
+               "dl_adj_params": _lib.AdjParams}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "droplet.h"', "int main(void){"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
