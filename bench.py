@@ -210,6 +210,8 @@ def run_ours(args):
         dist.all_reduce(t64, op=dist.ReduceOp.MAX)
     value64 = ws * N_PART / (float(t64[0]) * 1e-3)
 
+    adj = adjoint_bench(dev, torch) if not args.no_adjoint else None
+
     if rank == 0:
         peak, kind = _peaks()
         alg = update_bytes("mixed", N_GRID, N_PART)
@@ -231,6 +233,7 @@ def run_ours(args):
             "e2e": {"value": N_PART / (e2e_ms * 1e-3), "unit": "particle-updates/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "path": "dl_set_field (host FP64 field, pinned) + dl_update_step + dl_mean_vel"},
+            "adjoint": adj,
             "gpu_launches": int(launches),
             "clocks": clocks,
             "cpu_baseline": cpu_baseline(),
@@ -239,6 +242,65 @@ def run_ours(args):
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+ADJ = dict(n=128, np=200_000, radius_um=25.0, nsteps=400, checkpoint_every=20, dt=5e-4,
+           etk_dns=0.0158, tauk_dns=0.156, pair_factor=2.0)
+
+
+def adjoint_bench(dev, torch):
+    """Adjoint workload (128^3 frozen field, 200,000 droplets of 25 um, 400 substeps,
+    checkpoint every 20): device time of the forward pass and of the backward pass
+    (recompute + reverse sweep), per substep, beside the production update step on the
+    same field and droplets."""
+    import numpy as np
+    from mpi_2d_domain_decomp_turb_particles_b200 import Partlib, ParticleParams
+    from mpi_2d_domain_decomp_turb_particles_b200.adjoint import AdjointParams, DropletAdjoint
+    from mpi_2d_domain_decomp_turb_particles_b200.synthetic import spectral_field
+    n, npart = ADJ["n"], ADJ["np"]
+    phys = dict(dt=ADJ["dt"], rnu=PHYS["rnu"], etk_dns=ADJ["etk_dns"], tauk_dns=ADJ["tauk_dns"])
+    g = Partlib(ParticleParams(nx=n, npart=npart, radius_um=[ADJ["radius_um"]], precision="mixed",
+                               device=dev, **phys))
+    g.part_init()
+    s = g.scalars()
+    a_dns = s.radius[0]
+    tau = s.tau_cloud_const2 * a_dns * a_dns
+    grav = s.sv_const / s.tau_cloud_const2
+    field = spectral_field(n, seed=1234, device=f"cuda:{dev}")
+    g.set_fields(*field)
+    stream = torch.cuda.Stream(device=dev)
+    g.set_stream(stream)
+    upd_ms, upd_kms, _ = _time_update(g, stream, 50, 5, torch)
+    yp = g.get_particles()["yp"]
+    g.close()
+    x0 = torch.tensor(np.ascontiguousarray(yp[:, :3]), device=f"cuda:{dev}")
+    taus = torch.full((npart,), tau, dtype=torch.float64, device=f"cuda:{dev}")
+    rad = torch.full((npart,), a_dns, dtype=torch.float64, device=f"cuda:{dev}")
+    u = torch.stack(field).contiguous()
+    out = {}
+    for prec in ("mixed", "fp64"):
+        p = AdjointParams(n=n, nsteps=ADJ["nsteps"], dt=ADJ["dt"], gravity=grav, precision=prec,
+                          checkpoint_every=ADJ["checkpoint_every"], pair_factor=ADJ["pair_factor"], device=dev)
+        a = DropletAdjoint(p, npart)
+        a.set_field(u)
+        a.set_droplets(x0, taus, rad)
+        dx0 = torch.zeros((npart, 3), dtype=torch.float64, device=f"cuda:{dev}")
+        dtau = torch.zeros(npart, dtype=torch.float64, device=f"cuda:{dev}")
+        du = torch.zeros_like(u)
+        torch.cuda.synchronize()
+        for _ in range(2):   # the second pair is timed
+            loss, npairs = a.forward()
+            a.backward(dx0, dtau, du)
+        fms, bms = a.timing()
+        a.close()
+        steps = ADJ["nsteps"]
+        out[prec] = {"forward_ms_per_step": fms / steps, "backward_ms_per_step": bms / steps,
+                     "adjoint_over_forward": bms / fms, "loss": loss, "pairs": npairs}
+    return {"workload": "128^3 frozen synthetic field, 200,000 droplets of 25 um, 400 substeps, "
+                        "checkpoint every 20; loss = mean w_r of pairs within 2(a_i+a_j) + mean |x_T - x_0|^2",
+            "mixed": out["mixed"], "fp64": out["fp64"],
+            "update_step_ms_same_config": upd_ms, "update_kernels_ms_same_config": upd_kms,
+            "adjoint_over_update_step": out["mixed"]["backward_ms_per_step"] / upd_ms}
 
 
 def _oracle_sample(npart, n, steps, min_seconds=0.0):
@@ -304,6 +366,7 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint workload")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

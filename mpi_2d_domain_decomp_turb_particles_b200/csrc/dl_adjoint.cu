@@ -115,18 +115,43 @@ __device__ __forceinline__ int64_t stencil_at(const Field<T> &F, const double *x
     return corner;
 }
 
-template <typename T>
-__device__ __forceinline__ void interp(const Field<T> &F, const double *x, T *out)
+// FP64: the reference's order (x outer, z inner, v*bx*by*bz) so that the forward is
+// bit-identical to the FP64 reference; FP32: separable sums with FMA
+__device__ __forceinline__ void interp(const Field<double> &F, const double *x, double *out)
 {
-    T b[3][6];
-    const int64_t c0 = stencil_at<T>(F, x, b, nullptr);
+    double b[3][6];
+    const int64_t c0 = stencil_at<double>(F, x, b, nullptr);
     for (int comp = 0; comp < 3; comp++) {
-        const T *v = F.f + comp * F.comp + c0;
-        T acc = (T)0;
+        const double *v = F.f + comp * F.comp + c0;
+        double acc = 0.0;
         for (int a = 0; a < 6; a++)
             for (int bb = 0; bb < 6; bb++)
                 for (int c = 0; c < 6; c++)
                     acc = acc + v[a + F.py * bb + F.pz * c] * b[0][a] * b[1][bb] * b[2][c];
+        out[comp] = acc;
+    }
+}
+
+__device__ __forceinline__ void interp(const Field<float> &F, const double *x, float *out)
+{
+    float b[3][6];
+    const int64_t c0 = stencil_at<float>(F, x, b, nullptr);
+    for (int comp = 0; comp < 3; comp++) {
+        const float *v = F.f + comp * F.comp + c0;
+        float acc = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            float tz = 0.0f;
+#pragma unroll
+            for (int bb = 0; bb < 6; bb++) {
+                const float *row = v + F.pz * c + F.py * bb;
+                float ty = 0.0f;
+#pragma unroll
+                for (int a = 0; a < 6; a++) ty = fmaf(row[a], b[0][a], ty);
+                tz = fmaf(ty, b[1][bb], tz);
+            }
+            acc = fmaf(tz, b[2][c], acc);
+        }
         out[comp] = acc;
     }
 }
@@ -214,7 +239,7 @@ __global__ void __launch_bounds__(128) k_adj_segment(SegArgs<T> A)
     const int64_t slot = 3 * (int64_t)np;
     for (int j = 0; j < A.nstep; j++) {
         T U0[3];
-        interp<T>(A.F, x, U0);
+        interp(A.F, x, U0);
         if (A.first && j == 0) {   // PART_HISTORY_FVP / FDP first step: every level
             for (int c = 0; c < 3; c++) {
                 V[c] = A.init_velocity ? U0[c] : (c == 0 ? g * tau : (T)0);
@@ -566,12 +591,13 @@ __global__ void k_adj_seed_pairs(int np, int npairs, const int2 *pairs, const do
 }
 
 __global__ void k_adj_finish(int np, double cd, const double *xbar, const double *x, const double *x0,
-                             const double *taubar, double *dx0, double *dtau)
+                             const double *taubar, const int *perm, double *dx0, double *dtau)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= np) return;
-    for (int c = 0; c < 3; c++) dx0[3 * i + c] = xbar[c * np + i] - cd * (x[c * np + i] - x0[3 * i + c]);
-    dtau[i] = taubar[i];
+    const int o = perm[i];
+    for (int c = 0; c < 3; c++) dx0[3 * o + c] = xbar[c * np + i] - cd * (x[c * np + i] - x0[3 * i + c]);
+    dtau[o] = taubar[i];
 }
 
 }  // namespace
@@ -601,6 +627,8 @@ struct dl_adj {
     void *P = nullptr, *Q = nullptr;
     int *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr, *cell_key = nullptr, *cell_order = nullptr;
     int *scan_tmp = nullptr;
+    int *perm = nullptr;          // internal droplet index -> caller's index
+    std::vector<int> hperm;
     int2 *pairs = nullptr;
     int *d_npairs = nullptr;
     int npairs = 0, pair_cap = 0, nc = 0;
@@ -750,10 +778,17 @@ int find_pairs(dl_adj *a)
         return find_pairs<T>(a);
     }
     a->npairs = np2;
-    if (np2 > 1) {
+    if (np2 > 0) {
+        // (i, j) with i before j in the caller's order, sorted by the caller's indices: the
+        // pair sum then runs in the order of the reference's (i, j > i) loops
+        const std::vector<int> &pm = a->hperm;
         std::vector<int2> h(np2);
         ACUDA(a, cudaMemcpy(h.data(), a->pairs, sizeof(int2) * np2, cudaMemcpyDeviceToHost));
-        std::sort(h.begin(), h.end(), [](const int2 &u, const int2 &v) { return u.x != v.x ? u.x < v.x : u.y < v.y; });
+        for (auto &q : h)
+            if (pm[q.x] > pm[q.y]) std::swap(q.x, q.y);
+        std::sort(h.begin(), h.end(), [&](const int2 &u, const int2 &v) {
+            return pm[u.x] != pm[v.x] ? pm[u.x] < pm[v.x] : pm[u.y] < pm[v.y];
+        });
         ACUDA(a, cudaMemcpy(a->pairs, h.data(), sizeof(int2) * np2, cudaMemcpyHostToDevice));
     }
     return 0;
@@ -825,7 +860,8 @@ int backward_t(dl_adj *a, double *dx0, double *dtau, double *du, int64_t py, int
         dtaud = tmp + 3 * (size_t)np;
         dud = tmp + 4 * (size_t)np;
     }
-    k_adj_finish<<<dl_blocks(np, 256), 256, 0, a->stream>>>(np, cd, a->xbar, a->xs, a->x0, a->taubar, dx0d, dtaud);
+    k_adj_finish<<<dl_blocks(np, 256), 256, 0, a->stream>>>(np, cd, a->xbar, a->xs, a->x0, a->taubar, a->perm, dx0d,
+                                                            dtaud);
     ACUDA(a, cudaGetLastError());
     if (du) {
         const int64_t tot = (int64_t)llx * n * n;
@@ -905,6 +941,7 @@ extern "C" int dl_adj_create(const dl_adj_params *p, dl_adj **out)
     ADJ_ALLOC(a->cell_fill, sizeof(int) * (ncell + 1));
     ADJ_ALLOC(a->scan_tmp, sizeof(int) * 2 * (ncell / 1024 + 4));
     ADJ_ALLOC(a->cell_key, sizeof(int) * np);
+    ADJ_ALLOC(a->perm, sizeof(int) * np);
     ADJ_ALLOC(a->cell_order, sizeof(int) * np);
     ADJ_ALLOC(a->pairs, sizeof(int2) * a->pair_cap);
     ADJ_ALLOC(a->d_npairs, sizeof(int));
@@ -925,7 +962,7 @@ extern "C" int dl_adj_destroy(dl_adj *a)
     if (a->own_stream) cudaStreamSynchronize(a->own_stream);
     void *ptrs[] = {a->fpad, a->gpad, a->x0, a->tau, a->rad, a->xs, a->ss, a->ckx, a->cks, a->TX, a->TV, a->TU,
                     a->xbar, a->taubar, a->P, a->Q, a->cell_cnt, a->cell_start, a->cell_fill, a->scan_tmp,
-                    a->cell_key, a->cell_order, a->pairs, a->d_npairs, a->red};
+                    a->cell_key, a->cell_order, a->pairs, a->d_npairs, a->red, a->perm};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     for (auto &e : a->ev)
@@ -980,15 +1017,43 @@ extern "C" int dl_adj_set_droplets(dl_adj *a, const double *x0, const double *ta
 {
     if (!a || !x0 || !tau || !radius) return DL_E_ARG;
     const size_t np = a->p.np;
-    const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    ACUDA(a, cudaMemcpyAsync(a->x0, x0, sizeof(double) * 3 * np, k, a->stream));
-    ACUDA(a, cudaMemcpyAsync(a->tau, tau, sizeof(double) * np, k, a->stream));
-    ACUDA(a, cudaMemcpyAsync(a->rad, radius, sizeof(double) * np, k, a->stream));
+    std::vector<double> hx(3 * np), ht(np), hr(np);
+    const cudaMemcpyKind k = on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost;
     ACUDA(a, cudaStreamSynchronize(a->stream));
+    ACUDA(a, cudaMemcpy(hx.data(), x0, sizeof(double) * 3 * np, k));
+    ACUDA(a, cudaMemcpy(ht.data(), tau, sizeof(double) * np, k));
+    ACUDA(a, cudaMemcpy(hr.data(), radius, sizeof(double) * np, k));
+    // internal order: droplets sorted by 4x4x4-cell bricks of their initial position (the
+    // stencil gathers and gradient scatters of neighbouring threads then share cache lines)
+    const int nb = (a->n + 3) / 4;
+    std::vector<long long> key(np);
+    for (size_t i = 0; i < np; i++) {
+        int c[3];
+        for (int d = 0; d < 3; d++) {
+            const double w = hx[3 * i + d] - a->pi2 * std::floor(hx[3 * i + d] / a->pi2);
+            const int q = (int)(w / a->dx);
+            c[d] = std::min(std::max(q, 0), a->n - 1);
+        }
+        const long long brick = ((long long)(c[2] / 4) * nb + c[1] / 4) * nb + c[0] / 4;
+        key[i] = (brick * 64 + ((c[2] % 4) * 4 + c[1] % 4) * 4 + c[0] % 4) * (long long)np + (long long)i;
+    }
+    std::vector<int> order(np);
+    for (size_t i = 0; i < np; i++) order[i] = (int)i;
+    std::sort(order.begin(), order.end(), [&](int u, int v) { return key[u] < key[v]; });
+    a->hperm = order;   // internal index -> caller's index
+    std::vector<double> sx(3 * np), st(np), sr(np);
+    for (size_t q = 0; q < np; q++) {
+        const int i = order[q];
+        for (int d = 0; d < 3; d++) sx[3 * q + d] = hx[3 * (size_t)i + d];
+        st[q] = ht[i];
+        sr[q] = hr[i];
+    }
+    ACUDA(a, cudaMemcpy(a->x0, sx.data(), sizeof(double) * 3 * np, cudaMemcpyHostToDevice));
+    ACUDA(a, cudaMemcpy(a->tau, st.data(), sizeof(double) * np, cudaMemcpyHostToDevice));
+    ACUDA(a, cudaMemcpy(a->rad, sr.data(), sizeof(double) * np, cudaMemcpyHostToDevice));
+    ACUDA(a, cudaMemcpy(a->perm, order.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
     // pair cells at least as wide as the largest cutoff
-    std::vector<double> h(np);
-    ACUDA(a, cudaMemcpy(h.data(), a->rad, sizeof(double) * np, cudaMemcpyDeviceToHost));
-    const double rmax = *std::max_element(h.begin(), h.end());
+    const double rmax = *std::max_element(hr.begin(), hr.end());
     const double cut = a->p.pair_factor * 2.0 * rmax;
     int nc = cut > 0.0 ? (int)std::floor(a->pi2 / cut) : 128;
     a->nc = std::max(3, std::min(128, nc));
@@ -1024,20 +1089,21 @@ extern "C" int dl_adj_get_final(dl_adj *a, double *xN, double *vN)
     std::vector<double> x(3 * (size_t)np);
     ACUDA(a, cudaStreamSynchronize(a->stream));
     ACUDA(a, cudaMemcpy(x.data(), a->xs, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost));
+    const std::vector<int> &pm = a->hperm;
     if (xN)
         for (int i = 0; i < np; i++)
-            for (int c = 0; c < 3; c++) xN[3 * i + c] = x[(size_t)c * np + i];
+            for (int c = 0; c < 3; c++) xN[3 * pm[i] + c] = x[(size_t)c * np + i];
     if (vN) {
         if (a->mixed) {
             std::vector<float> v(3 * (size_t)np);
             ACUDA(a, cudaMemcpy(v.data(), a->ss, sizeof(float) * 3 * np, cudaMemcpyDeviceToHost));
             for (int i = 0; i < np; i++)
-                for (int c = 0; c < 3; c++) vN[3 * i + c] = v[(size_t)c * np + i];
+                for (int c = 0; c < 3; c++) vN[3 * pm[i] + c] = v[(size_t)c * np + i];
         } else {
             std::vector<double> v(3 * (size_t)np);
             ACUDA(a, cudaMemcpy(v.data(), a->ss, sizeof(double) * 3 * np, cudaMemcpyDeviceToHost));
             for (int i = 0; i < np; i++)
-                for (int c = 0; c < 3; c++) vN[3 * i + c] = v[(size_t)c * np + i];
+                for (int c = 0; c < 3; c++) vN[3 * pm[i] + c] = v[(size_t)c * np + i];
         }
     }
     return 0;
