@@ -20,8 +20,10 @@
 // adjoint state (x_bar, tau_bar and two three-deep shift registers of velocity and
 // fluid-velocity adjoints) in registers.  The interpolation adjoint is a scatter of
 // U_bar (x) weights into the grid gradient with atomics, plus the gradient of the
-// interpolant for x_bar.  Field and grid gradient use the halo-padded layout of the main
-// path, so no index wraps inside the stencil loops.
+// interpolant for x_bar.  Field and grid gradient are halo-padded (4 planes of periodic
+// images on every side, so no index wraps inside the stencil loops) with the three
+// components interleaved per point and a fourth pad slot: one vector load reads a
+// point's velocity and, in FP32, one vector atomic adds a point's gradient.
 //
 // Precision: DL_FP64 everything in FP64 (same operation order as the FP64 reference
 // adjoint, bit-identical forward); DL_MIXED FP32 velocities, histories, field, weights
@@ -92,9 +94,9 @@ __device__ __forceinline__ int wrapn(int i, int n)
 
 template <typename T>
 struct Field {
-    const T *f;        // padded field, component c at f + c * comp
+    const T *f;        // padded field, point p's component c at f[4 * p + c]
     T *g;              // padded grid gradient (same layout)
-    int64_t py, pz, comp;
+    int64_t py, pz;    // points per row and per plane
     int n;
     double dx;
 };
@@ -122,12 +124,12 @@ __device__ __forceinline__ void interp(const Field<double> &F, const double *x, 
     double b[3][6];
     const int64_t c0 = stencil_at<double>(F, x, b, nullptr);
     for (int comp = 0; comp < 3; comp++) {
-        const double *v = F.f + comp * F.comp + c0;
+        const double *v = F.f + 4 * c0 + comp;
         double acc = 0.0;
         for (int a = 0; a < 6; a++)
             for (int bb = 0; bb < 6; bb++)
                 for (int c = 0; c < 6; c++)
-                    acc = acc + v[a + F.py * bb + F.pz * c] * b[0][a] * b[1][bb] * b[2][c];
+                    acc = acc + v[4 * (a + F.py * bb + F.pz * c)] * b[0][a] * b[1][bb] * b[2][c];
         out[comp] = acc;
     }
 }
@@ -136,24 +138,46 @@ __device__ __forceinline__ void interp(const Field<float> &F, const double *x, f
 {
     float b[3][6];
     const int64_t c0 = stencil_at<float>(F, x, b, nullptr);
-    for (int comp = 0; comp < 3; comp++) {
-        const float *v = F.f + comp * F.comp + c0;
-        float acc = 0.0f;
+    float acc[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-        for (int c = 0; c < 6; c++) {
-            float tz = 0.0f;
+    for (int c = 0; c < 6; c++) {
+        float tz[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-            for (int bb = 0; bb < 6; bb++) {
-                const float *row = v + F.pz * c + F.py * bb;
-                float ty = 0.0f;
+        for (int bb = 0; bb < 6; bb++) {
+            const float4 *row = reinterpret_cast<const float4 *>(F.f) + c0 + F.pz * c + F.py * bb;
+            float ty[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-                for (int a = 0; a < 6; a++) ty = fmaf(row[a], b[0][a], ty);
-                tz = fmaf(ty, b[1][bb], tz);
+            for (int a = 0; a < 6; a++) {
+                const float4 v = row[a];
+                ty[0] = fmaf(v.x, b[0][a], ty[0]);
+                ty[1] = fmaf(v.y, b[0][a], ty[1]);
+                ty[2] = fmaf(v.z, b[0][a], ty[2]);
             }
-            acc = fmaf(tz, b[2][c], acc);
+            for (int q = 0; q < 3; q++) tz[q] = fmaf(ty[q], b[1][bb], tz[q]);
         }
-        out[comp] = acc;
+        for (int q = 0; q < 3; q++) acc[q] = fmaf(tz[q], b[2][c], acc[q]);
     }
+    for (int q = 0; q < 3; q++) out[q] = acc[q];
+}
+
+__device__ __forceinline__ void load3(const float *p, float *v)
+{
+    const float4 q = *reinterpret_cast<const float4 *>(p);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z;
+}
+__device__ __forceinline__ void load3(const double *p, double *v)
+{
+    const double2 q = *reinterpret_cast<const double2 *>(p);
+    v[0] = q.x; v[1] = q.y; v[2] = p[2];
+}
+// one vector atomic per point (FP32); three scalar atomics (FP64)
+__device__ __forceinline__ void add3(float *p, float a, float b, float c)
+{
+    atomicAdd(reinterpret_cast<float4 *>(p), make_float4(a, b, c, 0.0f));
+}
+__device__ __forceinline__ void add3(double *p, double a, double b, double c)
+{
+    atomicAdd(p, a); atomicAdd(p + 1, b); atomicAdd(p + 2, c);
 }
 
 // x_bar += J^T ubar; grid gradient += ubar (x) weights
@@ -168,14 +192,52 @@ __device__ __forceinline__ void interp_adjoint(const Field<T> &F, const double *
             for (int c = 0; c < 6; c++) {
                 const int64_t o = c0 + a + F.py * bb + F.pz * c;
                 const T w = b[0][a] * b[1][bb] * b[2][c];
-                const T sv = ub[0] * F.f[o] + ub[1] * F.f[F.comp + o] + ub[2] * F.f[2 * F.comp + o];
+                T f3[3];
+                load3(F.f + 4 * o, f3);
+                const T sv = ub[0] * f3[0] + ub[1] * f3[1] + ub[2] * f3[2];
                 gx = gx + sv * d[0][a] * b[1][bb] * b[2][c];
                 gy = gy + sv * b[0][a] * d[1][bb] * b[2][c];
                 gz = gz + sv * b[0][a] * b[1][bb] * d[2][c];
-                atomicAdd(F.g + o, ub[0] * w);
-                atomicAdd(F.g + F.comp + o, ub[1] * w);
-                atomicAdd(F.g + 2 * F.comp + o, ub[2] * w);
+                add3(F.g + 4 * o, ub[0] * w, ub[1] * w, ub[2] * w);
             }
+    xbar[0] = xbar[0] + (double)gx / F.dx;
+    xbar[1] = xbar[1] + (double)gy / F.dx;
+    xbar[2] = xbar[2] + (double)gz / F.dx;
+}
+
+// FP32: z planes outer, the 6 x 6 (x, y) points of a plane unrolled, separable sums, one
+// vector atomic per point
+template <>
+__device__ __forceinline__ void interp_adjoint<float>(const Field<float> &F, const double *x, const float *ub,
+                                                      double *xbar)
+{
+    float b[3][6], d[3][6];
+    const int64_t c0 = stencil_at<float>(F, x, b, d);
+    float gx = 0.0f, gy = 0.0f, gz = 0.0f;
+    for (int c = 0; c < 6; c++) {
+        const float bz = b[2][c], dz = d[2][c];
+        float tx = 0.0f, ty = 0.0f, tw = 0.0f;
+#pragma unroll
+        for (int bb = 0; bb < 6; bb++) {
+            float rx = 0.0f, rw = 0.0f;
+#pragma unroll
+            for (int a = 0; a < 6; a++) {
+                const int64_t o = c0 + a + F.py * bb + F.pz * c;
+                const float4 f = *reinterpret_cast<const float4 *>(F.f + 4 * o);
+                const float sv = fmaf(ub[2], f.z, fmaf(ub[1], f.y, ub[0] * f.x));
+                rx = fmaf(sv, d[0][a], rx);
+                rw = fmaf(sv, b[0][a], rw);
+                const float w = b[0][a] * b[1][bb] * bz;
+                atomicAdd(reinterpret_cast<float4 *>(F.g + 4 * o), make_float4(ub[0] * w, ub[1] * w, ub[2] * w, 0.0f));
+            }
+            tx = fmaf(rx, b[1][bb], tx);
+            ty = fmaf(rw, d[1][bb], ty);
+            tw = fmaf(rw, b[1][bb], tw);
+        }
+        gx = fmaf(tx, bz, gx);
+        gy = fmaf(ty, bz, gy);
+        gz = fmaf(tw, dz, gz);
+    }
     xbar[0] = xbar[0] + (double)gx / F.dx;
     xbar[1] = xbar[1] + (double)gy / F.dx;
     xbar[2] = xbar[2] + (double)gz / F.dx;
@@ -331,6 +393,7 @@ __global__ void __launch_bounds__(128) k_adj_reverse(RevArgs<T> A)
         const int64_t sj = (int64_t)(j + 3) * slot;
         T newV[3] = {(T)0, (T)0, (T)0}, newU[3] = {(T)0, (T)0, (T)0};
         T dtaubar = (T)0;
+#pragma unroll
         for (int c = 0; c < 3; c++) {
             const T V = A.TV[sj + c * np + i], Vn1 = A.TV[sj + slot + c * np + i];
             const T F1 = A.TV[sj - slot + c * np + i], F2 = A.TV[sj - 2 * slot + c * np + i];
@@ -347,18 +410,24 @@ __global__ void __launch_bounds__(128) k_adj_reverse(RevArgs<T> A)
             dtaubar = dtaubar + Vt * Acoef * ((tempd - tempv) - (T)9 * Vn1);
             // contributions to the adjoints of steps n, n-1, n-2 (and n-3), indices
             // below 0 go to step 0 (the first-step history copies)
-            for (int k = 0; k < 3; k++) {
-                const int idx = n - k < 0 ? 0 : n - k;
-                const int s = n + 1 - idx;
-                if (s < 3) P[s][c] = P[s][c] + cv[k];
-                else newV[c] = newV[c] + cv[k];
-            }
-            for (int k = 0; k < 4; k++) {
-                const int idx = n - k < 0 ? 0 : n - k;
-                const int s = n - idx;
-                if (s < 3) Q[s][c] = Q[s][c] + cu[k];
-                else newU[c] = newU[c] + cu[k];
-            }
+            // (registers P[1], P[2], newV hold steps n, n-1, n-2; Q[0], Q[1], Q[2], newU
+            // steps n .. n-3; the additions keep the reference adjoint's order)
+            P[1][c] = P[1][c] + cv[0];
+            if (n >= 1) P[2][c] = P[2][c] + cv[1];
+            else P[1][c] = P[1][c] + cv[1];
+            if (n >= 2) newV[c] = newV[c] + cv[2];
+            else if (n == 1) P[2][c] = P[2][c] + cv[2];
+            else P[1][c] = P[1][c] + cv[2];
+            Q[0][c] = Q[0][c] + cu[0];
+            if (n >= 1) Q[1][c] = Q[1][c] + cu[1];
+            else Q[0][c] = Q[0][c] + cu[1];
+            if (n >= 2) Q[2][c] = Q[2][c] + cu[2];
+            else if (n == 1) Q[1][c] = Q[1][c] + cu[2];
+            else Q[0][c] = Q[0][c] + cu[2];
+            if (n >= 3) newU[c] = newU[c] + cu[3];
+            else if (n == 2) Q[2][c] = Q[2][c] + cu[3];
+            else if (n == 1) Q[1][c] = Q[1][c] + cu[3];
+            else Q[0][c] = Q[0][c] + cu[3];
         }
         taubar = taubar + (double)dtaubar * (-A.dt / (24.0 * A.tau[i] * A.tau[i]));
         if (n == 0) {   // the initial velocity
@@ -385,7 +454,7 @@ __global__ void __launch_bounds__(128) k_adj_reverse(RevArgs<T> A)
 }
 
 // ---------------------------------------------------------------------------------------
-// Field conversion, gradient fold, loss
+// Field conversion (into the 4-interleaved padded layout), gradient fold, loss
 // ---------------------------------------------------------------------------------------
 template <typename T>
 __global__ void k_adj_pad(const double *v, int64_t py, int64_t pz, int n, T *out, int64_t opy, int64_t opz)
@@ -396,7 +465,7 @@ __global__ void k_adj_pad(const double *v, int64_t py, int64_t pz, int n, T *out
     const int x = (int)(i % e);
     const int64_t yz = i / e;
     const int y = (int)(yz % e), z = (int)(yz / e);
-    out[x + opy * y + opz * z] =
+    out[4 * (x + opy * y + opz * z)] =
         (T)v[wrapn(x - DL_PAD_LO, n) + py * wrapn(y - DL_PAD_LO, n) + pz * wrapn(z - DL_PAD_LO, n)];
 }
 
@@ -421,7 +490,7 @@ __global__ void k_adj_fold(const T *g, int64_t gpy, int64_t gpz, int n, double *
                 for (int ox = -1; ox <= 1; ox++) {
                     const int pxi = x + DL_PAD_LO + ox * n;
                     if (pxi < 0 || pxi >= e) continue;
-                    acc += (double)g[pxi + gpy * pyi + gpz * pzi];
+                    acc += (double)g[4 * (pxi + gpy * pyi + gpz * pzi)];
                 }
             }
         }
@@ -614,7 +683,7 @@ struct dl_adj {
     int n = 0, nseg = 0, K = 0;
     double dx = 0.0, pi2 = 0.0;
     void *fpad = nullptr, *gpad = nullptr;
-    int64_t py = 0, pz = 0, comp = 0;
+    int64_t py = 0, pz = 0, comp = 0;   // points per row, plane and field (4 values per point)
     int field_set = 0, drops_set = 0, forward_done = 0;
     double *x0 = nullptr, *tau = nullptr, *rad = nullptr;
     double *xs = nullptr;    // state x [3][np]
@@ -668,7 +737,6 @@ Field<T> field_of(dl_adj *a)
     F.g = tp<T>(a->gpad);
     F.py = a->py;
     F.pz = a->pz;
-    F.comp = a->comp;
     F.n = a->n;
     F.dx = a->dx;
     return F;
@@ -831,7 +899,7 @@ int backward_t(dl_adj *a, double *dx0, double *dtau, double *du, int64_t py, int
     const int np = a->p.np, n = a->n;
     const double cd = a->p.w_disp * 2.0 / (double)np;
     ACUDA(a, cudaEventRecord(a->ev[2], a->stream));
-    ACUDA(a, cudaMemsetAsync(a->gpad, 0, 3 * (size_t)a->comp * a->esz, a->stream));
+    ACUDA(a, cudaMemsetAsync(a->gpad, 0, 4 * (size_t)a->comp * a->esz, a->stream));
     k_adj_seed<T><<<dl_blocks(np, 256), 256, 0, a->stream>>>(np, cd, a->xs, a->x0, a->xbar, a->taubar, tp<T>(a->P),
                                                             tp<T>(a->Q));
     ACUDA(a, cudaGetLastError());
@@ -867,7 +935,7 @@ int backward_t(dl_adj *a, double *dx0, double *dtau, double *du, int64_t py, int
         const int64_t tot = (int64_t)llx * n * n;
         for (int c = 0; c < 3; c++) {
             k_adj_fold<T><<<(int)((tot + 255) / 256), 256, 0, a->stream>>>(
-                tp<T>(a->gpad) + c * a->comp, a->py, a->pz, n, dud + (size_t)c * pz * n, py, pz, llx);
+                tp<T>(a->gpad) + c, a->py, a->pz, n, dud + (size_t)c * pz * n, py, pz, llx);
             ACUDA(a, cudaGetLastError());
         }
     }
@@ -916,8 +984,8 @@ extern "C" int dl_adj_create(const dl_adj_params *p, dl_adj **out)
     int r = 0;
 #define ADJ_ALLOC(ptr, bytes)                                   \
     if (!r) r = aalloc(a, (void **)&(ptr), (size_t)(bytes));
-    ADJ_ALLOC(a->fpad, 3 * a->comp * es);
-    ADJ_ALLOC(a->gpad, 3 * a->comp * es);
+    ADJ_ALLOC(a->fpad, 4 * a->comp * es);
+    ADJ_ALLOC(a->gpad, 4 * a->comp * es);
     ADJ_ALLOC(a->x0, 3 * np * 8);
     ADJ_ALLOC(a->tau, np * 8);
     ADJ_ALLOC(a->rad, np * 8);
@@ -1001,10 +1069,10 @@ extern "C" int dl_adj_set_field(dl_adj *a, int icpt, const double *v, int64_t pi
     const int blocks = (int)((tot + 255) / 256);
     if (a->mixed)
         k_adj_pad<float><<<blocks, 256, 0, a->stream>>>(src, pitch_y, pitch_z, n,
-                                                        tp<float>(a->fpad) + (icpt - 1) * a->comp, a->py, a->pz);
+                                                        tp<float>(a->fpad) + (icpt - 1), a->py, a->pz);
     else
         k_adj_pad<double><<<blocks, 256, 0, a->stream>>>(src, pitch_y, pitch_z, n,
-                                                         tp<double>(a->fpad) + (icpt - 1) * a->comp, a->py, a->pz);
+                                                         tp<double>(a->fpad) + (icpt - 1), a->py, a->pz);
     ACUDA(a, cudaGetLastError());
     if (tmp) ACUDA(a, cudaFreeAsync(tmp, a->stream));
     ACUDA(a, cudaStreamSynchronize(a->stream));
@@ -1023,23 +1091,31 @@ extern "C" int dl_adj_set_droplets(dl_adj *a, const double *x0, const double *ta
     ACUDA(a, cudaMemcpy(hx.data(), x0, sizeof(double) * 3 * np, k));
     ACUDA(a, cudaMemcpy(ht.data(), tau, sizeof(double) * np, k));
     ACUDA(a, cudaMemcpy(hr.data(), radius, sizeof(double) * np, k));
-    // internal order: droplets sorted by 4x4x4-cell bricks of their initial position (the
-    // stencil gathers and gradient scatters of neighbouring threads then share cache lines)
-    const int nb = (a->n + 3) / 4;
-    std::vector<long long> key(np);
+    // internal order: droplets sorted along the Morton curve of the cells of their initial
+    // position, so that the stencils of a warp cover a compact box (shared cache lines in
+    // the gathers, nearby grid points in the gradient atomics)
+    auto spread = [](uint64_t v) {
+        v &= 0x1fffff;
+        v = (v | v << 32) & 0x1f00000000ffffULL;
+        v = (v | v << 16) & 0x1f0000ff0000ffULL;
+        v = (v | v << 8) & 0x100f00f00f00f00fULL;
+        v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+        v = (v | v << 2) & 0x1249249249249249ULL;
+        return v;
+    };
+    std::vector<uint64_t> key(np);
     for (size_t i = 0; i < np; i++) {
-        int c[3];
+        uint64_t c[3];
         for (int d = 0; d < 3; d++) {
             const double w = hx[3 * i + d] - a->pi2 * std::floor(hx[3 * i + d] / a->pi2);
             const int q = (int)(w / a->dx);
-            c[d] = std::min(std::max(q, 0), a->n - 1);
+            c[d] = (uint64_t)std::min(std::max(q, 0), a->n - 1);
         }
-        const long long brick = ((long long)(c[2] / 4) * nb + c[1] / 4) * nb + c[0] / 4;
-        key[i] = (brick * 64 + ((c[2] % 4) * 4 + c[1] % 4) * 4 + c[0] % 4) * (long long)np + (long long)i;
+        key[i] = spread(c[0]) | spread(c[1]) << 1 | spread(c[2]) << 2;
     }
     std::vector<int> order(np);
     for (size_t i = 0; i < np; i++) order[i] = (int)i;
-    std::sort(order.begin(), order.end(), [&](int u, int v) { return key[u] < key[v]; });
+    std::stable_sort(order.begin(), order.end(), [&](int u, int v) { return key[u] < key[v]; });
     a->hperm = order;   // internal index -> caller's index
     std::vector<double> sx(3 * np), st(np), sr(np);
     for (size_t q = 0; q < np; q++) {
