@@ -232,6 +232,51 @@ int dl_set_stream(dl_ctx *ctx, void *stream);
 int dl_timing(dl_ctx *ctx, int reset, double *avg_update_ms, int *nsteps, int64_t *kernel_launches);
 
 /* ---------------------------------------------------------------------------------------
+ * Carrier flow: spectral Navier-Stokes step on the device (turb.f90:506-691)
+ * ------------------------------------------------------------------------------------- */
+/* Pseudo-spectral FP64 step of the reference: curl and velocity to physical space,
+ * u x omega, forward transform (1/n^3), dealiasing at shell int(n/2 - 1.5), Crank-Nicolson
+ * viscous + AB2 nonlinear update, stochastic forcing (supforSTH, flowlib.f90:378-562) or
+ * deterministic forcing of shells 1-2 (supforDET, 195-229), projection, symmetrize
+ * (233-334) and dealiasing.  Spectral state: 3 components of n x n x (n/2+1) complex
+ * (re, im interleaved), component-major, mode (kz, ky, kx >= 0) at (z*n + y)*(n/2+1) + x. */
+typedef struct dl_flow_params {
+    int n;                       /* grid points per side (even) */
+    int forcing;                 /* 0 none, 1 deterministic (force[0..1]), 2 stochastic (iseedf) */
+    int iseedf;                  /* parameter.d seed of the stochastic forcing (used as -iseedf) */
+    int device;
+    double nu, dt;
+    double force[2];             /* energies of shells 1 and 2 (forcing = 1) */
+} dl_flow_params;
+
+typedef struct dl_flow dl_flow;
+int dl_flow_create(const dl_flow_params *p, dl_flow **out);
+int dl_flow_destroy(dl_flow *f);
+const char *dl_flow_last_error(const dl_flow *f);
+int dl_flow_set_stream(dl_flow *f, void *stream);
+int dl_flow_sync(dl_flow *f);
+/* new flow from a physical velocity (3 components in the INTERPOLATE layout v(llx, ly, lz),
+ * component c at u + c * pitch_z * n), host or device: transform, projection, symmetrize,
+ * dealiasing; N_old = u as the reference's new-flow start (turb.f90:452-454). */
+int dl_flow_set_velocity(dl_flow *f, const double *u, int64_t pitch_y, int64_t pitch_z, int on_device);
+/* spectral state (and N_old; NULL -> N_old = u), host or device; symmetrized and dealiased */
+int dl_flow_set_spectral(dl_flow *f, const double *uh, const double *nold, int on_device);
+int dl_flow_get_spectral(dl_flow *f, double *uh, double *nold);
+/* stochastic forcing restart record: b1r, b2r, b3r (3 x 150 doubles, (6,5,5) each) and
+ * the ranff state (input_outputf, turb.f90:459) */
+int dl_flow_get_forcing_state(dl_flow *f, double *b450, int *iseedf, int *iyf, int *ivf32);
+int dl_flow_set_forcing_state(dl_flow *f, const double *b450, int iseedf, int iyf, const int *ivf32);
+/* One time step.  The physical velocity of the state at the start of the step (the field
+ * the particle substep of this step interpolates, turb.f90:537-539) is left on the device
+ * (dl_flow_velocity) and, when droplets is not NULL, set as that context's field. */
+int dl_flow_step(dl_flow *f, dl_ctx *droplets);
+/* device pointer to physical component icpt (1..3) of the last step's velocity
+ * (n^3, x fastest; pitches n and n*n), NULL before the first step */
+const double *dl_flow_velocity(dl_flow *f, int icpt);
+/* energy per shell ik = int(|k| + 0.5), ik = 0..nshell-1 (kx = 0 modes count half) */
+int dl_flow_spectrum(dl_flow *f, double *ek, int nshell);
+
+/* ---------------------------------------------------------------------------------------
  * Droplet adjoint (no counterpart in the reference)
  * ------------------------------------------------------------------------------------- */
 /* Gradients of a droplet statistic through nsteps substeps of the reference's

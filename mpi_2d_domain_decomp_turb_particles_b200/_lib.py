@@ -79,6 +79,13 @@ class AdjParams(C.Structure):
     ]
 
 
+class FlowParams(C.Structure):
+    _fields_ = [
+        ("n", C.c_int), ("forcing", C.c_int), ("iseedf", C.c_int), ("device", C.c_int),
+        ("nu", C.c_double), ("dt", C.c_double), ("force", C.c_double * 2),
+    ]
+
+
 # name -> (restype, argtypes); the exported surface of include/droplet.h
 _vp, _ip, _dp, _fp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_float)
 SIGNATURES = {
@@ -126,6 +133,19 @@ SIGNATURES = {
     "dl_get_phase_times": (C.c_int, [_vp, _dp]),
     "dl_set_stream": (C.c_int, [_vp, C.c_void_p]),
     "dl_timing": (C.c_int, [_vp, C.c_int, _dp, _ip, C.POINTER(C.c_int64)]),
+    "dl_flow_create": (C.c_int, [C.POINTER(FlowParams), C.POINTER(C.c_void_p)]),
+    "dl_flow_destroy": (C.c_int, [_vp]),
+    "dl_flow_last_error": (C.c_char_p, [_vp]),
+    "dl_flow_set_stream": (C.c_int, [_vp, C.c_void_p]),
+    "dl_flow_sync": (C.c_int, [_vp]),
+    "dl_flow_set_velocity": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_int64, C.c_int]),
+    "dl_flow_set_spectral": (C.c_int, [_vp, C.c_void_p, C.c_void_p, C.c_int]),
+    "dl_flow_get_spectral": (C.c_int, [_vp, _dp, _dp]),
+    "dl_flow_get_forcing_state": (C.c_int, [_vp, _dp, _ip, _ip, _ip]),
+    "dl_flow_set_forcing_state": (C.c_int, [_vp, _dp, C.c_int, C.c_int, _ip]),
+    "dl_flow_step": (C.c_int, [_vp, _vp]),
+    "dl_flow_velocity": (C.c_void_p, [_vp, C.c_int]),
+    "dl_flow_spectrum": (C.c_int, [_vp, _dp, C.c_int]),
     "dl_adj_create": (C.c_int, [C.POINTER(AdjParams), C.POINTER(C.c_void_p)]),
     "dl_adj_destroy": (C.c_int, [_vp]),
     "dl_adj_last_error": (C.c_char_p, [_vp]),

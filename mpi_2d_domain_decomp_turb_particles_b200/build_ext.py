@@ -57,7 +57,8 @@ def build(verbose: bool = False, force: bool = False) -> str:
             if r.returncode != 0:
                 raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
     if force or _stale(OUT, objs):
-        cmd = [nvcc, "-shared", "-o", OUT, *objs, "-lcudart", "-Wno-deprecated-gpu-targets"]
+        cmd = [nvcc, "-shared", "-o", OUT, *objs, "-lcudart", "-lcufft", "-Xlinker", "-rpath=/usr/local/cuda/lib64",
+               "-Wno-deprecated-gpu-targets"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
