@@ -100,12 +100,12 @@ def _profile_traffic():
     return float(m.group(1)) if m else None
 
 
-def _make(precision, dev, npart=N_PART, n=N_GRID):
+def _make(precision, dev, npart=N_PART, n=N_GRID, hdi=False):
     import numpy as np
     from mpi_2d_domain_decomp_turb_particles_b200 import Partlib, ParticleParams
     from mpi_2d_domain_decomp_turb_particles_b200.synthetic import droplets
     p = ParticleParams(nx=n, npart=npart, radius_um=SETS_UM, precision=precision, device=dev,
-                       new_particle=True, **PHYS)
+                       new_particle=True, hdi_included=hdi, nonoverlap=hdi, hdi_trunc=50.0, **PHYS)
     g = Partlib(p)
     g.part_init()
     s = g.scalars()
@@ -211,6 +211,7 @@ def run_ours(args):
     value64 = ws * N_PART / (float(t64[0]) * 1e-3)
 
     adj = adjoint_bench(dev, torch) if not args.no_adjoint else None
+    full = full_step_bench(dev, torch, field) if not args.no_full else None
 
     if rank == 0:
         peak, kind = _peaks()
@@ -233,6 +234,7 @@ def run_ours(args):
             "e2e": {"value": N_PART / (e2e_ms * 1e-3), "unit": "particle-updates/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "path": "dl_set_field (host FP64 field, pinned) + dl_update_step + dl_mean_vel"},
+            "full_step": full,
             "adjoint": adj,
             "gpu_launches": int(launches),
             "clocks": clocks,
@@ -242,6 +244,58 @@ def run_ours(args):
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def full_step_bench(dev, torch, field):
+    """The whole time step of the headline configuration: the device flow step (256^3 FP64
+    pseudo-spectral, stochastic forcing) and the droplet substep with hydrodynamic
+    interaction (1M droplets, radii U[10, 40] um, mixed precision), device time per step."""
+    from mpi_2d_domain_decomp_turb_particles_b200.flow import Flow
+    fl = Flow(N_GRID, PHYS["rnu"], PHYS["dt"], forcing=2, iseedf=232300, device=dev)
+    u = torch.stack(field).contiguous()
+    fl.set_velocity(u)
+    stream = torch.cuda.Stream(device=dev)
+    fl.set_stream(stream)
+    for _ in range(3):
+        fl.step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nf = 10
+    e0.record(stream)
+    for _ in range(nf):
+        fl.step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    flow_ms = e0.elapsed_time(e1) / nf
+    # droplets with HDI, fed by the flow
+    g = _make("mixed", dev, hdi=True)
+    g.set_stream(stream)
+    fl.step(g)
+    g.periodic()
+    g.overlap_det()
+    g.sync()
+    for _ in range(2):
+        fl.step(g)
+        g.particle_step()
+    torch.cuda.synchronize()
+    ts, iters = [], []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fl.step(g)
+        _c, gm = g.particle_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+        iters.append(gm.iterations)
+    ph = g.phase_times()
+    g.close()
+    fl.close()
+    return {"workload": "256^3 FP64 flow step (stochastic forcing) + 1M-droplet substep with HDI (50 radii), mixed",
+            "flow_step_ms": flow_ms, "step_ms": statistics.median(ts),
+            "particle_phase_ms": {"interp_advance": ph[0], "cell_list": ph[1], "collision": ph[2], "hdi": ph[3],
+                                  "periodic_relocate": ph[4], "overlap": ph[5]},
+            "gmres_iterations": iters}
 
 
 ADJ = dict(n=128, np=200_000, radius_um=25.0, nsteps=400, checkpoint_every=20, dt=5e-4,
@@ -367,6 +421,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint workload")
+    ap.add_argument("--no-full", action="store_true", help="skip the flow + HDI full-step workload")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
