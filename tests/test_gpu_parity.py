@@ -305,3 +305,26 @@ def test_periodic_reorder_matches_oracle():
     o.periodic()
     g.periodic()
     assert np.array_equal(g.get_particles()["yp"], o.yp[:o.nps])
+
+
+def test_coalescence_growth_mode_matches_oracle():
+    """Past nstep_grow (turb.f90:588-590) collided pairs merge (COALESCE) instead of being
+    relocated: FP64 state, droplet count and merged radii identical to the oracle."""
+    n = 32
+    p = dense_params(n=n, npart=6000, nonoverlap=True)
+    g, o = make(p)
+    f = smooth_field(n)
+    g.set_fields(*f)
+    g.periodic(); g.overlap_det()
+    o.periodic(); o.overlap_det()
+    g.set_step(39998, 0.0)
+    o.seti("istep", 39998)
+    merged = 0
+    for step in range(8):
+        n0 = g.nps
+        rep, _ = g.particle_step()
+        o.particle_step(*f)
+        merged += n0 - g.nps
+        assert g.nps == o.nps, f"step {step}"
+        assert np.array_equal(gpu_state(g), oracle_state(o)), f"step {step}"
+    assert merged > 0
