@@ -383,8 +383,9 @@ static int allocate_state(dl_ctx *c)
     ALLOC(c->long_rows, sizeof(int) * (c->nrows + 1));
     ALLOC(c->n_long, sizeof(int));
     ALLOC(c->leave_nid, m);
-    ALLOC(c->lv_blk, sizeof(int) * (m / 1024 + 4));
     ALLOC(c->lv_refs, sizeof(int) * m);
+    ALLOC(c->lv_list, sizeof(int) * m);
+    ALLOC(c->lv_n, sizeof(int));
     ALLOC(c->lv_old, sizeof(int) * m);
     ALLOC(c->lv_new, sizeof(int) * m);
     ALLOC(c->lv_dev, sizeof(int) * m);
@@ -437,9 +438,9 @@ extern "C" int dl_destroy(dl_ctx *c)
     for (int k = 0; k < 3; k++) { F(c->vpv[k]); F(c->dmv[k]); F(c->pert[k]); F(c->f64_own[k]); }
     F(c->rad); F(c->gid); F(c->ref_of_dev); F(c->dev_of_ref); F(c->keys); F(c->perm); F(c->perm_scratch);
     F(c->long_rows); F(c->n_long);
-    F(c->brick_start); F(c->brick_cnt); F(c->lhnode); F(c->bg); F(c->ghosts); F(c->d_nghost); F(c->gh_blk); F(c->gh_start); F(c->pert_tmp); F(c->lv_src);
+    F(c->brick_start); F(c->brick_cnt); F(c->lhnode); F(c->bg); F(c->ghosts); F(c->d_nghost); F(c->gh_blk); F(c->gh_start); F(c->pert_tmp); F(c->lv_src); F(c->lv_list); F(c->lv_n);
     F(c->ent_row); F(c->ent_ix); F(c->row_start); F(c->row_fill); F(c->row_ent); F(c->leave_nid);
-    F(c->lv_blk); F(c->lv_refs); F(c->lv_old); F(c->lv_new); F(c->lv_dev); F(c->lv_dep); F(c->d_err);
+    F(c->lv_refs); F(c->lv_old); F(c->lv_new); F(c->lv_dev); F(c->lv_dep); F(c->d_err);
     F(c->xfer64); F(c->xfer_i); F(c->hist_i); F(c->hist_d); F(c->acc_i); F(c->acc_d); F(c->out_i); F(c->out_d);
     F(c->counts); F(c->cand); F(c->pairs); F(c->contacts); F(c->remove_dev); F(c->pair_buf); F(c->pair_ibuf); F(c->mv_acc);
     F(c->ovl_list); F(c->ovl_cnt); F(c->fpad_own);
@@ -1330,7 +1331,10 @@ extern "C" int dl_particle_step(dl_ctx *c, dl_coll_report *coll, dl_gmres_report
     const bool hdi = c->dc.hdi;
     const bool nonoverlap = c->p.nonoverlap || c->p.hdi_included;
     cudaEventRecord(c->ev[0], c->stream);
-    bool fused = !hdi;
+    // the fused kernel flags departures before COLLISION_DET; COALESCE (growth mode)
+    // renumbers droplets in between, so those steps flag them afterwards (PERIODIC order)
+    const bool growth = c->istep >= nstep_grow && nonoverlap;
+    bool fused = !hdi && !growth;
     if (fused) {
         timing_begin(c);
         r = launch_interp(c, 0, 1);   // PREPARE_INTERP..PART_ADVANCE + position update + wrap
@@ -1357,6 +1361,8 @@ extern "C" int dl_particle_step(dl_ctx *c, dl_coll_report *coll, dl_gmres_report
         r = run_gmres(c, gm);
         if (r < 0) return r;
         warn = r;   // GMRES not converged: the reference prints and carries on
+    }
+    if (!fused) {
         r = dl_part_history_fdp(c);
         if (r) return r;
         r = dl_part_advance(c);

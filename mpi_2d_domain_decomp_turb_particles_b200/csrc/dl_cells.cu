@@ -583,13 +583,16 @@ __device__ __forceinline__ int leave_nid_of(double y, double z, double pi2)
 }
 
 __global__ void k_periodic_flags(int nps, double pi2, double *px, double *py, double *pz, const int *ref,
-                                 signed char *leave_nid)
+                                 signed char *leave_nid, int *lv_list, int *lv_n)
 {
     int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= nps) return;
     double x = px[d], y = py[d], z = pz[d];
     int nid = leave_nid_of(y, z, pi2);
-    if (nid) leave_nid[ref[d]] = (signed char)nid;
+    if (nid) {
+        leave_nid[ref[d]] = (signed char)nid;
+        lv_list[atomicAdd(lv_n, 1)] = ref[d];
+    }
     if (x >= pi2) x = x - pi2;
     if (x < 0.0) x = x + pi2;
     if (y >= pi2) y = y - pi2;
@@ -600,35 +603,39 @@ __global__ void k_periodic_flags(int nps, double pi2, double *px, double *py, do
 }
 
 // ---- PERIODIC reorder (partlib.f90:866-1133) on the device --------------------------
-// 1. count flagged reference indices per block of 1024, 2. scan, 3. compact them in
-// ascending order, 4. one CTA replays the swap-with-last loop over the departing droplets
-// only (thread 0), appends them in neighbour order, and rewrites ref_of_dev/dev_of_ref.
-__global__ void __launch_bounds__(1024) k_lv_count(int n, const signed char *nid, int *blk)
-{
-    int i = blockIdx.x * 1024 + threadIdx.x;
-    int f = (i < n && nid[i] != 0) ? 1 : 0;
-    int c = __syncthreads_count(f);
-    if (threadIdx.x == 0) blk[blockIdx.x] = c;
-}
+// The kernels that flag departing droplets also append their reference indices to a
+// list.  One CTA then sorts the list (bitonic, in shared memory; a block scan over the
+// flags when more than kSortMax droplets left), drops entries whose flag was cleared
+// since (RELOCATE) and duplicates, replays the swap-with-last loop over the departing
+// droplets only (thread 0), appends them in neighbour order, rewrites
+// ref_of_dev/dev_of_ref and resets the flags and the list.
+constexpr int kSortMax = 4096;
 
-__global__ void __launch_bounds__(1024) k_lv_compact(int n, const signed char *nid, const int *off, int *refs)
+__device__ __forceinline__ int block_excl_scan(int v, int *ws, int &total)
 {
-    __shared__ int wsum[32];
-    const int i = blockIdx.x * 1024 + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const bool f = i < n && nid[i] != 0;
-    unsigned m = __ballot_sync(0xffffffffu, f);
-    if (lane == 0) wsum[w] = __popc(m);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) ws[w] = incl;
     __syncthreads();
     if (w == 0) {
-        int v = wsum[lane], incl = v;
+        const int a = lane < nw ? ws[lane] : 0;
+        int ai = a;
         for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
+            const int t = __shfl_up_sync(0xffffffffu, ai, o);
+            if (lane >= o) ai += t;
         }
-        wsum[lane] = incl - v;
+        ws[lane] = ai - a;
+        if (lane == 31) ws[32] = ai;
     }
     __syncthreads();
-    if (f) refs[off[blockIdx.x] + wsum[w] + __popc(m & ((1u << lane) - 1))] = i;
+    const int ex = ws[w] + incl - v;
+    total = ws[32];
+    __syncthreads();
+    return ex;
 }
 
 // The HDI disturbance velocity pertvel is indexed by reference position and PERIODIC does
@@ -647,14 +654,68 @@ __device__ void keep_by_reference(int m, const int *src_dev, const int *dev_tmp,
         }
 }
 
-__global__ void __launch_bounds__(1024) k_lv_reorder(int n, const int *ktot, const int *P, signed char *nid,
+__global__ void __launch_bounds__(1024) k_lv_reorder(int n, int *lv_list, int *lv_n, int *Pg, signed char *nid,
                                                      int *dep, int *old_ref, int *new_ref, int *dev_tmp,
                                                      int *ref_of_dev, int *dev_of_ref, int *err, void *pt0,
                                                      void *pt1, void *pt2, int pesz, void *ptmp, int *src_dev)
 {
     __shared__ int s_m, s_k;
+    __shared__ int ws[33];
+    __shared__ int skey[kSortMax];
+    __shared__ int sP[kSortMax];
+    const int kraw = *lv_n;
+    int *P;
+    int kk = 0;
+    if (kraw <= kSortMax) {
+        // sort the appended list (padded to a power of two)
+        int np2 = 1;
+        while (np2 < kraw) np2 <<= 1;
+        for (int i = threadIdx.x; i < np2; i += blockDim.x) skey[i] = i < kraw ? lv_list[i] : INT_MAX;
+        __syncthreads();
+        for (int k2 = 2; k2 <= np2; k2 <<= 1)
+            for (int j = k2 >> 1; j > 0; j >>= 1) {
+                for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+                    const int ixj = i ^ j;
+                    if (ixj > i) {
+                        const bool up = (i & k2) == 0;
+                        const int a = skey[i], b = skey[ixj];
+                        if ((a > b) == up) { skey[i] = b; skey[ixj] = a; }
+                    }
+                }
+                __syncthreads();
+            }
+        // keep flagged, distinct entries (4 per thread, in order)
+        const int base = threadIdx.x * 4;
+        int keep[4], cnt = 0;
+        for (int q = 0; q < 4; q++) {
+            const int i = base + q;
+            const int v = i < kraw ? skey[i] : INT_MAX;
+            keep[q] = v != INT_MAX && nid[v] != 0 && (i == 0 || skey[i - 1] != v);
+            cnt += keep[q];
+        }
+        int total;
+        int o = block_excl_scan(cnt, ws, total);
+        for (int q = 0; q < 4; q++)
+            if (keep[q]) sP[o++] = skey[base + q];
+        kk = total;
+        P = sP;
+    } else {
+        // many departures: the flags in reference order, compacted by block scans
+        int off = 0;
+        for (int b = 0; b < n; b += blockDim.x) {
+            const int i = b + threadIdx.x;
+            const int f = (i < n && nid[i] != 0) ? 1 : 0;
+            int total;
+            const int o = block_excl_scan(f, ws, total);
+            if (f) Pg[off + o] = i;
+            off += total;
+        }
+        kk = off;
+        P = Pg;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
-        const int k = *ktot;
+        const int k = kk;
         int lo = 0, hi = k - 1, sum = 0, nf = 0, nd = 0;
         while (lo <= hi) {                 // each pass consumes at least one departing droplet
             const int h = P[lo] + 1;       // 1-based position of the next hole the scan reaches
@@ -704,6 +765,7 @@ __global__ void __launch_bounds__(1024) k_lv_reorder(int n, const int *ktot, con
         dev_of_ref[new_ref[j]] = dev_tmp[j];
     }
     for (int j = threadIdx.x; j < k; j += blockDim.x) nid[P[j]] = 0;
+    if (threadIdx.x == 0) *lv_n = 0;
     __syncthreads();
     if (pesz == 8)
         keep_by_reference<unsigned long long>(m, src_dev, dev_tmp, (unsigned long long *)pt0,
@@ -937,7 +999,7 @@ int launch_periodic(dl_ctx *c)
     if (c->nps > 0) {
         k_periodic_flags<<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(
             c->nps, c->dc.pi2, c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2], c->ref_of_dev,
-            c->leave_nid);
+            c->leave_nid, c->lv_list, c->lv_n);
         DL_CHECK_LAUNCH(c);
     }
     return launch_periodic_reorder(c);
@@ -948,15 +1010,14 @@ int launch_periodic_reorder(dl_ctx *c)
 {
     const int n = c->nps;
     if (n == 0) return 0;
-    const int nblk = dl_blocks(n, 1024);
-    k_lv_count<<<nblk, 1024, 0, c->stream>>>(n, c->leave_nid, c->lv_blk);
-    DL_CHECK_LAUNCH(c);
-    int r = dl_scan(c, c->lv_blk, c->lv_blk, nblk);   // in place: the scan reads before it writes per chunk
-    if (r) return r;
-    k_lv_compact<<<nblk, 1024, 0, c->stream>>>(n, c->leave_nid, c->lv_blk, c->lv_refs);
-    DL_CHECK_LAUNCH(c);
     const int pesz = c->pert[0] ? (int)c->esz : 0;
-    k_lv_reorder<<<1, 1024, 0, c->stream>>>(n, c->lv_blk + nblk, c->lv_refs, c->leave_nid, c->lv_dep, c->lv_old,
+    static bool carve = false;
+    if (!carve) {
+        cudaFuncSetAttribute(k_lv_reorder, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        carve = true;
+    }
+    k_lv_reorder<<<1, 1024, 0, c->stream>>>(n, c->lv_list, c->lv_n, c->lv_refs, c->leave_nid, c->lv_dep, c->lv_old,
                                             c->lv_new, c->lv_dev, c->ref_of_dev, c->dev_of_ref, c->d_err,
                                             c->pert[0], c->pert[1], c->pert[2], pesz, c->pert_tmp, c->lv_src);
     DL_CHECK_LAUNCH(c);

@@ -144,7 +144,7 @@ struct dl_ctx {
     int *n_long;
     // PERIODIC: departing droplets flagged by reference index, then reordered on the device
     signed char *leave_nid;      // [msize] neighbour code 1..8 of a droplet leaving the pencil, else 0
-    int *lv_blk;                 // [nblk + 1] per-1024-block counts -> offsets
+    int *lv_list, *lv_n;         // [msize] departing reference indices appended by the flagging kernels; count
     int *lv_refs;                // [msize] leaving reference indices, ascending
     int *lv_old, *lv_new, *lv_dev, *lv_dep;   // [msize] remap scratch
     int *lv_src;                 // [msize] (HDI) device holding each new reference index before the reorder

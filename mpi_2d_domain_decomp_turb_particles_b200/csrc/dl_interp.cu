@@ -142,6 +142,7 @@ struct InterpArgs {
     double *qx, *qy, *qz;           // new positions (other buffer)
     const int *ref_of_dev;
     signed char *leave_nid;         // PERIODIC departure flags by reference index
+    int *lv_list, *lv_n;            // departing reference indices (appended) and their count
     int *err;                       // device error flags
 };
 
@@ -276,7 +277,11 @@ __device__ __forceinline__ void epilogue_one(const InterpArgs<T> &A, int d, cons
     A.qx[d] = wrap_coord(xn[0], A.pi2);
     A.qy[d] = wrap_coord(xn[1], A.pi2);
     A.qz[d] = wrap_coord(xn[2], A.pi2);
-    if (nid) A.leave_nid[A.ref_of_dev[d]] = (signed char)nid;
+    if (nid) {
+        const int r = A.ref_of_dev[d];
+        A.leave_nid[r] = (signed char)nid;
+        A.lv_list[atomicAdd(A.lv_n, 1)] = r;
+    }
 }
 
 // History, advance, position update, wrap and departure flags of every droplet, with the
@@ -994,11 +999,23 @@ static int launch_interp_t(dl_ctx *c, int comp_lo, int ncomp, int fused)
         A.qx = c->pos[1 - c->pcur][0]; A.qy = c->pos[1 - c->pcur][1]; A.qz = c->pos[1 - c->pcur][2];
         A.ref_of_dev = c->ref_of_dev;
         A.leave_nid = c->leave_nid;
+        A.lv_list = c->lv_list;
+        A.lv_n = c->lv_n;
     }
     constexpr size_t sm = interp_smem<T, BX, BY, BZ, XS, YS, S, MAXD, NG>();
     static_assert(sm <= 227 * 1024, "shared memory budget");
     auto kern = k_interp<T, BX, BY, BZ, XS, YS, S, MAXD, NG, GW>;
     DL_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    static bool carve = false;
+    if (!carve) {
+        // the kernels between two k_interp launches keep the shared-memory carveout that
+        // k_interp needs, so the SMs are not reconfigured at every kernel boundary
+        cudaFuncSetAttribute(k_advance_fused<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        carve = true;
+    }
     const int grid = std::min(c->nbricks, c->num_sms);
     kern<<<grid, (NG * GW + 1) * 32, sm, c->stream>>>(c->tmap, A);
     DL_CHECK_LAUNCH(c);
