@@ -78,12 +78,19 @@ class DropletAdjoint:
         dev = int(hasattr(u, "is_cuda") and u.is_cuda)
         if not dev:
             u = np.ascontiguousarray(u, dtype=np.float64)
+        else:
+            import torch
+            u = u.contiguous()
+            torch.cuda.current_stream(u.device).synchronize()   # the library reads on its own stream
         n, llx = u.shape[1], u.shape[3]
         for c in range(3):
             self._chk(self.lib.dl_adj_set_field(self.h, c + 1, self._ptr(u[c]), llx, llx * n, dev))
 
     def set_droplets(self, x0, tau, radius):
         dev = int(hasattr(x0, "is_cuda") and x0.is_cuda)
+        if dev:
+            import torch
+            torch.cuda.current_stream(x0.device).synchronize()
         if not dev:
             x0 = np.ascontiguousarray(x0, dtype=np.float64)
             tau = np.ascontiguousarray(tau, dtype=np.float64)
@@ -102,6 +109,9 @@ class DropletAdjoint:
             dtau = np.zeros(self.np)
             du = np.zeros((3, self.p.n, self.p.n, llx or self.p.n + 2))
         dev = int(hasattr(dx0, "is_cuda") and dx0.is_cuda)
+        if dev:
+            import torch
+            torch.cuda.current_stream(dx0.device).synchronize()   # outputs allocated by torch
         n = self.p.n
         llx = du.shape[3] if du is not None else n
         self._chk(self.lib.dl_adj_backward(self.h, self._ptr(dx0), self._ptr(dtau), self._ptr(du), llx, llx * n, dev))

@@ -562,6 +562,9 @@ static int part_init_common(dl_ctx *c)
     if (!c->initialized) {
         int r = allocate_state(c);
         if (r) return r;
+        // the zeroing of the new buffers runs on the legacy stream, which the context's
+        // non-blocking stream does not wait for: finish it before any kernel of the context
+        DL_CUDA(c, cudaDeviceSynchronize());
         c->initialized = 1;
     }
     return 0;
@@ -1149,6 +1152,7 @@ extern "C" int dl_get_contacts(dl_ctx *c, int *ids3, double *rec12, int cap, int
     if (ncontact) *ncontact = n;
     if (!ids3 && !rec12) return 0;
     std::vector<ContactRec> cr(n);
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));
     if (n) DL_CUDA(c, cudaMemcpy(cr.data(), c->contacts, sizeof(ContactRec) * n, cudaMemcpyDeviceToHost));
     std::vector<int> refs(c->nps);
     if (c->nps) DL_CUDA(c, cudaMemcpy(refs.data(), c->ref_of_dev, sizeof(int) * c->nps, cudaMemcpyDeviceToHost));

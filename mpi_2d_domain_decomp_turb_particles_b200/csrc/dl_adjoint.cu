@@ -1019,6 +1019,11 @@ extern "C" int dl_adj_create(const dl_adj_params *p, dl_adj **out)
         dl_adj_destroy(a);
         return r;
     }
+    // the buffers were zeroed on the legacy stream; the context's stream does not wait for it
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        dl_adj_destroy(a);
+        return DL_E_CUDA;
+    }
     *out = a;
     return 0;
 }

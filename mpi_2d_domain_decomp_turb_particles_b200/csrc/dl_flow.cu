@@ -300,6 +300,7 @@ struct dl_flow {
     double b[3][5][5][6];
     int iseedf = 0, iyf = 0, ivf[32];
     int64_t launches = 0;
+    cudaEvent_t ev_ready = nullptr, ev_used = nullptr;   // ordering with a droplet context's stream
 };
 
 namespace {
@@ -425,6 +426,9 @@ extern "C" int dl_flow_create(const dl_flow_params *p, dl_flow **out)
     if (cudaSetDevice(p->device) != cudaSuccess) return fail(DL_E_CUDA);
     if (cudaStreamCreateWithFlags(&f->own_stream, cudaStreamNonBlocking) != cudaSuccess) return fail(DL_E_CUDA);
     f->stream = f->own_stream;
+    if (cudaEventCreateWithFlags(&f->ev_ready, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&f->ev_used, cudaEventDisableTiming) != cudaSuccess)
+        return fail(DL_E_CUDA);
     const int64_t n3 = (int64_t)n * n * n;
     if (cudaMalloc(&f->u, sizeof(double2) * 3 * f->G.M) != cudaSuccess ||
         cudaMalloc(&f->nold, sizeof(double2) * 3 * f->G.M) != cudaSuccess ||
@@ -433,8 +437,8 @@ extern "C" int dl_flow_create(const dl_flow_params *p, dl_flow **out)
         cudaMalloc(&f->afor, sizeof(double) * 450) != cudaSuccess ||
         cudaMalloc(&f->spec_part, sizeof(double) * 296 * 1024) != cudaSuccess)
         return fail(DL_E_ALLOC);
-    cudaMemset(f->u, 0, sizeof(double2) * 3 * f->G.M);
-    cudaMemset(f->nold, 0, sizeof(double2) * 3 * f->G.M);
+    cudaMemsetAsync(f->u, 0, sizeof(double2) * 3 * f->G.M, f->stream);
+    cudaMemsetAsync(f->nold, 0, sizeof(double2) * 3 * f->G.M, f->stream);
     int dims[3] = {n, n, n};
     if (cufftPlanMany(&f->c2r, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, 6) != CUFFT_SUCCESS)
         return fail(DL_E_ALLOC);
@@ -457,6 +461,8 @@ extern "C" int dl_flow_destroy(dl_flow *f)
     void *ptrs[] = {f->u, f->nold, f->work, f->phys, f->afor, f->spec_part};
     for (void *q : ptrs)
         if (q) cudaFree(q);
+    if (f->ev_ready) cudaEventDestroy(f->ev_ready);
+    if (f->ev_used) cudaEventDestroy(f->ev_used);
     if (f->own_stream) cudaStreamDestroy(f->own_stream);
     delete f;
     return 0;
@@ -566,10 +572,16 @@ extern "C" int dl_flow_step(dl_flow *f, dl_ctx *droplets)
     FFT(f, cufftExecZ2D(f->c2r, reinterpret_cast<cufftDoubleComplex *>(f->work), f->phys));
     f->phys_valid = 1;
     if (droplets) {
+        // the droplet context converts the velocity on its own stream: order it after the
+        // inverse transform, and order this flow's next writes after the conversion
+        FCUDA(f, cudaEventRecord(f->ev_ready, f->stream));
+        FCUDA(f, cudaStreamWaitEvent(droplets->stream, f->ev_ready, 0));
         for (int c = 0; c < 3; c++) {
             const int r = dl_set_field(droplets, c + 1, f->phys + (3 + c) * n3, n, (int64_t)n * n, 1);
             if (r) return ffail(f, r, std::string("dl_flow_step: dl_set_field: ") + dl_last_error(droplets));
         }
+        FCUDA(f, cudaEventRecord(f->ev_used, droplets->stream));
+        FCUDA(f, cudaStreamWaitEvent(f->stream, f->ev_used, 0));
     }
     k_cross<<<blocks(n3, 256), 256, 0, f->stream>>>(n3, f->phys);
     FCUDA(f, cudaGetLastError());

@@ -451,7 +451,7 @@ int gmres_buffers(dl_ctx *c)
             cudaMalloc(&c->dots, sizeof(double) * (kRedGrid + 2 * (kMaxIter + 4)) + 64) != cudaSuccess)
             return dl_fail(c, DL_E_ALLOC, "HDI_GMRES: cudaMalloc failed");
         c->rf32 = (float *)p;
-        DL_CUDA(c, cudaMemset(c->dots, 0, sizeof(double) * (kRedGrid + 2 * (kMaxIter + 4)) + 64));
+        DL_CUDA(c, cudaMemsetAsync(c->dots, 0, sizeof(double) * (kRedGrid + 2 * (kMaxIter + 4)) + 64, c->stream));
     }
     return 0;
 }

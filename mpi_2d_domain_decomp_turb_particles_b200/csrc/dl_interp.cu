@@ -164,10 +164,12 @@ struct Elems<float> {
 // Field tile of one component of one brick, as one TMA box.  Component c's box starts
 // XS*c cells lower in x and YS*c cells lower in y than component 0's, which moves the
 // three components' copies of a stencil into different banks (corner offset shift CSHIFT)
-// while keeping the TMA x coordinate 16-byte aligned.
-template <typename T, int BX, int BY, int BZ, int XS, int YS>
+// while keeping the TMA x coordinate 16-byte aligned.  The box reaches M cells beyond the
+// brick in y and z (x has 2 below and 1 above by its alignment), so droplets that drifted
+// that far since the last spatial re-sort still read their stencil from the tile.
+template <typename T, int BX, int BY, int BZ, int XS, int YS, int M>
 struct Geo {
-    static constexpr int EX = BX + 8 + 2 * XS, EY = BY + 5 + 2 * YS, EZ = BZ + 5;
+    static constexpr int EX = BX + 8 + 2 * XS, EY = BY + 5 + 2 * YS + 2 * M, EZ = BZ + 5 + 2 * M;
     static constexpr int PLANE = EX * EY;
     static constexpr int VOL = PLANE * EZ;
     static constexpr int BOX_BYTES = VOL * (int)sizeof(T);
@@ -366,11 +368,11 @@ struct GroupAux {
           sizeof(unsigned short) * (R * CAP + MAXD * 3)) + 127) / 128 * 128;
 };
 
-template <typename T, int BX, int BY, int BZ, int XS, int YS, int S, int MAXD, int NG, int GW>
+template <typename T, int BX, int BY, int BZ, int XS, int YS, int M, int S, int MAXD, int NG, int GW>
 __global__ void __launch_bounds__((NG * GW + 1) * 32, 1) k_interp(const __grid_constant__ CUtensorMap tmap,
                                                                     InterpArgs<T> A)
 {
-    using G = Geo<T, BX, BY, BZ, XS, YS>;
+    using G = Geo<T, BX, BY, BZ, XS, YS, M>;
     using X = GroupAux<T, MAXD>;
     constexpr int R = Elems<T>::R;
     constexpr int NSW = X::NSW;
@@ -412,7 +414,7 @@ __global__ void __launch_bounds__((NG * GW + 1) * 32, 1) k_interp(const __grid_c
                     mbar_arrive_expect_tx(&full[s], (unsigned)G::BOX_BYTES);
                     // padded coordinates of the box origin (grid origin + DL_PAD_LO)
                     tma_load_4d(stage + s * G::STAGE_ELEMS, &tmap, &full[s], bxi * BX - XS * c,
-                                byi * BY + 2 - YS * c, bzi * BZ + 2, c);
+                                byi * BY + 2 - YS * c - M, bzi * BZ + 2 - M, c);
                 }
             }
             // wait (bounded) for the copies still in flight before leaving
@@ -473,8 +475,9 @@ __global__ void __launch_bounds__((NG * GW + 1) * 32, 1) k_interp(const __grid_c
                 // stencil corner in component 0's tile (origin bxi*BX-4, byi*BY-2, bzi*BZ-2); in
                 // component c's tile the same stencil starts CSHIFT*c words further on
                 const int lx = node[0] - bxi * BX + 2, ly = node[1] - byi * BY, lz = node[2] - bzi * BZ;
-                const bool in = lx >= 0 && lx + 2 * XS + 5 < G::EX && ly >= 0 && ly < BY && lz >= 0 && lz < BZ;
-                const int cr = in ? (lz * G::EY + ly) * G::EX + lx : -1;
+                const bool in = lx >= 0 && lx + 2 * XS + 5 < G::EX && ly >= -M && ly < BY + M && lz >= -M &&
+                                lz < BZ + M;
+                const int cr = in ? ((lz + M) * G::EY + (ly + M)) * G::EX + lx : -1;
                 scorner[i] = cr;
                 // bucket this droplet's tasks by starting bank (stages start on 128-byte
                 // boundaries, so the bank is set by the offset alone)
@@ -587,10 +590,10 @@ __global__ void __launch_bounds__((NG * GW + 1) * 32, 1) k_interp(const __grid_c
     }
 }
 
-template <typename T, int BX, int BY, int BZ, int XS, int YS, int S, int MAXD, int NG>
+template <typename T, int BX, int BY, int BZ, int XS, int YS, int M, int S, int MAXD, int NG>
 constexpr size_t interp_smem()
 {
-    using G = Geo<T, BX, BY, BZ, XS, YS>;
+    using G = Geo<T, BX, BY, BZ, XS, YS, M>;
     return (size_t)S * G::STAGE_BYTES + 128 + NG * GroupAux<T, MAXD>::BYTES;
 }
 
@@ -848,9 +851,9 @@ __global__ void k_mean_vel(int nps, const T *ux, const T *uy, const T *uz, const
 // brick configurations (cells) per precision
 // brick / pipeline configuration per precision: brick cells, component shifts (bank
 // spreading), TMA stages, droplets per chunk, consumer groups x warps per group
-constexpr int F32_BX = 16, F32_BY = 16, F32_BZ = 8, F32_XS = 0, F32_YS = 1, F32_S = 6, F32_MAXD = 256;
+constexpr int F32_BX = 16, F32_BY = 16, F32_BZ = 6, F32_XS = 0, F32_YS = 1, F32_M = 1, F32_S = 6, F32_MAXD = 256;
 constexpr int F32_NG = 2, F32_GW = 6;
-constexpr int F64_BX = 16, F64_BY = 8, F64_BZ = 4, F64_XS = 2, F64_YS = 0, F64_S = 6, F64_MAXD = 64;
+constexpr int F64_BX = 16, F64_BY = 8, F64_BZ = 4, F64_XS = 2, F64_YS = 0, F64_M = 0, F64_S = 6, F64_MAXD = 64;
 constexpr int F64_NG = 2, F64_GW = 6;
 
 template <typename T>
@@ -949,10 +952,10 @@ static int make_tmap(dl_ctx *c, int box_x, int box_y, int box_z)
     return 0;
 }
 
-template <typename T, int BX, int BY, int BZ, int XS, int YS, int S, int MAXD, int NG, int GW>
+template <typename T, int BX, int BY, int BZ, int XS, int YS, int M, int S, int MAXD, int NG, int GW>
 static int launch_interp_t(dl_ctx *c, int comp_lo, int ncomp, int fused)
 {
-    using G = Geo<T, BX, BY, BZ, XS, YS>;
+    using G = Geo<T, BX, BY, BZ, XS, YS, M>;
     if (c->tmap_base != c->fpad) {
         int r = make_tmap(c, G::EX, G::EY, G::EZ);
         if (r) return r;
@@ -1002,9 +1005,9 @@ static int launch_interp_t(dl_ctx *c, int comp_lo, int ncomp, int fused)
         A.lv_list = c->lv_list;
         A.lv_n = c->lv_n;
     }
-    constexpr size_t sm = interp_smem<T, BX, BY, BZ, XS, YS, S, MAXD, NG>();
+    constexpr size_t sm = interp_smem<T, BX, BY, BZ, XS, YS, M, S, MAXD, NG>();
     static_assert(sm <= 227 * 1024, "shared memory budget");
-    auto kern = k_interp<T, BX, BY, BZ, XS, YS, S, MAXD, NG, GW>;
+    auto kern = k_interp<T, BX, BY, BZ, XS, YS, M, S, MAXD, NG, GW>;
     DL_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     static bool carve = false;
     if (!carve) {
@@ -1031,9 +1034,9 @@ int launch_interp(dl_ctx *c, int icpt, int fused)
     if (c->nps == 0) return 0;
     int lo = icpt > 0 ? icpt - 1 : 0, nc = icpt > 0 ? 1 : 3;
     if (c->mixed)
-        return launch_interp_t<float, F32_BX, F32_BY, F32_BZ, F32_XS, F32_YS, F32_S, F32_MAXD, F32_NG, F32_GW>(
+        return launch_interp_t<float, F32_BX, F32_BY, F32_BZ, F32_XS, F32_YS, F32_M, F32_S, F32_MAXD, F32_NG, F32_GW>(
             c, lo, nc, fused);
-    return launch_interp_t<double, F64_BX, F64_BY, F64_BZ, F64_XS, F64_YS, F64_S, F64_MAXD, F64_NG, F64_GW>(
+    return launch_interp_t<double, F64_BX, F64_BY, F64_BZ, F64_XS, F64_YS, F64_M, F64_S, F64_MAXD, F64_NG, F64_GW>(
         c, lo, nc, fused);
 }
 

@@ -47,6 +47,10 @@ class Flow:
         dev = int(hasattr(u, "is_cuda") and u.is_cuda)
         if not dev:
             u = np.ascontiguousarray(u, dtype=np.float64)
+        else:
+            import torch
+            u = u.contiguous()
+            torch.cuda.current_stream(u.device).synchronize()   # the library reads on its own stream
         ptr = C.c_void_p(u.data_ptr()) if dev else u.ctypes.data_as(C.c_void_p)
         llx = u.shape[3]
         self._chk(self.lib.dl_flow_set_velocity(self.h, ptr, llx, llx * self.n, dev))

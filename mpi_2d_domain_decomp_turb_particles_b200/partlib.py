@@ -182,7 +182,9 @@ class Partlib:
         C-contiguous float64 numpy array (copied to the device) or a CUDA torch tensor
         (used in place; keep it alive)."""
         if hasattr(v, "is_cuda") and v.is_cuda:
+            import torch
             assert v.dtype.is_floating_point and v.element_size() == 8 and v.is_contiguous()
+            torch.cuda.current_stream(v.device).synchronize()   # the library reads on its own stream
             nz, ny, px = v.shape
             self._fields[icpt - 1] = v
             self._chk(self.lib.dl_set_field(self.h, icpt, C.c_void_p(v.data_ptr()), px, px * ny, 1))
@@ -198,8 +200,10 @@ class Partlib:
     def set_field_padded(self, t):
         """A CUDA tensor in the halo-padded layout of ``field_padded_shape`` (float32 for the
         mixed path, float64 for FP64), e.g. written by the on-device flow solver."""
+        import torch
         assert t.is_cuda and t.is_contiguous()
         assert t.element_size() == (4 if self.params.precision == "mixed" else 8)
+        torch.cuda.current_stream(t.device).synchronize()   # the library reads on its own stream
         self._fields[0] = t
         self._chk(self.lib.dl_set_field_padded(self.h, C.c_void_p(t.data_ptr())))
 
