@@ -173,6 +173,12 @@ int dl_complete_ypn(dl_ctx *ctx);                           /* COMPLETE_YPN(id),
 /* MEAN_VEL(id), partlib.f90:1889-1980: out = vpmean(3,nset), vpvar(3,nset),
  * vpabs(3,nset), vphoriz(nset), vpxyz(nset) (11*nset doubles, already reduced). */
 int dl_mean_vel(dl_ctx *ctx, double *out);
+/* MEAN_VEL inside dl_particle_step (turb.f90:582): on steps with istep mod ieout == 0,
+ * after PART_ADVANCE and before COLLISION_DET.  0 (the default) turns it off. */
+int dl_set_mean_vel_interval(dl_ctx *ctx, int ieout);
+/* The MEAN_VEL vector (layout of dl_mean_vel) of the last dl_particle_step that computed
+ * it, and that step's istep (0 when none has). */
+int dl_get_step_mean_vel(dl_ctx *ctx, double *out, int *istep);
 int dl_collision_det(dl_ctx *ctx, dl_coll_report *rep);     /* COLLISION_DET(id), partlib.f90:1166-1846 */
 int dl_update_part_position(dl_ctx *ctx);                   /* UPDATE_PART_POSITION(id), partlib.f90:730-757 */
 int dl_relocate(dl_ctx *ctx);                               /* RELOCATE(id), partlib.f90:1984-2012 */
@@ -207,7 +213,9 @@ int dl_get_removal_list(dl_ctx *ctx, int *removepart, int cap, int *ncoll);
  * 1..8 whose source is src2.  Unordered. */
 int dl_get_pairs(dl_ctx *ctx, int *rows4, int cap, int *npairs);
 /* Contact-shell records (partlib.f90:1431-1438): ints (ih1, src2, jid2) and 12 doubles
- * (index1, index2, va(3), vb(3), xd(3), Wr) per record.  Unordered. */
+ * (index1, index2, va(3), vb(3), xd(3), Wr) per record, in the reference's detection
+ * order (ih1 ascending, neighbour cell, ih2 descending in ypn order), the order of the
+ * Vp11/Vp12/Vp22 statistics files (partlib.f90:1707-1740). */
 int dl_get_contacts(dl_ctx *ctx, int *ids3, double *rec12, int cap, int *ncontact);
 /* collist(20, ntotpair) in the reference's detection order (partlib.f90:1557-1562). */
 int dl_get_collist(dl_ctx *ctx, double *collist20, int cap, int *ntotpair);

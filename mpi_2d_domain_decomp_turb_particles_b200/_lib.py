@@ -126,6 +126,8 @@ SIGNATURES = {
     "dl_get_histograms": (C.c_int, [_vp, C.c_int, _ip, _dp]),
     "dl_get_collision_counts": (C.c_int, [_vp, _ip, _ip]),
     "dl_get_removal_list": (C.c_int, [_vp, _ip, C.c_int, _ip]),
+    "dl_set_mean_vel_interval": (C.c_int, [_vp, C.c_int]),
+    "dl_get_step_mean_vel": (C.c_int, [_vp, _dp, _ip]),
     "dl_get_pairs": (C.c_int, [_vp, _ip, C.c_int, _ip]),
     "dl_get_contacts": (C.c_int, [_vp, _ip, _dp, C.c_int, _ip]),
     "dl_get_collist": (C.c_int, [_vp, _dp, C.c_int, _ip]),

@@ -907,6 +907,22 @@ extern "C" int dl_mean_vel(dl_ctx *c, double *out)
     return r;
 }
 
+extern "C" int dl_set_mean_vel_interval(dl_ctx *c, int ieout)
+{
+    CHECK_INIT(c);
+    if (ieout < 0) return dl_fail(c, DL_E_ARG, "dl_set_mean_vel_interval: ieout < 0");
+    c->mv_every = ieout;
+    return 0;
+}
+
+extern "C" int dl_get_step_mean_vel(dl_ctx *c, double *out, int *istep)
+{
+    CHECK_INIT(c);
+    if (istep) *istep = c->mv_istep;
+    if (out) memcpy(out, c->mv_out, sizeof(double) * 11 * c->dc.nset);
+    return 0;
+}
+
 extern "C" int dl_collision_det(dl_ctx *c, dl_coll_report *rep)
 {
     CHECK_INIT(c);
@@ -1158,11 +1174,25 @@ extern "C" int dl_get_contacts(dl_ctx *c, int *ids3, double *rec12, int cap, int
     if (c->nps) DL_CUDA(c, cudaMemcpy(refs.data(), c->ref_of_dev, sizeof(int) * c->nps, cudaMemcpyDeviceToHost));
     std::vector<Ghost> gh(c->nghost);
     if (c->nghost) DL_CUDA(c, cudaMemcpy(gh.data(), c->ghosts, sizeof(Ghost) * c->nghost, cudaMemcpyDeviceToHost));
+    // Detection order of COLLISION_DET (partlib.f90:1269-1568): ih1 ascending, then the
+    // neighbour cell (loopkey ascending), then down the cell's linked list, i.e. ih2
+    // descending in ypn order (owned droplets by reference index, ghost g at nps + g).
+    const int nps = c->nps;
+    auto ypn = [&](int e) { return e < nps ? refs[e] : e; };
+    std::vector<int> ord(n);
+    for (int i = 0; i < n; i++) ord[i] = i;
+    std::sort(ord.begin(), ord.end(), [&](int x, int y) {
+        const ContactRec &p = cr[x], &q = cr[y];
+        if (refs[p.a] != refs[q.a]) return refs[p.a] < refs[q.a];
+        if (p.loopkey != q.loopkey) return p.loopkey < q.loopkey;
+        return ypn(p.b) > ypn(q.b);
+    });
     for (int i = 0; i < std::min(n, cap); i++) {
-        int src = cr[i].b < c->nps ? cr[i].b : gh[cr[i].b - c->nps].src;
-        int jid = cr[i].b < c->nps ? 0 : gh[cr[i].b - c->nps].jid;
-        if (ids3) { ids3[3 * i] = refs[cr[i].a] + 1; ids3[3 * i + 1] = refs[src] + 1; ids3[3 * i + 2] = jid; }
-        if (rec12) memcpy(rec12 + 12 * i, cr[i].rec, sizeof(double) * 12);
+        const ContactRec &r = cr[ord[i]];
+        int src = r.b < nps ? r.b : gh[r.b - nps].src;
+        int jid = r.b < nps ? 0 : gh[r.b - nps].jid;
+        if (ids3) { ids3[3 * i] = refs[r.a] + 1; ids3[3 * i + 1] = refs[src] + 1; ids3[3 * i + 2] = jid; }
+        if (rec12) memcpy(rec12 + 12 * i, r.rec, sizeof(double) * 12);
     }
     return n > cap ? dl_fail(c, DL_E_CAPACITY, "dl_get_contacts: buffer too small") : 0;
 }
@@ -1371,6 +1401,11 @@ extern "C" int dl_particle_step(dl_ctx *c, dl_coll_report *coll, dl_gmres_report
         if (r) return r;
         r = dl_part_advance(c);
         if (r) return r;
+    }
+    if (c->mv_every > 0 && c->istep % c->mv_every == 0) {   // turb.f90:582
+        r = dl_mean_vel(c, c->mv_out);
+        if (r) return r;
+        c->mv_istep = c->istep;
     }
     cudaEventRecord(c->ev[3], c->stream);
     dl_coll_report rep;

@@ -176,6 +176,9 @@ struct dl_ctx {
 
     // ---- MEAN_VEL ----
     double *mv_acc;
+    int mv_every;                // dl_particle_step computes MEAN_VEL when istep % mv_every == 0
+    int mv_istep;                // istep of the last such call (0: none)
+    double mv_out[11 * 10];
 
     // ---- HDI (allocated on first use) ----
     int *nei_cnt, *nei_start;    // CSR over owned droplets (device order)

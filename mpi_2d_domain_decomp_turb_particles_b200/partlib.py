@@ -267,6 +267,17 @@ class Partlib:
         self._chk(self.lib.dl_mean_vel(self.h, _dptr(out)))
         return out
 
+    def set_mean_vel_interval(self, ieout: int):
+        """particle_step runs MEAN_VEL on steps with istep % ieout == 0 (turb.f90:582)."""
+        self._chk(self.lib.dl_set_mean_vel_interval(self.h, int(ieout)))
+
+    def step_mean_vel(self):
+        """(istep, MEAN_VEL vector) of the last particle_step that computed it."""
+        out = np.zeros(11 * self.nset)
+        ist = C.c_int(0)
+        self._chk(self.lib.dl_get_step_mean_vel(self.h, _dptr(out), C.byref(ist)))
+        return ist.value, out
+
     def collision_det(self) -> CollReport:
         r = CollReport()
         self._chk(self.lib.dl_collision_det(self.h, C.byref(r)))

@@ -146,9 +146,15 @@ def _compare_collision(g, o, rep, exact_sums):
     nset = o.geti("nset")
     assert np.array_equal(ct.T.ravel(), o.arr("colltype", np.int32))
     assert np.array_equal(nir.T.ravel(), o.arr("nir", np.int32))
+    # contact-shell records in the reference's detection order (the Vp*.dat line order)
     ids, rec = g.contacts()
     oc = o.contacts()
-    assert sorted(map(tuple, ids.tolist())) == sorted((c[0], c[1], c[2]) for c in oc)
+    assert ids.tolist() == [[c[0], c[1], c[2]] for c in oc]
+    orec = np.array([c[3] for c in oc]).reshape(-1, 12)
+    if exact_sums:
+        assert np.array_equal(rec, orec)
+    else:
+        assert np.array_equal(rec[:, :2], orec[:, :2])
 
 
 def test_particle_steps_separate_calls_fp64_match_oracle():
