@@ -198,6 +198,27 @@ int dl_particle_step(dl_ctx *ctx, dl_coll_report *coll, dl_gmres_report *gmres);
 int dl_update_step(dl_ctx *ctx);
 
 /* ---------------------------------------------------------------------------------------
+ * Growth diagnostics (turb.f90:557-562, 596-598: every 100th step once droplets grow).
+ * FP64 in both precisions; sums over droplets are fixed-shape reductions (repeatable,
+ * rounding-different from the reference's sequential sums).
+ * ------------------------------------------------------------------------------------- */
+/* INTERP_SCALAR(v, jjj), partlib.f90:4101-4290: the INTERPOLATE stencil with the
+ * PREPARE_INTERP weights of the current positions over the FP64 scalar field v (layout
+ * of dl_set_field), negative values replaced by 0.00001; jjj = 1 fills enst_p, 2 disp_p.
+ * The values follow the droplets until the next call that moves or renumbers them. */
+int dl_interp_scalar(dl_ctx *ctx, const double *v, int64_t pitch_y, int64_t pitch_z, int jjj, int on_device);
+/* enst_p (jjj = 1) or disp_p (jjj = 2) in reference order, nps values. */
+int dl_get_scalar(dl_ctx *ctx, int jjj, double *out);
+/* LOCAL_St_AVG, partlib.f90:4294-4330: mean and largest-droplet local Stokes numbers
+ * from disp_p, both divided by St of radius(1); nproc = 1, npart_t = nps. */
+int dl_local_st_avg(dl_ctx *ctx, double *st_avg, double *st_max_avg);
+/* SIZE_DIST_LOGARITHMIC, partlib.f90:3873-3933: sizebin(1:360) and the scaled
+ * mdensbin(1:360) of the mass ratio (r/radius(1))^3 on a 2^(1/32) geometric grid. */
+int dl_size_dist_log(dl_ctx *ctx, int *sizebin360, double *mdensbin360);
+/* SIZE_AVG, partlib.f90:3937-3972: r_avg and r_max_avg in units of radius(1). */
+int dl_size_avg(dl_ctx *ctx, double *r_avg, double *r_max_avg);
+
+/* ---------------------------------------------------------------------------------------
  * Statistics (COLLISION_DET outputs), reference layouts
  * ------------------------------------------------------------------------------------- */
 /* Accumulated histograms (nset, nset, 0:nbin-1) as written on the last 5-step boundary
@@ -283,6 +304,11 @@ int dl_flow_step(dl_flow *f, dl_ctx *droplets);
 const double *dl_flow_velocity(dl_flow *f, int icpt);
 /* energy per shell ik = int(|k| + 0.5), ik = 0..nshell-1 (kx = 0 modes count half) */
 int dl_flow_spectrum(dl_flow *f, double *ek, int nshell);
+/* DISSIP, partlib.f90:3976-4082: the local dissipation rate 2 nu S_ij S_ij of the current
+ * spectral velocity (the state the next dl_flow_step starts from, as turb.f90:532 calls
+ * it before that step's transforms), physical, n^3 doubles, x fastest.  *field is a
+ * device pointer valid until the next call or dl_flow_destroy. */
+int dl_flow_dissipation(dl_flow *f, const double **field);
 
 /* ---------------------------------------------------------------------------------------
  * Droplet adjoint (no counterpart in the reference)

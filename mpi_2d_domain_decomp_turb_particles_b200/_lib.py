@@ -127,6 +127,11 @@ SIGNATURES = {
     "dl_get_collision_counts": (C.c_int, [_vp, _ip, _ip]),
     "dl_get_removal_list": (C.c_int, [_vp, _ip, C.c_int, _ip]),
     "dl_set_mean_vel_interval": (C.c_int, [_vp, C.c_int]),
+    "dl_interp_scalar": (C.c_int, [_vp, _vp, C.c_int64, C.c_int64, C.c_int, C.c_int]),
+    "dl_get_scalar": (C.c_int, [_vp, C.c_int, _dp]),
+    "dl_local_st_avg": (C.c_int, [_vp, _dp, _dp]),
+    "dl_size_dist_log": (C.c_int, [_vp, _ip, _dp]),
+    "dl_size_avg": (C.c_int, [_vp, _dp, _dp]),
     "dl_get_step_mean_vel": (C.c_int, [_vp, _dp, _ip]),
     "dl_get_pairs": (C.c_int, [_vp, _ip, C.c_int, _ip]),
     "dl_get_contacts": (C.c_int, [_vp, _ip, _dp, C.c_int, _ip]),
@@ -148,6 +153,7 @@ SIGNATURES = {
     "dl_flow_step": (C.c_int, [_vp, _vp]),
     "dl_flow_velocity": (C.c_void_p, [_vp, C.c_int]),
     "dl_flow_spectrum": (C.c_int, [_vp, _dp, C.c_int]),
+    "dl_flow_dissipation": (C.c_int, [_vp, C.POINTER(C.c_void_p)]),
     "dl_adj_create": (C.c_int, [C.POINTER(AdjParams), C.POINTER(C.c_void_p)]),
     "dl_adj_destroy": (C.c_int, [_vp]),
     "dl_adj_last_error": (C.c_char_p, [_vp]),

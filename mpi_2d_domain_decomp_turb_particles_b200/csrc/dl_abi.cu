@@ -447,6 +447,7 @@ extern "C" int dl_destroy(dl_ctx *c)
     F(c->nei_cnt); F(c->nei_start); F(c->nei_idx); F(c->nei_coef); F(c->nei_coef64); F(c->overlap_flag);
     F(c->kry); F(c->xg); F(c->rg); F(c->bg64); F(c->tmp64); F(c->wv); F(c->xt); F(c->dots);
     F(c->nei_fill); F(c->nei_blk); F(c->nei_key); F(c->rf32);
+    F(c->scal[0]); F(c->scal[1]); F(c->gr_part); F(c->gr_bins); F(c->gr_mdens); F(c->scal_field);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     for (int i = 0; i < 2 * dl_ctx::NTEV; i++)
@@ -820,12 +821,6 @@ static int maybe_resort(dl_ctx *c)
     if (c->steps_since_sort >= c->resort_interval || !c->sorted) return launch_brick_sort(c);
     return 0;
 }
-
-#define CHECK_INIT(c)                                                                   \
-    do {                                                                                \
-        if (!(c)) return DL_E_ARG;                                                      \
-        if (!(c)->initialized) return dl_fail((c), DL_E_STATE, "call dl_part_init first"); \
-    } while (0)
 
 extern "C" int dl_prepare_interp(dl_ctx *c)
 {

@@ -301,6 +301,11 @@ struct dl_flow {
     int iseedf = 0, iyf = 0, ivf[32];
     int64_t launches = 0;
     cudaEvent_t ev_ready = nullptr, ev_used = nullptr;   // ordering with a droplet context's stream
+    // DISSIP (allocated on first use): one-component inverse plan and buffers
+    cufftHandle c2r1 = 0;
+    bool have_c2r1 = false;
+    double2 *diss_spec = nullptr;
+    double *diss_phys = nullptr, *diss = nullptr;
 };
 
 namespace {
@@ -390,6 +395,45 @@ void stochastic_amplitudes(dl_flow *f, double *a /* [3][5][5][6] */)
     }
 }
 
+// DISSIP (partlib.f90:3976-4082): the spectral strain component `which` of u^
+// (0: e12, 1: e23, 2: e31, 3: e11, 4: e22, 5: e33).  k*u then multiplication by i as
+// the reference's (re, im) -> (-im, re) swap; off-diagonal terms 0.5*(a + b).
+__global__ void k_strain(Grid G, const double2 *__restrict__ u, int which, double2 *__restrict__ out)
+{
+    const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= G.M) return;
+    int x, y, z;
+    double kx, ky, kz;
+    mode_of(G, m, x, y, z, kx, ky, kz);
+    const double2 ux = u[m], uy = u[G.M + m], uz = u[2 * G.M + m];
+    auto ik = [](double k, double2 v) { return make_double2(-(k * v.y), k * v.x); };
+    double2 r;
+    switch (which) {
+    case 0: { double2 a = ik(ky, ux), b = ik(kx, uy); r = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y + b.y)); break; }
+    case 1: { double2 a = ik(kz, uy), b = ik(ky, uz); r = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y + b.y)); break; }
+    case 2: { double2 a = ik(kx, uz), b = ik(kz, ux); r = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y + b.y)); break; }
+    case 3: r = ik(kx, ux); break;
+    case 4: r = ik(ky, uy); break;
+    default: r = ik(kz, uz); break;
+    }
+    out[m] = r;
+}
+
+// edissip = 2 t12^2 + 2 t23^2 + 2 t31^2 + t11^2 + t22^2 + t33^2, then 2 nu edissip,
+// accumulated in the reference's order (partlib.f90:4007-4080).
+__global__ void k_dissip_acc(int64_t n3, const double *__restrict__ t, int which, double nu, double *__restrict__ e)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n3) return;
+    const double v = t[i];
+    double a;
+    if (which == 0) a = 2.0 * v * v;
+    else if (which < 3) a = e[i] + 2.0 * v * v;
+    else a = e[i] + v * v;
+    if (which == 5) a = 2.0 * nu * a;
+    e[i] = a;
+}
+
 int finish(dl_flow *f)
 {
     k_finish<<<blocks(f->G.M, 256), 256, 0, f->stream>>>(f->G, f->u, f->work);
@@ -458,7 +502,8 @@ extern "C" int dl_flow_destroy(dl_flow *f)
     if (f->own_stream) cudaStreamSynchronize(f->own_stream);
     if (f->have_c2r) cufftDestroy(f->c2r);
     if (f->have_r2c) cufftDestroy(f->r2c);
-    void *ptrs[] = {f->u, f->nold, f->work, f->phys, f->afor, f->spec_part};
+    if (f->have_c2r1) cufftDestroy(f->c2r1);
+    void *ptrs[] = {f->u, f->nold, f->work, f->phys, f->afor, f->spec_part, f->diss_spec, f->diss_phys, f->diss};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     if (f->ev_ready) cudaEventDestroy(f->ev_ready);
@@ -618,6 +663,34 @@ extern "C" const double *dl_flow_velocity(dl_flow *f, int icpt)
 {
     if (!f || icpt < 1 || icpt > 3 || !f->phys_valid) return nullptr;
     return f->phys + (int64_t)(2 + icpt) * f->G.n * f->G.n * f->G.n;
+}
+
+extern "C" int dl_flow_dissipation(dl_flow *f, const double **field)
+{
+    if (!f || !field) return DL_E_ARG;
+    *field = nullptr;
+    if (!f->state_set) return ffail(f, DL_E_STATE, "dl_flow_dissipation: set the velocity first");
+    const int n = f->G.n;
+    const int64_t n3 = (int64_t)n * n * n;
+    if (!f->diss) {
+        if (cudaMalloc(&f->diss_spec, sizeof(double2) * f->G.M) != cudaSuccess ||
+            cudaMalloc(&f->diss_phys, sizeof(double) * n3) != cudaSuccess ||
+            cudaMalloc(&f->diss, sizeof(double) * n3) != cudaSuccess)
+            return ffail(f, DL_E_ALLOC, "dl_flow_dissipation: buffers");
+        FFT(f, cufftPlan3d(&f->c2r1, n, n, n, CUFFT_Z2D));
+        f->have_c2r1 = true;
+    }
+    FFT(f, cufftSetStream(f->c2r1, f->stream));
+    for (int w = 0; w < 6; w++) {
+        k_strain<<<blocks(f->G.M, 256), 256, 0, f->stream>>>(f->G, f->u, w, f->diss_spec);
+        FCUDA(f, cudaGetLastError());
+        FFT(f, cufftExecZ2D(f->c2r1, reinterpret_cast<cufftDoubleComplex *>(f->diss_spec), f->diss_phys));
+        k_dissip_acc<<<blocks(n3, 256), 256, 0, f->stream>>>(n3, f->diss_phys, w, f->p.nu, f->diss);
+        FCUDA(f, cudaGetLastError());
+        f->launches += 2;
+    }
+    *field = f->diss;
+    return 0;
 }
 
 extern "C" int dl_flow_spectrum(dl_flow *f, double *ek, int nshell)

@@ -174,6 +174,14 @@ struct dl_ctx {
     std::vector<double> collist; // collist(20, ntotpair) (host)
     std::vector<int> pairs_host; // rows (ih1, src2, jid2, type)
 
+    // ---- growth diagnostics (allocated on first use) ----
+    double *scal[2];             // enst_p, disp_p of INTERP_SCALAR, device order
+    double *gr_part;             // per-block partial sums of LOCAL_St_AVG / SIZE_AVG
+    int *gr_bins;                // SIZE_DIST_LOGARITHMIC counts [360]
+    double *gr_mdens;            // and mass densities [360]
+    double *scal_field;          // device copy of a host scalar field
+    size_t scal_field_cap;
+
     // ---- MEAN_VEL ----
     double *mv_acc;
     int mv_every;                // dl_particle_step computes MEAN_VEL when istep % mv_every == 0
@@ -231,6 +239,11 @@ int dl_fail(dl_ctx *c, int code, const std::string &msg);
         (ctx)->launches++;                   \
         DL_CUDA(ctx, cudaGetLastError());    \
     } while (0)
+#define CHECK_INIT(c)                                                                   \
+    do {                                                                                \
+        if (!(c)) return DL_E_ARG;                                                      \
+        if (!(c)->initialized) return dl_fail((c), DL_E_STATE, "call dl_part_init first"); \
+    } while (0)
 
 // ---------------------------------------------------------------------------------------
 // Kernel launchers implemented in the .cu files
@@ -245,6 +258,7 @@ int launch_advance(dl_ctx *c);
 int launch_update_position(dl_ctx *c, int track_leave);
 int launch_convert_field(dl_ctx *c, int icpt);
 int launch_mean_vel(dl_ctx *c, double *host_out);
+int launch_interp_scalar(dl_ctx *c, const double *v, int64_t pitch_y, int64_t pitch_z, double *out);
 // dl_cells.cu
 int launch_headlist(dl_ctx *c, double dist);
 int launch_collision(dl_ctx *c, dl_coll_report *rep);

@@ -1191,3 +1191,48 @@ int launch_mean_vel(dl_ctx *c, double *host_out)
 {
     return c->mixed ? mean_vel_t<float>(c, host_out) : mean_vel_t<double>(c, host_out);
 }
+
+// ---------------------------------------------------------------------------------------
+// INTERP_SCALAR (partlib.f90:4101-4290): the PREPARE_INTERP weights of the current
+// positions and the 6x6x6 stencil of INTERPOLATE over an FP64 scalar field read straight
+// from global memory (x outer, y, z inner; v*bx*by*bz left to right), negative results
+// replaced by 0.00001.  Called every 100th step of a growth run: plain loads, no tiles.
+// ---------------------------------------------------------------------------------------
+__global__ void k_interp_scalar(int nps, const double *__restrict__ px, const double *__restrict__ py,
+                                const double *__restrict__ pz, double dx, int n, const double *__restrict__ v,
+                                int64_t fy, int64_t fz, double *__restrict__ out)
+{
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= nps) return;
+    const double pos[3] = {px[d], py[d], pz[d]};
+    double w[3][6];
+    int node[3];
+    for (int k = 0; k < 3; k++) {
+        double z;
+        node[k] = node_frac(pos[k], dx, &z);
+        lagrange6(z, w[k]);
+    }
+    int64_t oy[6], oz[6];
+    int ix[6];
+    for (int q = 0; q < 6; q++) {
+        ix[q] = wrapi(node[0] - 2 + q, n);
+        oy[q] = fy * wrapi(node[1] - 2 + q, n);
+        oz[q] = fz * wrapi(node[2] - 2 + q, n);
+    }
+    double acc = 0.0;
+    for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 6; b++)
+            for (int c = 0; c < 6; c++) acc = acc + v[ix[a] + oy[b] + oz[c]] * w[0][a] * w[1][b] * w[2][c];
+    if (acc < 0.0) acc = 0.00001;
+    out[d] = acc;
+}
+
+int launch_interp_scalar(dl_ctx *c, const double *v, int64_t pitch_y, int64_t pitch_z, double *out)
+{
+    if (c->nps == 0) return 0;
+    k_interp_scalar<<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(
+        c->nps, c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2], c->dc.dx, c->dc.n, v, pitch_y, pitch_z,
+        out);
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}

@@ -94,6 +94,25 @@ class Flow:
         """The last step's physical velocity as a (3, n, n, n) numpy array (copy)."""
         return np.stack([t.cpu().numpy() for t in self.velocity_tensors()])
 
+    def dissipation_tensor(self):
+        """DISSIP (partlib.f90:3976-4082) of the current spectral velocity: the local
+        dissipation rate as an (n, n, n) float64 CUDA tensor viewing the flow's buffer
+        (valid until the next call).  Call it before the step it belongs to."""
+        import torch
+        p = C.c_void_p()
+        self._chk(self.lib.dl_flow_dissipation(self.h, C.byref(p)))
+        self._chk(self.lib.dl_flow_sync(self.h))
+        n = self.n
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (n, n, n), "typestr": "<f8", "data": (p.value, False),
+                                        "version": 3, "strides": None}
+        return torch.as_tensor(_View(), device="cuda")
+
+    def dissipation(self):
+        """DISSIP as an (n, n, n) numpy array (copy)."""
+        return self.dissipation_tensor().cpu().numpy()
+
     def spectrum(self, nshell):
         e = np.zeros(nshell)
         self._chk(self.lib.dl_flow_spectrum(self.h, e.ctypes.data_as(C.POINTER(C.c_double)), nshell))

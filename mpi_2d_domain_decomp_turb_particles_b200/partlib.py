@@ -267,6 +267,43 @@ class Partlib:
         self._chk(self.lib.dl_mean_vel(self.h, _dptr(out)))
         return out
 
+    # -- growth diagnostics (turb.f90:557-562, 596-598) -----------------------------------
+    def interp_scalar(self, v, jjj: int = 2):
+        """INTERP_SCALAR (partlib.f90:4101-4290) of a (nz, ny, llx) float64 field, numpy
+        or CUDA tensor; jjj = 1 fills enst_p, 2 disp_p."""
+        if hasattr(v, "is_cuda") and v.is_cuda:
+            import torch
+            assert v.dtype == torch.float64 and v.is_contiguous()
+            torch.cuda.current_stream(v.device).synchronize()   # the library reads on its own stream
+            nz, ny, px = v.shape
+            self._chk(self.lib.dl_interp_scalar(self.h, C.c_void_p(v.data_ptr()), px, px * ny, jjj, 1))
+            return
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        nz, ny, px = v.shape
+        self._chk(self.lib.dl_interp_scalar(self.h, v.ctypes.data_as(C.c_void_p), px, px * ny, jjj, 0))
+
+    def scalar(self, jjj: int = 2) -> np.ndarray:
+        """enst_p (1) or disp_p (2) in reference order."""
+        out = np.zeros(self.nps)
+        self._chk(self.lib.dl_get_scalar(self.h, jjj, _dptr(out)))
+        return out
+
+    def local_st_avg(self):
+        a, b = C.c_double(0), C.c_double(0)
+        self._chk(self.lib.dl_local_st_avg(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def size_dist_log(self):
+        sb = np.zeros(360, np.int32)
+        md = np.zeros(360)
+        self._chk(self.lib.dl_size_dist_log(self.h, _iptr(sb), _dptr(md)))
+        return sb, md
+
+    def size_avg(self):
+        a, b = C.c_double(0), C.c_double(0)
+        self._chk(self.lib.dl_size_avg(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def set_mean_vel_interval(self, ieout: int):
         """particle_step runs MEAN_VEL on steps with istep % ieout == 0 (turb.f90:582)."""
         self._chk(self.lib.dl_set_mean_vel_interval(self.h, int(ieout)))

@@ -18,6 +18,13 @@ Files and the reference lines they follow (units opened in turb.f90:351-395):
   ``(f10.6, 10(1x,f11.5))``, to unit index1*100 + index2*10.  A set pair whose unit the
   reference never opens (a set index above 2) goes to ``fort.<unit>``, the default file
   of an unopened unit.
+* growth diagnostics, every 100th step of a growth run: ``size_dist.dat`` (unit 1001)
+  ``istep, npart, npart_t, sizebin(1:360)`` in ``(2x, I10, I10, I10, 360(I10))``,
+  ``mdens_dist.dat`` (1002) the same with ``mdensbin`` in ``360(1pe14.6)``
+  (SIZE_DIST_LOGARITHMIC, partlib.f90:3921-3925), ``size_avg.dat`` (1003) ``istep, npart,
+  npart_t, r_avg, r_max_avg`` and ``st_avg.dat`` (1004) ``istep, npart, npart_t, st_avg,
+  st_max_avg`` in ``(2x, I10, I10, I10, 2(1pe14.6))`` (SIZE_AVG 3967-3969, LOCAL_St_AVG
+  4325-4326).
 * ``meanv_part_vel.dat`` (unit 106) and ``vel_mag_part.dat`` (unit 107), MEAN_VEL
   (partlib.f90:1889-1980): ``time, vpmean(:,1), vpvar(:,1), vpmean(:,2), vpvar(:,2)`` in
   ``13(1pe12.4)`` and ``time, vpabs(:,1), vphoriz(1), vpxyz(1), vpabs(:,2), vphoriz(2),
@@ -166,6 +173,25 @@ def histogram_lines(hist):
     return out
 
 
+def _growth_head(istep, npart, npart_t):
+    return "  " + fmt_i(istep, 10) + fmt_i(npart, 10) + fmt_i(npart_t, 10)
+
+
+def size_dist_line(istep, npart, npart_t, sizebin):
+    """format (2x, I10, I10, I10, 360(I10)), partlib.f90:3924."""
+    return _growth_head(istep, npart, npart_t) + line_i(sizebin, 10)
+
+
+def mdens_dist_line(istep, npart, npart_t, mdensbin):
+    """format (2x, I10, I10, I10, 360(1pe14.6)), partlib.f90:3925."""
+    return _growth_head(istep, npart, npart_t) + line_e(mdensbin, 14, 6)
+
+
+def avg_line(istep, npart, npart_t, a, b):
+    """format (2x, I10, I10, I10, 2(1pe14.6)), partlib.f90:3969 and 4326."""
+    return _growth_head(istep, npart, npart_t) + line_e((a, b), 14, 6)
+
+
 def vp_file(index1, index2):
     unit = index1 * 100 + index2 * 10
     return {110: "Vp11.dat", 120: "Vp12.dat", 220: "Vp22.dat"}.get(unit, f"fort.{unit}")
@@ -188,6 +214,7 @@ class StatFiles:
         self._fh = {}
         self._fresh = fresh
         for name in ("collision.dat", "detectpairs.dat", "meanv_part_vel.dat", "vel_mag_part.dat",
+                     "size_dist.dat", "mdens_dist.dat", "size_avg.dat", "st_avg.dat",
                      *(f"{h}{a}{b}.dat" for h in _HIST_ORDER for a, b in _PAIRS)):
             self._f(name)
         for a, b in _PAIRS:
@@ -252,3 +279,14 @@ class StatFiles:
         a, b = mean_vel_lines(time, mv, nset)
         self._w("meanv_part_vel.dat", a)
         self._w("vel_mag_part.dat", b)
+
+    # -- growth diagnostics -------------------------------------------------------------
+    def write_size_dist(self, istep, npart, npart_t, sizebin, mdensbin):
+        self._w("size_dist.dat", size_dist_line(istep, npart, npart_t, sizebin))
+        self._w("mdens_dist.dat", mdens_dist_line(istep, npart, npart_t, mdensbin))
+
+    def write_size_avg(self, istep, npart, npart_t, r_avg, r_max_avg):
+        self._w("size_avg.dat", avg_line(istep, npart, npart_t, r_avg, r_max_avg))
+
+    def write_st_avg(self, istep, npart, npart_t, st_avg, st_max_avg):
+        self._w("st_avg.dat", avg_line(istep, npart, npart_t, st_avg, st_max_avg))

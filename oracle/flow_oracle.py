@@ -174,6 +174,30 @@ class FlowOracle:
         self.nold = N
         return u
 
+    def dissipation(self):
+        """DISSIP, partlib.f90:3976-4082: 2 nu S_ij S_ij of the current spectral velocity in
+        physical space, (n, n, n) [z, y, x]; derivatives as k*u then the (re, im) -> (-im, re)
+        swap, terms accumulated in the reference's order."""
+        n = self.n
+        kx, ky, kz = self._kvec()
+        ux, uy, uz = self.uh
+
+        def ik(k, v):
+            return -(k * v.imag) + 1j * (k * v.real)
+
+        terms = [0.5 * (ik(ky, ux) + ik(kx, uy)), 0.5 * (ik(kz, uy) + ik(ky, uz)), 0.5 * (ik(kx, uz) + ik(kz, ux)),
+                 ik(kx, ux), ik(ky, uy), ik(kz, uz)]
+        e = None
+        for w, t in enumerate(terms):
+            p = np.fft.irfftn(t, s=(n,) * 3, axes=(0, 1, 2)) * n ** 3
+            if w == 0:
+                e = 2.0 * p * p
+            elif w < 3:
+                e = e + 2.0 * p * p
+            else:
+                e = e + p * p
+        return 2.0 * self.nu * e
+
     def spectrum(self, nshell):
         e = np.sum(np.abs(self.uh) ** 2, axis=0)
         e[:, :, 0] *= 0.5

@@ -87,6 +87,10 @@ def _load():
     lib.orc_overlap_det.restype = C.c_int
     lib.orc_overlap_det.argtypes = [vp, C.c_int]
     lib.orc_mean_vel.argtypes = [vp, dp]
+    lib.orc_interp_scalar.argtypes = [vp, dp, C.c_int, C.c_long, C.c_long]
+    lib.orc_local_st_avg.argtypes = [vp, dp, dp]
+    lib.orc_size_dist_log.argtypes = [vp, ip, dp]
+    lib.orc_size_avg.argtypes = [vp, dp, dp]
     lib.orc_afun_precomp.argtypes = [vp, dp, C.c_int]
     lib.orc_findindex.argtypes = [vp, C.c_double, C.c_double, ip, ip]
     lib.orc_adj_forward.restype = C.c_int
@@ -336,6 +340,30 @@ class Oracle:
         out = np.zeros(11 * nset)
         self.lib.orc_mean_vel(self._s, out.ctypes.data_as(C.POINTER(C.c_double)))
         return out
+
+    # -- growth diagnostics -------------------------------------------------------------
+    def interp_scalar(self, v: np.ndarray, jjj: int) -> np.ndarray:
+        """INTERP_SCALAR after prepare_interp; returns enst_p (jjj=1) / disp_p (jjj=2)."""
+        ptr, py, pz = self._field_ptr(v)
+        self.lib.orc_interp_scalar(self._s, ptr, jjj, py, pz)
+        return self.arr("enst_p" if jjj == 1 else "disp_p")[:self.nps].copy()
+
+    def local_st_avg(self):
+        a, b = C.c_double(0), C.c_double(0)
+        self.lib.orc_local_st_avg(self._s, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def size_dist_log(self):
+        sb = np.zeros(360, np.int32)
+        md = np.zeros(360)
+        self.lib.orc_size_dist_log(self._s, sb.ctypes.data_as(C.POINTER(C.c_int)),
+                                   md.ctypes.data_as(C.POINTER(C.c_double)))
+        return sb, md
+
+    def size_avg(self):
+        a, b = C.c_double(0), C.c_double(0)
+        self.lib.orc_size_avg(self._s, C.byref(a), C.byref(b))
+        return a.value, b.value
 
     def relocate(self):
         self.lib.orc_relocate(self._s)

@@ -161,6 +161,7 @@ void orc_destroy(orc_state *s)
     free(s->colltype); free(s->nir); free(s->contacts); free(s->pairs); free(s->removepart);
     free(s->collist);
     free(s->nei_num); free(s->nei_data); free(s->axreshaped); free(s->breshaped);
+    free(s->enst_p); free(s->disp_p);
     free(s);
 }
 
@@ -1577,6 +1578,8 @@ double *orc_ptr_d(orc_state *s, const char *name, long *len)
     if (NAME_IS("dmove")) { *len = 3 * m; return s->dmove; }
     if (NAME_IS("bg")) { *len = 18 * m; return s->bg; }
     if (NAME_IS("pertvel")) { *len = 3 * m; return s->pertvel; }
+    if (NAME_IS("enst_p")) { *len = s->enst_p ? m : 0; return s->enst_p; }
+    if (NAME_IS("disp_p")) { *len = s->disp_p ? m : 0; return s->disp_p; }
     if (NAME_IS("ypn")) { *len = (long)s->nypn * s->newsize; return s->ypn; }
     if (NAME_IS("vpn")) { *len = 3L * s->newsize; return s->vpn; }
     if (NAME_IS("radius")) { *len = 10; return s->radius; }
@@ -1702,4 +1705,90 @@ void orc_set_i(orc_state *s, const char *name, int v)
 void orc_set_d(orc_state *s, const char *name, double v)
 {
     if (NAME_IS("time")) s->time = v;
+}
+
+/* ------------------------------------------------------------------------------------
+ * Growth diagnostics
+ * ---------------------------------------------------------------------------------- */
+/* INTERP_SCALAR, partlib.f90:4101-4290: the INTERPOLATE stencil with the PREPARE_INTERP
+ * weights (the halo exchange of a single rank is the periodic wrap), then negative values
+ * replaced by 0.00001 (4272-4281). */
+void orc_interp_scalar(orc_state *s, const double *v, int jjj, long pitch_y, long pitch_z)
+{
+    int ih;
+    double *out;
+    if (!s->enst_p) s->enst_p = (double *)zalloc(sizeof(double) * s->msize);
+    if (!s->disp_p) s->disp_p = (double *)zalloc(sizeof(double) * s->msize);
+    out = jjj == 1 ? s->enst_p : s->disp_p;
+    for (ih = 0; ih < s->nps; ih++) {
+        int node[3], n;
+        double bx[6], by[6], bz[6], acc;
+        for (n = 0; n < 6; n++) {
+            bx[n] = BG(s, ih, n, 0);
+            by[n] = BG(s, ih, n, 1);
+            bz[n] = BG(s, ih, n, 2);
+        }
+        node[0] = LH(s, ih, 0);
+        node[1] = LH(s, ih, 1);
+        node[2] = LH(s, ih, 2);
+        acc = stencil_sum(s, v, pitch_y, pitch_z, node, bx, by, bz);
+        if (acc < 0.0) acc = 0.00001;
+        out[ih] = acc;
+    }
+}
+
+/* LOCAL_St_AVG, partlib.f90:4294-4330 (nproc = 1, npart_t = nps). */
+void orc_local_st_avg(orc_state *s, double *st_avg, double *st_max_avg)
+{
+    double st_sum = 0.0, st_max, st_1, r;
+    long i, imax = 0;
+    for (i = 0; i < s->nps; i++) {
+        double taup = s->tau_cloud_const2 * (YP(s, 6, i) * YP(s, 6, i));
+        st_sum = st_sum + taup * sqrt(s->disp_p[i] / s->rnu);
+    }
+    for (i = 1; i < s->nps; i++)            /* MAXLOC: the first maximum */
+        if (YP(s, 6, i) > YP(s, 6, imax)) imax = i;
+    r = YP(s, 6, imax);
+    st_max = s->nps ? s->tau_cloud_const2 * (r * r) * sqrt(s->disp_p[imax] / s->rnu) : 0.0;
+    st_1 = (s->tau_cloud_const2 * (s->radius[0] * s->radius[0])) / s->tauk_dns;
+    *st_avg = (st_sum / (double)s->nps) / st_1;
+    *st_max_avg = (st_max / 1.0) / st_1;
+}
+
+/* SIZE_DIST_LOGARITHMIC, partlib.f90:3873-3933: 360 bins of the mass ratio
+ * (r / radius(1))^3 on a 2^(1/32) geometric grid, counts and mass density. */
+void orc_size_dist_log(orc_state *s, int *sizebin, double *mdensbin)
+{
+    const int nnbin = 360;
+    const double scal = 32.0;
+    const double rho_bin = pow(2.0, 1.0 / scal);
+    const double lrho = log(rho_bin);
+    long i;
+    int k;
+    for (k = 0; k < nnbin; k++) { sizebin[k] = 0; mdensbin[k] = 0.0; }
+    for (i = 0; i < s->nps; i++) {
+        const double y = YP(s, 6, i);
+        const double q = y / s->radius[0];
+        const double m_ratio = q * q * q;
+        const double x = log(m_ratio) / lrho + 1.5;
+        int ir = x >= 1.0 ? (x < (double)nnbin ? (int)x : nnbin) : 1;
+        sizebin[ir - 1] = sizebin[ir - 1] + 1;
+        mdensbin[ir - 1] = mdensbin[ir - 1] + (4.0 / 3.0) * s->rho_water * s->pi * (y * y * y);
+    }
+    for (k = 0; k < nnbin; k++) mdensbin[k] = 3.0 * scal * mdensbin[k] / log(2.0);
+}
+
+/* SIZE_AVG, partlib.f90:3937-3972 (nproc = 1, npart_t = nps). */
+void orc_size_avg(orc_state *s, double *r_avg, double *r_max_avg)
+{
+    double r_sum = 0.0, rmax = 0.0;
+    long i;
+    for (i = 0; i < s->nps; i++) {
+        const double y = YP(s, 6, i);
+        r_sum = r_sum + y * y * y;
+        if (i == 0 || y > rmax) rmax = y;
+    }
+    rmax = rmax * rmax * rmax;
+    *r_avg = pow(r_sum / (double)s->nps, 1.0 / 3.0) / s->radius[0];
+    *r_max_avg = pow(rmax / 1.0, 1.0 / 3.0) / s->radius[0];
 }

@@ -130,6 +130,9 @@ typedef struct orc_state {
     double gmres_res, gmres_norm_rhs;
 
     int error;                 /* 0 ok; <0 error code; see ORC_E_* */
+
+    /* ---- growth diagnostics (global.f90:47) ---- */
+    double *enst_p, *disp_p;   /* INTERP_SCALAR outputs, msize each (allocated on first use) */
 } orc_state;
 
 enum {
@@ -172,6 +175,13 @@ int  orc_nei_list_precomp(orc_state *s);                /* 3218-3371 */
 void orc_afun_precomp(orc_state *s, const double *x, int icall); /* 3375-3510 */
 int  orc_hdi_gmres(orc_state *s);                       /* 2756-3005 */
 void orc_coalesce(orc_state *s);                        /* 3642-3825 */
+
+/* Growth diagnostics (turb.f90:557-562, 596-598).  Integer-valued real exponents
+ * (x**2.0, x**3.0) are evaluated as products and x**0.5 as sqrt. */
+void orc_interp_scalar(orc_state *s, const double *v, int jjj, long pitch_y, long pitch_z); /* 4101-4290 */
+void orc_local_st_avg(orc_state *s, double *st_avg, double *st_max_avg);                    /* 4294-4330 */
+void orc_size_dist_log(orc_state *s, int *sizebin360, double *mdensbin360);                 /* 3873-3933 */
+void orc_size_avg(orc_state *s, double *r_avg, double *r_max_avg);                          /* 3937-3972 */
 
 /* Interpolation + advance only (the measured unit of the CPU baseline): for each of the
  * three components it runs the INTERPOLATE stencil, then PART_HISTORY_FVP/FDP,

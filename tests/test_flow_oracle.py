@@ -71,3 +71,27 @@ def test_stochastic_forcing_drives_low_shells_from_rest():
     e = f.spectrum(8)
     assert e[1] > 0 and e[2] > 0
     assert e[4:].max() < 1e-3 * e[1:3].max()
+
+
+def test_dissipation_of_a_shear_wave():
+    """u_x = A sin(z): S_31 = A cos(z) / 2, so 2 nu S_ij S_ij = nu A^2 cos^2(z)."""
+    n, nu, amp = 16, 0.05, 0.7
+    f = FlowOracle(n, nu, 0.01)
+    f.set_velocity(shear_wave(n, amp))
+    z = np.arange(n) * 2 * np.pi / n
+    want = nu * amp ** 2 * np.cos(z) ** 2
+    e = f.dissipation()
+    assert np.abs(e - want[:, None, None]).max() < 1e-14
+
+
+def test_mean_dissipation_is_nu_mean_gradient_squared():
+    """For a periodic solenoidal field <2 nu S:S> = nu <|grad u|^2> = nu sum_k k^2 |u_k|^2."""
+    n, nu = 16, 0.02
+    f = FlowOracle(n, nu, 0.005)
+    f.set_velocity(random_velocity(n))
+    k2 = f.KX ** 2 + f.KY ** 2 + f.KZ ** 2
+    w = np.where(f.KX == 0, 1.0, 2.0)
+    want = nu * np.sum(w * k2 * np.sum(np.abs(f.uh) ** 2, axis=0))
+    e = f.dissipation()
+    assert e.min() >= 0.0
+    assert abs(e.mean() - want) < 1e-12 * want
