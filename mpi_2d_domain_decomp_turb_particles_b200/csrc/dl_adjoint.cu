@@ -16,13 +16,16 @@
 // segment of K steps in registers (one launch per segment).  The forward pass stores a
 // checkpoint (x, V, V_{-1}, V_{-2}, U_{-1..-3}) at every segment start.  The backward
 // pass walks the segments in reverse: it recomputes the segment from its checkpoint,
-// storing (x_n, V_n, U_n) per step, then runs the reverse sweep of the segment with the
-// adjoint state (x_bar, tau_bar and two three-deep shift registers of velocity and
-// fluid-velocity adjoints) in registers.  The interpolation adjoint is a scatter of
-// U_bar (x) weights into the grid gradient with atomics, plus the gradient of the
-// interpolant for x_bar.  Field and grid gradient are halo-padded (4 planes of periodic
-// images on every side, so no index wraps inside the stencil loops) with the three
-// components interleaved per point and a fourth pad slot: one vector load reads a
+// storing (x_n, V_n, U_n) and the interpolant's Jacobian dU_n/dx per step (one pass over
+// the stencil gives both), then runs the reverse sweep of the segment with the adjoint
+// state (x_bar, tau_bar and two three-deep shift registers of velocity and
+// fluid-velocity adjoints) in registers: x_bar takes J^T U_bar from the stored Jacobian
+// and U_bar_n is stored in place of U_n.  The grid gradient (the scatter U_bar (x)
+// weights) is then deposited per segment: one warp per droplet sums the segment's steps
+// per stencil point and adds each point once per run of steps with the same stencil
+// corner, instead of once per step.  Field and grid gradient are halo-padded (4 planes
+// of periodic images on every side, so no index wraps inside the stencil loops) with the
+// three components interleaved per point and a fourth pad slot: one vector load reads a
 // point's velocity and, in FP32, one vector atomic adds a point's gradient.
 //
 // Precision: DL_FP64 everything in FP64 (same operation order as the FP64 reference
@@ -34,6 +37,7 @@
 #include <algorithm>
 #include <cmath>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace {
@@ -160,6 +164,71 @@ __device__ __forceinline__ void interp(const Field<float> &F, const double *x, f
     for (int q = 0; q < 3; q++) out[q] = acc[q];
 }
 
+// FP32 interpolant and its Jacobian in one pass over the stencil: U[q] and
+// J[q][k] = dU[q]/d(fraction k) (divide by dx for the spatial derivative)
+__device__ __forceinline__ void interp_jac(const Field<float> &F, const double *x, float *U, float (*J)[3])
+{
+    float b[3][6], d[3][6];
+    const int64_t c0 = stencil_at<float>(F, x, b, d);
+    float au[3] = {0.0f, 0.0f, 0.0f}, ax[3] = {0.0f, 0.0f, 0.0f}, ay[3] = {0.0f, 0.0f, 0.0f},
+          az[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll 1
+    for (int c = 0; c < 6; c++) {
+        float tu[3] = {0.0f, 0.0f, 0.0f}, tx[3] = {0.0f, 0.0f, 0.0f}, ty[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int bb = 0; bb < 6; bb++) {
+            const float4 *row = reinterpret_cast<const float4 *>(F.f) + c0 + F.pz * c + F.py * bb;
+            float ru[3] = {0.0f, 0.0f, 0.0f}, rx[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int a = 0; a < 6; a++) {
+                const float4 v = row[a];
+                ru[0] = fmaf(v.x, b[0][a], ru[0]); rx[0] = fmaf(v.x, d[0][a], rx[0]);
+                ru[1] = fmaf(v.y, b[0][a], ru[1]); rx[1] = fmaf(v.y, d[0][a], rx[1]);
+                ru[2] = fmaf(v.z, b[0][a], ru[2]); rx[2] = fmaf(v.z, d[0][a], rx[2]);
+            }
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                tu[q] = fmaf(ru[q], b[1][bb], tu[q]);
+                tx[q] = fmaf(rx[q], b[1][bb], tx[q]);
+                ty[q] = fmaf(ru[q], d[1][bb], ty[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            au[q] = fmaf(tu[q], b[2][c], au[q]);
+            ax[q] = fmaf(tx[q], b[2][c], ax[q]);
+            ay[q] = fmaf(ty[q], b[2][c], ay[q]);
+            az[q] = fmaf(tu[q], d[2][c], az[q]);
+        }
+    }
+    for (int q = 0; q < 3; q++) {
+        U[q] = au[q];
+        J[q][0] = ax[q]; J[q][1] = ay[q]; J[q][2] = az[q];
+    }
+}
+
+// FP64 interpolant in the reference's order (bit-identical to interp) and its Jacobian
+__device__ __forceinline__ void interp_jac(const Field<double> &F, const double *x, double *U, double (*J)[3])
+{
+    double b[3][6], d[3][6];
+    const int64_t c0 = stencil_at<double>(F, x, b, d);
+    for (int comp = 0; comp < 3; comp++) {
+        const double *v = F.f + 4 * c0 + comp;
+        double acc = 0.0, jx = 0.0, jy = 0.0, jz = 0.0;
+        for (int a = 0; a < 6; a++)
+            for (int bb = 0; bb < 6; bb++)
+                for (int c = 0; c < 6; c++) {
+                    const double f = v[4 * (a + F.py * bb + F.pz * c)];
+                    acc = acc + f * b[0][a] * b[1][bb] * b[2][c];
+                    jx = jx + f * d[0][a] * b[1][bb] * b[2][c];
+                    jy = jy + f * b[0][a] * d[1][bb] * b[2][c];
+                    jz = jz + f * b[0][a] * b[1][bb] * d[2][c];
+                }
+        U[comp] = acc;
+        J[comp][0] = jx; J[comp][1] = jy; J[comp][2] = jz;
+    }
+}
+
 __device__ __forceinline__ void load3(const float *p, float *v)
 {
     const float4 q = *reinterpret_cast<const float4 *>(p);
@@ -180,68 +249,10 @@ __device__ __forceinline__ void add3(double *p, double a, double b, double c)
     atomicAdd(p, a); atomicAdd(p + 1, b); atomicAdd(p + 2, c);
 }
 
-// x_bar += J^T ubar; grid gradient += ubar (x) weights
-template <typename T>
-__device__ __forceinline__ void interp_adjoint(const Field<T> &F, const double *x, const T *ub, double *xbar)
-{
-    T b[3][6], d[3][6];
-    const int64_t c0 = stencil_at<T>(F, x, b, d);
-    T gx = (T)0, gy = (T)0, gz = (T)0;
-    for (int a = 0; a < 6; a++)
-        for (int bb = 0; bb < 6; bb++)
-            for (int c = 0; c < 6; c++) {
-                const int64_t o = c0 + a + F.py * bb + F.pz * c;
-                const T w = b[0][a] * b[1][bb] * b[2][c];
-                T f3[3];
-                load3(F.f + 4 * o, f3);
-                const T sv = ub[0] * f3[0] + ub[1] * f3[1] + ub[2] * f3[2];
-                gx = gx + sv * d[0][a] * b[1][bb] * b[2][c];
-                gy = gy + sv * b[0][a] * d[1][bb] * b[2][c];
-                gz = gz + sv * b[0][a] * b[1][bb] * d[2][c];
-                add3(F.g + 4 * o, ub[0] * w, ub[1] * w, ub[2] * w);
-            }
-    xbar[0] = xbar[0] + (double)gx / F.dx;
-    xbar[1] = xbar[1] + (double)gy / F.dx;
-    xbar[2] = xbar[2] + (double)gz / F.dx;
-}
-
-// FP32: z planes outer, the 6 x 6 (x, y) points of a plane unrolled, separable sums, one
-// vector atomic per point
-template <>
-__device__ __forceinline__ void interp_adjoint<float>(const Field<float> &F, const double *x, const float *ub,
-                                                      double *xbar)
-{
-    float b[3][6], d[3][6];
-    const int64_t c0 = stencil_at<float>(F, x, b, d);
-    float gx = 0.0f, gy = 0.0f, gz = 0.0f;
-    for (int c = 0; c < 6; c++) {
-        const float bz = b[2][c], dz = d[2][c];
-        float tx = 0.0f, ty = 0.0f, tw = 0.0f;
-#pragma unroll
-        for (int bb = 0; bb < 6; bb++) {
-            float rx = 0.0f, rw = 0.0f;
-#pragma unroll
-            for (int a = 0; a < 6; a++) {
-                const int64_t o = c0 + a + F.py * bb + F.pz * c;
-                const float4 f = *reinterpret_cast<const float4 *>(F.f + 4 * o);
-                const float sv = fmaf(ub[2], f.z, fmaf(ub[1], f.y, ub[0] * f.x));
-                rx = fmaf(sv, d[0][a], rx);
-                rw = fmaf(sv, b[0][a], rw);
-                const float w = b[0][a] * b[1][bb] * bz;
-                atomicAdd(reinterpret_cast<float4 *>(F.g + 4 * o), make_float4(ub[0] * w, ub[1] * w, ub[2] * w, 0.0f));
-            }
-            tx = fmaf(rx, b[1][bb], tx);
-            ty = fmaf(rw, d[1][bb], ty);
-            tw = fmaf(rw, b[1][bb], tw);
-        }
-        gx = fmaf(tx, bz, gx);
-        gy = fmaf(ty, bz, gy);
-        gz = fmaf(tw, dz, gz);
-    }
-    xbar[0] = xbar[0] + (double)gx / F.dx;
-    xbar[1] = xbar[1] + (double)gy / F.dx;
-    xbar[2] = xbar[2] + (double)gz / F.dx;
-}
+// c + a*b: FMA in FP32, separate multiply and add in FP64 (the FP64 path keeps the
+// reference's rounding)
+__device__ __forceinline__ float madd(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double madd(double a, double b, double c) { return c + a * b; }
 
 // state block: x[3] (double, np each) + 18 arrays of T: V, F1, F2, U1, U2, U3 (x3 each)
 template <typename T>
@@ -260,10 +271,11 @@ struct SegArgs {
     State<T> ckpt;          // checkpoint written at the segment start (x null: none)
     double *TX;             // trajectory (recompute): slot j + 3 for step s0 + j, [slot][3][np]
     T *TV, *TU;
+    T *TJ;                  // recompute: interpolant Jacobian of step s0 + j, [j][9][np]
 };
 
 // K forward steps of one droplet; optional checkpoint at the start and trajectory
-template <typename T>
+template <typename T, bool JAC>
 __global__ void __launch_bounds__(128) k_adj_segment(SegArgs<T> A)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -301,7 +313,14 @@ __global__ void __launch_bounds__(128) k_adj_segment(SegArgs<T> A)
     const int64_t slot = 3 * (int64_t)np;
     for (int j = 0; j < A.nstep; j++) {
         T U0[3];
-        interp(A.F, x, U0);
+        if constexpr (JAC) {
+            T J[3][3];
+            interp_jac(A.F, x, U0, J);
+            for (int q = 0; q < 3; q++)
+                for (int k = 0; k < 3; k++) A.TJ[((int64_t)j * 9 + 3 * q + k) * np + i] = J[q][k];
+        } else {
+            interp(A.F, x, U0);
+        }
         if (A.first && j == 0) {   // PART_HISTORY_FVP / FDP first step: every level
             for (int c = 0; c < 3; c++) {
                 V[c] = A.init_velocity ? U0[c] : (c == 0 ? g * tau : (T)0);
@@ -363,7 +382,8 @@ struct RevArgs {
     double dt, g;
     const double *tau;
     const double *TX;
-    const T *TV, *TU;
+    const T *TV, *TJ;
+    T *TU;
     double *xbar, *taubar;
     T *P, *Q;
 };
@@ -436,8 +456,14 @@ __global__ void __launch_bounds__(128) k_adj_reverse(RevArgs<T> A)
             else
                 taubar = taubar + A.g * (double)P[1][0];
         }
-        const double xn[3] = {A.TX[sj + 0 * np + i], A.TX[sj + 1 * np + i], A.TX[sj + 2 * np + i]};
-        interp_adjoint<T>(A.F, xn, Q[0], xb);
+        // x_bar from the Jacobian stored by the recompute; U_bar of this step replaces U_n
+        // in the trajectory (no later reverse step reads it) for the deposition kernel
+        for (int k = 0; k < 3; k++) {
+            T gk = (T)0;
+            for (int q = 0; q < 3; q++) gk = madd(Q[0][q], A.TJ[((int64_t)j * 9 + 3 * q + k) * np + i], gk);
+            xb[k] = xb[k] + (double)gk / A.F.dx;
+        }
+        for (int c = 0; c < 3; c++) A.TU[sj + c * np + i] = Q[0][c];
         for (int c = 0; c < 3; c++) {
             P[0][c] = P[1][c]; P[1][c] = P[2][c]; P[2][c] = newV[c];
             Q[0][c] = Q[1][c]; Q[1][c] = Q[2][c]; Q[2][c] = newU[c];
@@ -450,6 +476,75 @@ __global__ void __launch_bounds__(128) k_adj_reverse(RevArgs<T> A)
             A.P[(k * 3 + c) * np + i] = P[k][c];
             A.Q[(k * 3 + c) * np + i] = Q[k][c];
         }
+    }
+}
+
+// FP32 grid-gradient deposition of one segment: one warp per droplet, lane t holds step t
+// (weights and U_bar staged in shared memory); the steps are cut into runs with the same
+// stencil corner, and for each run the lanes own the 216 stencil points, sum
+// U_bar_t (x) w_t over the run's steps in registers and add each point once with one
+// vector atomic.  A droplet rarely changes cell within a segment, so the grid sees one
+// atomic per point per droplet-segment instead of one per step.
+constexpr int kDepWarps = 4;
+constexpr int kDepRow = 21;   // bx[6], by[6], bz[6], U_bar[3]
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kDepWarps) k_adj_deposit(Field<T> F, int np, int nstep,
+                                                                const double *__restrict__ TX,
+                                                                const T *__restrict__ TUbar)
+{
+    __shared__ T sw[kDepWarps][32][kDepRow];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * kDepWarps + w;
+    if (i >= np) return;   // whole warps leave together
+    const int64_t slot = 3 * (int64_t)np;
+    T *row = sw[w][lane];
+    for (int t0 = 0; t0 < nstep; t0 += 32) {
+        const int cnt = min(32, nstep - t0);
+        const int t = t0 + lane;
+        int64_t corner = -1;
+        if (lane < cnt) {
+            const int64_t st = (int64_t)(t + 3) * slot;
+            const double x[3] = {TX[st + i], TX[st + np + i], TX[st + 2 * np + i]};
+            T b[3][6];
+            corner = stencil_at<T>(F, x, b, nullptr);
+            for (int k = 0; k < 3; k++)
+                for (int q = 0; q < 6; q++) row[6 * k + q] = b[k][q];
+            for (int c = 0; c < 3; c++) row[18 + c] = TUbar[st + c * np + i];
+        }
+        __syncwarp();
+        int s0 = 0;
+        while (s0 < cnt) {
+            const int64_t cs = __shfl_sync(0xffffffffu, corner, s0);
+            const unsigned diff = __ballot_sync(0xffffffffu, lane > s0 && lane < cnt && corner != cs);
+            const int e = diff ? __ffs(diff) - 1 : cnt;
+            T g[7][3];
+            int pa[7], pb[7], pc[7];
+#pragma unroll
+            for (int k = 0; k < 7; k++) {
+                const int p = lane + 32 * k;
+                const int pp = p < 216 ? p : 0;
+                pa[k] = pp % 6; pb[k] = (pp / 6) % 6; pc[k] = pp / 36;
+                g[k][0] = g[k][1] = g[k][2] = (T)0;
+            }
+            for (int q = s0; q < e; q++) {
+                const T *r = sw[w][q];
+                const T u0 = r[18], u1 = r[19], u2 = r[20];
+#pragma unroll
+                for (int k = 0; k < 7; k++) {
+                    const T wt = r[pa[k]] * r[6 + pb[k]] * r[12 + pc[k]];
+                    g[k][0] = madd(u0, wt, g[k][0]);
+                    g[k][1] = madd(u1, wt, g[k][1]);
+                    g[k][2] = madd(u2, wt, g[k][2]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 7; k++)
+                if (lane + 32 * k < 216)
+                    add3(F.g + 4 * (cs + pa[k] + F.py * pb[k] + F.pz * pc[k]), g[k][0], g[k][1], g[k][2]);
+            s0 = e;
+        }
+        __syncwarp();
     }
 }
 
@@ -692,6 +787,7 @@ struct dl_adj {
     void *cks = nullptr;     // [nseg][18][np]
     double *TX = nullptr;    // trajectory [(K+4)][3][np]
     void *TV = nullptr, *TU = nullptr;
+    void *TJ = nullptr;      // interpolant Jacobians of the recomputed segment [K][9][np]
     double *xbar = nullptr, *taubar = nullptr;
     void *P = nullptr, *Q = nullptr;
     int *cell_cnt = nullptr, *cell_start = nullptr, *cell_fill = nullptr, *cell_key = nullptr, *cell_order = nullptr;
@@ -775,14 +871,18 @@ int run_segment(dl_adj *a, int seg, bool record)
         A.TX = a->TX;
         A.TV = tp<T>(a->TV);
         A.TU = tp<T>(a->TU);
+        A.TJ = tp<T>(a->TJ);
     } else {
         A.in = state_of<T>(a->xs, a->ss);
         A.out = state_of<T>(a->xs, a->ss);
         A.ckpt = state_of<T>(a->ckx + (size_t)seg * 3 * np, (char *)a->cks + seg * cks);
         A.TX = nullptr;
-        A.TV = A.TU = nullptr;
+        A.TV = A.TU = A.TJ = nullptr;
     }
-    k_adj_segment<T><<<dl_blocks(np, 128), 128, 0, a->stream>>>(A);
+    if (record)
+        k_adj_segment<T, true><<<dl_blocks(np, 128), 128, 0, a->stream>>>(A);
+    else
+        k_adj_segment<T, false><<<dl_blocks(np, 128), 128, 0, a->stream>>>(A);
     ACUDA(a, cudaGetLastError());
     return 0;
 }
@@ -803,11 +903,15 @@ int run_reverse(dl_adj *a, int seg)
     A.TX = a->TX;
     A.TV = tp<T>(a->TV);
     A.TU = tp<T>(a->TU);
+    A.TJ = tp<T>(a->TJ);
     A.xbar = a->xbar;
     A.taubar = a->taubar;
     A.P = tp<T>(a->P);
     A.Q = tp<T>(a->Q);
     k_adj_reverse<T><<<dl_blocks(np, 128), 128, 0, a->stream>>>(A);
+    ACUDA(a, cudaGetLastError());
+    k_adj_deposit<T><<<(np + kDepWarps - 1) / kDepWarps, 32 * kDepWarps, 0, a->stream>>>(A.F, np, A.nstep, a->TX,
+                                                                                        tp<T>(a->TU));
     ACUDA(a, cudaGetLastError());
     return 0;
 }
@@ -996,6 +1100,7 @@ extern "C" int dl_adj_create(const dl_adj_params *p, dl_adj **out)
     ADJ_ALLOC(a->TX, (size_t)(a->K + 4) * 3 * np * 8);
     ADJ_ALLOC(a->TV, (size_t)(a->K + 4) * 3 * np * es);
     ADJ_ALLOC(a->TU, (size_t)(a->K + 4) * 3 * np * es);
+    ADJ_ALLOC(a->TJ, (size_t)a->K * 9 * np * es);
     ADJ_ALLOC(a->xbar, 3 * np * 8);
     ADJ_ALLOC(a->taubar, np * 8);
     ADJ_ALLOC(a->P, 9 * np * es);
@@ -1033,7 +1138,7 @@ extern "C" int dl_adj_destroy(dl_adj *a)
     if (!a) return 0;
     cudaSetDevice(a->p.device);
     if (a->own_stream) cudaStreamSynchronize(a->own_stream);
-    void *ptrs[] = {a->fpad, a->gpad, a->x0, a->tau, a->rad, a->xs, a->ss, a->ckx, a->cks, a->TX, a->TV, a->TU,
+    void *ptrs[] = {a->fpad, a->gpad, a->x0, a->tau, a->rad, a->xs, a->ss, a->ckx, a->cks, a->TX, a->TV, a->TU, a->TJ,
                     a->xbar, a->taubar, a->P, a->Q, a->cell_cnt, a->cell_start, a->cell_fill, a->scan_tmp,
                     a->cell_key, a->cell_order, a->pairs, a->d_npairs, a->red, a->perm};
     for (void *q : ptrs)
