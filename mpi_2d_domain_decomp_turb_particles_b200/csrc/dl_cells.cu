@@ -659,14 +659,30 @@ __global__ void __launch_bounds__(1024) k_lv_reorder(int n, int *lv_list, int *l
                                                      int *ref_of_dev, int *dev_of_ref, int *err, void *pt0,
                                                      void *pt1, void *pt2, int pesz, void *ptmp, int *src_dev)
 {
-    __shared__ int s_m, s_k;
+    __shared__ int s_m, s_k, s_fr;
     __shared__ int ws[33];
     __shared__ int skey[kSortMax];
     __shared__ int sP[kSortMax];
+    __shared__ signed char sQ[kSortMax];    // sorted path: departing flags of the tail positions
+    int *sDep = skey;                       // sorted path, after compaction: (nid << 27 | position) in departure order
     const int kraw = *lv_n;
     int *P;
     int kk = 0;
-    if (kraw <= kSortMax) {
+    if (kraw <= (int)blockDim.x) {
+        // few departures (the usual case): rank sort, one entry per thread, ties by slot
+        if (threadIdx.x < kraw) sP[threadIdx.x] = lv_list[threadIdx.x];
+        __syncthreads();
+        if (threadIdx.x < kraw) {
+            const int v = sP[threadIdx.x];
+            int rank = 0;
+            for (int j = 0; j < kraw; j++) {
+                const int u = sP[j];
+                rank += (u < v) || (u == v && j < (int)threadIdx.x);
+            }
+            skey[rank] = v;
+        }
+        __syncthreads();
+    } else if (kraw <= kSortMax) {
         // sort the appended list (padded to a power of two)
         int np2 = 1;
         while (np2 < kraw) np2 <<= 1;
@@ -684,6 +700,8 @@ __global__ void __launch_bounds__(1024) k_lv_reorder(int n, int *lv_list, int *l
                 }
                 __syncthreads();
             }
+    }
+    if (kraw <= kSortMax) {
         // keep flagged, distinct entries (4 per thread, in order)
         const int base = threadIdx.x * 4;
         int keep[4], cnt = 0;
@@ -714,7 +732,75 @@ __global__ void __launch_bounds__(1024) k_lv_reorder(int n, int *lv_list, int *l
         P = Pg;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (kraw <= kSortMax && n < (1 << 27)) {
+        // Sorted path, the swap-with-last replay in closed form.  With L = n - k droplets
+        // staying, the holes are the departing positions below L (ascending) and the
+        // fillers the staying positions of the tail [L, n), taken from the top: hole i
+        // receives the i-th staying tail position.  Numbering the tail from the top
+        // (s = 0 at n - 1), the replay pops tail position s as departure number s + 1;
+        // hole i + 1 is numbered after the filler of hole i, and the lowest tail
+        // position, when it departs below the last filler, is numbered right after it.
+        const int k = kk, L = n - k;
+        for (int t = threadIdx.x; t < k; t += blockDim.x) sQ[t] = 0;
+        if (threadIdx.x == 0) s_fr = -1;
+        __syncthreads();
+        for (int t = threadIdx.x; t < k; t += blockDim.x)
+            if (P[t] >= L) sQ[n - 1 - P[t]] = 1;
+        __syncthreads();
+        const int base = threadIdx.x * 4;
+        int stay[4], cnt = 0;
+        for (int q = 0; q < 4; q++) {
+            const int t = base + q;
+            stay[q] = t < k && !sQ[t];
+            cnt += stay[q];
+        }
+        int r;
+        int jf = block_excl_scan(cnt, ws, r);   // r staying tail positions = r holes
+        for (int q = 0; q < 4; q++)
+            if (stay[q]) {
+                const int t = base + q;
+                old_ref[jf] = n - 1 - t;           // filler of hole jf + 1
+                new_ref[jf] = P[jf];
+                if (jf + 1 < r) sDep[t + 1] = (nid[P[jf + 1]] << 27) | P[jf + 1];
+                if (jf == r - 1) s_fr = t;
+                jf++;
+            }
+        __syncthreads();
+        const int sfr = s_fr;
+        if (threadIdx.x == 0 && r > 0) sDep[0] = (nid[P[0]] << 27) | P[0];
+        for (int t = threadIdx.x; t < k; t += blockDim.x) {
+            const int pos = P[t];
+            if (pos >= L) {
+                const int st = n - 1 - pos;
+                const int idx = (st == k - 1 && st > sfr) ? sfr + 1 : st + 1;
+                sDep[idx] = (nid[pos] << 27) | pos;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            // new slots at the end in departure order, grouped by nid 1..8
+            const int lane = threadIdx.x;
+            int m = r, slot = L;
+            for (int q = 1; q <= 8; q++)
+                for (int c0 = 0; c0 < k; c0 += 32) {
+                    const int j = c0 + lane;
+                    const int v = j < k ? sDep[j] : 0;
+                    const bool pred = j < k && (v >> 27) == q;
+                    const unsigned bal = __ballot_sync(0xffffffffu, pred);
+                    if (pred) {
+                        const int pos = __popc(bal & ((1u << lane) - 1u));
+                        old_ref[m + pos] = v & ((1 << 27) - 1);
+                        new_ref[m + pos] = slot + pos;
+                    }
+                    m += __popc(bal);
+                    slot += __popc(bal);
+                }
+            if (lane == 0) {
+                s_m = m;
+                s_k = k;
+            }
+        }
+    } else if (threadIdx.x == 0) {
         const int k = kk;
         int lo = 0, hi = k - 1, sum = 0, nf = 0, nd = 0;
         while (lo <= hi) {                 // each pass consumes at least one departing droplet
