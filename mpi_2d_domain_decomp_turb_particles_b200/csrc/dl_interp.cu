@@ -848,12 +848,11 @@ __global__ void k_mean_vel(int nps, const T *ux, const T *uy, const T *uz, const
         if (sacc[i] != 0.0) atomicAdd(&acc[i], sacc[i]);
 }
 
-// brick configurations (cells) per precision
 // brick / pipeline configuration per precision: brick cells, component shifts (bank
 // spreading), TMA stages, droplets per chunk, consumer groups x warps per group
 constexpr int F32_BX = 16, F32_BY = 16, F32_BZ = 6, F32_XS = 0, F32_YS = 1, F32_M = 1, F32_S = 6, F32_MAXD = 256;
 constexpr int F32_NG = 2, F32_GW = 6;
-constexpr int F64_BX = 16, F64_BY = 8, F64_BZ = 4, F64_XS = 2, F64_YS = 0, F64_M = 0, F64_S = 6, F64_MAXD = 64;
+constexpr int F64_BX = 8, F64_BY = 8, F64_BZ = 8, F64_XS = 2, F64_YS = 0, F64_M = 1, F64_S = 5, F64_MAXD = 64;
 constexpr int F64_NG = 2, F64_GW = 6;
 
 template <typename T>
