@@ -210,8 +210,17 @@ def run_ours(args):
         dist.all_reduce(t64, op=dist.ReduceOp.MAX)
     value64 = ws * N_PART / (float(t64[0]) * 1e-3)
 
+    errs = errors_bench(dev, torch, field)
     adj = adjoint_bench(dev, torch) if not args.no_adjoint else None
     full = full_step_bench(dev, torch, field) if not args.no_full else None
+    del field
+    torch.cuda.empty_cache()
+    c4 = None
+    if not args.no_config4:
+        try:
+            c4 = config4_bench(dev, torch)
+        except Exception as ex:   # reported, not fatal: the headline numbers stand alone
+            c4 = {"error": f"{type(ex).__name__}: {ex}"}
 
     if rank == 0:
         peak, kind = _peaks()
@@ -234,7 +243,9 @@ def run_ours(args):
             "e2e": {"value": N_PART / (e2e_ms * 1e-3), "unit": "particle-updates/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "path": "dl_set_field (host FP64 field, pinned) + dl_update_step + dl_mean_vel"},
+            "errors_vs_fp64": errs,
             "full_step": full,
+            "config4": c4,
             "adjoint": adj,
             "gpu_launches": int(launches),
             "clocks": clocks,
@@ -296,6 +307,125 @@ def full_step_bench(dev, torch, field):
             "particle_phase_ms": {"interp_advance": ph[0], "cell_list": ph[1], "collision": ph[2], "hdi": ph[3],
                                   "periodic_relocate": ph[4], "overlap": ph[5]},
             "gmres_iterations": iters}
+
+
+def errors_bench(dev, torch, field, steps=10):
+    """Relative error of each floating-point output of the mixed path against the FP64
+    path (bit-identical to the FP64 oracle on identical inputs) on the headline workload:
+    interpolated velocity at identical positions, then over `steps` full particle steps
+    (collision detection and statistics on) the settling velocity (set means of yp(4)),
+    the RDF bins, w_r at contact and the collision kernel (collision counts)."""
+    import numpy as np
+    g = {p: _make(p, dev) for p in ("mixed", "fp64")}
+    for x in g.values():
+        x.set_fields(*field)
+        x.prepare_interp()
+        for k in (1, 2, 3):
+            x.interpolate(None, k)
+    vm, v64 = g["mixed"].get_particles()["vp"], g["fp64"].get_particles()["vp"]
+    urms = float(np.sqrt(np.mean(v64 ** 2)))
+    out = {"interpolated_velocity": {"rel_l2": float(np.linalg.norm(vm - v64) / np.linalg.norm(v64)),
+                                     "max_abs_over_urms": float(np.abs(vm - v64).max() / urms)}}
+    acc = {p: {"icc": np.zeros(3), "wr": [], "nir": None} for p in g}
+    for p, x in g.items():
+        for _ in range(steps):
+            rep, _gm = x.particle_step()
+            acc[p]["icc"] += np.array(rep.icc[:])
+            if rep.ncontact:
+                acc[p]["wr"].append(x.contacts()[1][:, 11])
+            if rep.written:
+                acc[p]["nir"] = x.histograms(written=True)["nirbin"].astype(np.float64)
+    radius = np.array(g["fp64"].scalars().radius[:len(SETS_UM)])
+    settle = {}
+    for p, x in g.items():
+        yp = x.get_particles()["yp"]
+        sidx = np.argmin(np.abs(yp[:, 6][:, None] - radius[None, :]), axis=1)
+        settle[p] = np.array([yp[sidx == k, 3].mean() for k in range(len(SETS_UM))])
+    out["settling_velocity"] = {"rel_per_set": (np.abs(settle["mixed"] - settle["fp64"]) /
+                                                np.abs(settle["fp64"])).tolist(),
+                                "sets_um": SETS_UM}
+    nm, n64 = acc["mixed"]["nir"], acc["fp64"]["nir"]
+    out["rdf_bins"] = {"rel_l2": float(np.linalg.norm(nm - n64) / max(np.linalg.norm(n64), 1e-300)),
+                       "pairs_counted": int(n64.sum())}
+    wm = np.concatenate(acc["mixed"]["wr"]) if acc["mixed"]["wr"] else np.zeros(0)
+    w64 = np.concatenate(acc["fp64"]["wr"]) if acc["fp64"]["wr"] else np.zeros(0)
+    out["wr_at_contact"] = {"mean_mixed": float(wm.mean()) if wm.size else None,
+                            "mean_fp64": float(w64.mean()) if w64.size else None,
+                            "rel": float(abs(wm.mean() - w64.mean()) / abs(w64.mean())) if wm.size and w64.size else None,
+                            "records": [int(wm.size), int(w64.size)]}
+    cm, c64 = acc["mixed"]["icc"].sum(), acc["fp64"]["icc"].sum()
+    out["collision_kernel"] = {"collisions_mixed": int(cm), "collisions_fp64": int(c64),
+                               "rel": float(abs(cm - c64) / c64) if c64 else None}
+    out["steps"] = steps
+    out["reference"] = "FP64 GPU path (bit-identical to the FP64 oracle on identical inputs)"
+    for x in g.values():
+        x.close()
+    return out
+
+
+C4 = dict(n=512, npart=5_000_000, nu=3e-4, dt=5e-4, etk_dns=0.00484, tauk_dns=0.078, lognormal=(25.0, 0.3),
+          clip_um=(10.0, 60.0))
+
+
+def config4_bench(dev, torch, steps=4):
+    """512^3 stochastic forcing, nu = 3e-4, 5,000,000 lognormal droplets (mean 25 um, sigma
+    0.3, clipped to [10, 60] um) with HDI and coalescence (growth mode), the full mixed path:
+    per-phase device times and the update phase's algorithmic HBM GB/s."""
+    import numpy as np
+    from mpi_2d_domain_decomp_turb_particles_b200 import Partlib, ParticleParams
+    from mpi_2d_domain_decomp_turb_particles_b200.bytes_model import update_bytes
+    from mpi_2d_domain_decomp_turb_particles_b200.flow import Flow
+    from mpi_2d_domain_decomp_turb_particles_b200.synthetic import droplets, spectral_field
+    n, npart = C4["n"], C4["npart"]
+    field = spectral_field(n, seed=1234, device=f"cuda:{dev}")
+    fl = Flow(n, C4["nu"], C4["dt"], forcing=2, iseedf=232300, device=dev)
+    fl.set_velocity(torch.stack(field).contiguous())
+    del field
+    p = ParticleParams(nx=n, npart=npart, radius_um=[10.0, 25.0, 60.0], precision="mixed", device=dev,
+                       new_particle=True, hdi_included=True, nonoverlap=True, hdi_trunc=50.0,
+                       dt=C4["dt"], rnu=C4["nu"], etk_dns=C4["etk_dns"], tauk_dns=C4["tauk_dns"])
+    g = Partlib(p)
+    g.part_init()
+    s = g.scalars()
+    yp = droplets(npart, s.radius[1] / 25.0, lognormal=C4["lognormal"], seed=290710)
+    lo, hi = (c * s.radius[1] / 25.0 for c in C4["clip_um"])
+    yp[:, 6] = np.clip(yp[:, 6], lo, hi)
+    g.set_particles(yp)
+    stream = torch.cuda.Stream(device=dev)
+    g.set_stream(stream)
+    fl.set_stream(stream)
+    g.set_step(40000, 0.0)             # growth mode: COALESCE on contact (turb.f90:591)
+    fl.step(g)
+    g.periodic()
+    g.overlap_det()
+    g.sync()
+    fl.step(g)
+    g.particle_step()
+    torch.cuda.synchronize()
+    flow_ms, step_ms, phases, iters = [], [], [], []
+    for _ in range(steps):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        fl.step(g)
+        e[1].record(stream)
+        _c, gm = g.particle_step()
+        e[2].record(stream)
+        torch.cuda.synchronize()
+        flow_ms.append(e[0].elapsed_time(e[1]))
+        step_ms.append(e[0].elapsed_time(e[2]))
+        phases.append(g.phase_times())
+        iters.append(gm.iterations)
+    ph = np.median(np.array(phases), axis=0)
+    nps = g.nps
+    upd_gbs = update_bytes("mixed", n, nps) / (ph[0] * 1e-3) / 1e9 if ph[0] > 0 else None
+    g.close()
+    fl.close()
+    return {"workload": "512^3 FP64 flow step (stochastic forcing, nu 3e-4) + 5M lognormal droplets (25 um, "
+                        "sigma 0.3, [10, 60] um), HDI (50 radii) and coalescence, mixed",
+            "step_ms": statistics.median(step_ms), "flow_step_ms": statistics.median(flow_ms),
+            "particle_phase_ms": {"interp_advance": ph[0], "cell_list": ph[1], "collision": ph[2], "hdi": ph[3],
+                                  "periodic_coalesce": ph[4], "overlap": ph[5]},
+            "update_phase_algorithmic_gbs": upd_gbs, "droplets_after": nps, "gmres_iterations": iters}
 
 
 ADJ = dict(n=128, np=200_000, radius_um=25.0, nsteps=400, checkpoint_every=20, dt=5e-4,
@@ -385,12 +515,49 @@ def _oracle_sample(npart, n, steps, min_seconds=0.0):
     return npart / dt, orc.num_threads(), dt
 
 
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def _cpu_flow_step(n=N_GRID):
+    """One FP64 flow step of the numpy/scipy restatement (scipy.fft, all cores)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from flow_oracle import FlowOracle
+    rng = np.random.default_rng(3)
+    f = FlowOracle(n, PHYS["rnu"], PHYS["dt"], forcing=1, force=(0.3, 0.2), workers=-1)
+    f.set_velocity(rng.standard_normal((3, n, n, n)))
+    f.step()
+    t = time.perf_counter()
+    f.step()
+    return time.perf_counter() - t
+
+
 def cpu_baseline():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
     npart = 200_000
     v, th, dt = _oracle_sample(npart, N_GRID, 3, min_seconds=10.0)
+    orc.set_num_threads(1)
+    n1 = 20_000
+    v1, _, dt1 = _oracle_sample(n1, N_GRID, 3, min_seconds=4.0)
+    orc.set_num_threads(th)
+    flow_s = _cpu_flow_step()
     return {"value": v, "unit": "particle-updates/s", "cores": th, "kind": "port",
             "sample": f"{npart} droplets on the 256^3 FP64 field, >= 10 s of update steps "
-                      f"(interpolation + history + advance + position), OpenMP over droplets; {dt:.3f} s/step"}
+                      f"(interpolation + history + advance + position), OpenMP over droplets; {dt:.3f} s/step",
+            "cpu_model": _cpu_model(), "one_core_value": v1,
+            "one_core_sample": f"{n1} droplets, 1 thread, {dt1:.3f} s/step",
+            "flow_step_s_256": flow_s,
+            "flow_sample": f"one 256^3 FP64 flow step of the numpy restatement with scipy.fft on {os.cpu_count()} "
+                           f"workers"}
 
 
 def run_reference(args):
@@ -422,6 +589,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint workload")
     ap.add_argument("--no-full", action="store_true", help="skip the flow + HDI full-step workload")
+    ap.add_argument("--no-config4", action="store_true", help="skip the 512^3 / 5M-droplet workload")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

@@ -8,6 +8,7 @@
 #include "dl_internal.cuh"
 
 #include <algorithm>
+#include <unordered_map>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -215,6 +216,32 @@ __global__ void k_coalesce_set(int m, const int *dev, const double *newrad, T sv
 
 template <typename T>
 T *tp(void *p) { return reinterpret_cast<T *>(p); }
+
+__global__ void k_gather_int(int m, const int *idx, const int *src, int *out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) out[i] = src[idx[i]];
+}
+
+__global__ void k_set_ref(int m, const int *dev, const int *newref, int *ref_of_dev)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) ref_of_dev[dev[i]] = newref[i];
+}
+
+// values indexed by reference position that must stay there while droplets are renumbered:
+// gather from the old holders (src), then scatter to the new holders (dst)
+template <typename E>
+__global__ void k_move_by_ref(int m, const int *src, const int *dst, E *p0, E *p1, E *p2, E *tmp, int gather)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    E *p[3] = {p0, p1, p2};
+    for (int c = 0; c < 3; c++) {
+        if (gather) tmp[(int64_t)c * m + i] = p[c][src[i]];
+        else p[c][dst[i]] = tmp[(int64_t)c * m + i];
+    }
+}
 
 // collist rows: for entry e (owned device index, or nps + ghost index) the reference index,
 // the ypn index and yp(1:8) as COLLISION_DET sees it (shifted ghost coordinates, new velocity).
@@ -1263,33 +1290,75 @@ static int coalesce_apply(dl_ctx *c, const std::vector<int> &devs, const std::ve
     return 0;
 }
 
+template <typename E>
+static int pert_keep(dl_ctx *c, const std::vector<int> &src, const std::vector<int> &dst)
+{
+    const int m = (int)src.size();
+    if (m == 0 || !c->pert[0]) return 0;
+    int *d_idx = nullptr;
+    E *tmp = nullptr;
+    DL_CUDA(c, cudaMallocAsync((void **)&d_idx, sizeof(int) * 2 * m, c->stream));
+    DL_CUDA(c, cudaMallocAsync((void **)&tmp, sizeof(E) * 3 * m, c->stream));
+    DL_CUDA(c, cudaMemcpyAsync(d_idx, src.data(), sizeof(int) * m, cudaMemcpyHostToDevice, c->stream));
+    DL_CUDA(c, cudaMemcpyAsync(d_idx + m, dst.data(), sizeof(int) * m, cudaMemcpyHostToDevice, c->stream));
+    E *P[3] = {tp<E>(c->pert[0]), tp<E>(c->pert[1]), tp<E>(c->pert[2])};
+    for (int gather = 1; gather >= 0; gather--) {
+        k_move_by_ref<E><<<dl_blocks(m, 256), 256, 0, c->stream>>>(m, d_idx, d_idx + m, P[0], P[1], P[2], tmp, gather);
+        DL_CHECK_LAUNCH(c);
+    }
+    DL_CUDA(c, cudaFreeAsync(tmp, c->stream));
+    DL_CUDA(c, cudaFreeAsync(d_idx, c->stream));
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));   // the index vectors are host temporaries
+    return 0;
+}
+
+// COALESCE (partlib.f90:3642-3825): the reference's swap-with-last bookkeeping over the
+// collided pairs, run on the host over the few reference positions it touches (looked up
+// on the device), then applied to the device state: new radii and terminal velocities,
+// renumbered reference indices, deleted droplets dropped by a compacting re-sort.
+// pertvel stays at its reference index (COALESCE moves yp, vp, dmove, fvp, fdp only,
+// partlib.f90:3676-3728).
 extern "C" int dl_coalesce(dl_ctx *c)
 {
     CHECK_INIT(c);
     const int np = (int)c->collist.size() / 20;
     if (np == 0) return 0;
-    int n = c->nps;
-    std::vector<int> dev_of_ref(n);
-    DL_CUDA(c, cudaStreamSynchronize(c->stream));
-    DL_CUDA(c, cudaMemcpy(dev_of_ref.data(), c->dev_of_ref, sizeof(int) * n, cudaMemcpyDeviceToHost));
-    // pertvel stays at its reference index (COALESCE moves yp, vp, dmove, fvp, fdp only,
-    // partlib.f90:3676-3728)
-    std::vector<double> pert_by_ref;
-    if (c->pert[0]) {
-        pert_by_ref.resize((size_t)3 * n);
-        int rp = c->mixed ? pert_io_t<float>(c, pert_by_ref.data(), 0) : pert_io_t<double>(c, pert_by_ref.data(), 0);
-        if (rp) return rp;
+    const int n = c->nps;
+    // reference positions the bookkeeping reads: both droplets of every pair and the tail
+    std::vector<int> need;
+    int jmax = 0;
+    for (int i = 0; i < np; i++) {
+        const double *cl = &c->collist[(size_t)i * 20];
+        const int p1 = (int)cl[8], p2 = (int)cl[18];
+        if (p1 <= n) need.push_back(p1 - 1);
+        if (p2 <= n) { need.push_back(p2 - 1); jmax++; }
     }
-    std::vector<int> slot(dev_of_ref);   // reference position -> device droplet (mutated by swaps)
-    std::map<int, double> setrad;        // device droplet -> new radius (or -1 = deleted)
+    for (int q = 0; q < jmax && q < n; q++) need.push_back(n - 1 - q);
+    std::sort(need.begin(), need.end());
+    need.erase(std::unique(need.begin(), need.end()), need.end());
+    const int m = (int)need.size();
+    std::vector<int> got(m);
+    {
+        int *d = nullptr;
+        DL_CUDA(c, cudaMallocAsync((void **)&d, sizeof(int) * 2 * m, c->stream));
+        DL_CUDA(c, cudaMemcpyAsync(d, need.data(), sizeof(int) * m, cudaMemcpyHostToDevice, c->stream));
+        k_gather_int<<<dl_blocks(m, 256), 256, 0, c->stream>>>(m, d, c->dev_of_ref, d + m);
+        DL_CHECK_LAUNCH(c);
+        DL_CUDA(c, cudaMemcpyAsync(got.data(), d + m, sizeof(int) * m, cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaFreeAsync(d, c->stream));
+        DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    std::unordered_map<int, int> orig, slot;   // reference position -> device droplet (slot mutated by swaps)
+    for (int q = 0; q < m; q++) orig[need[q]] = slot[need[q]] = got[q];
+    std::map<int, double> setrad;               // device droplet -> new radius (or -1 = deleted)
     int jj = 0;
     for (int i = 0; i < np; i++) {
         const double *cl = &c->collist[(size_t)i * 20];
-        int p1 = (int)cl[8], p2 = (int)cl[18];
+        const int p1 = (int)cl[8], p2 = (int)cl[18];
         if (p1 <= n) setrad[slot[p1 - 1]] = pow(pow(cl[6], 3.0) + pow(cl[16], 3.0), 1.0 / 3.0);
         if (p2 <= n) {
             jj++;
-            int last = n - jj;   // 0-based position nps-jj+1
+            const int last = n - jj;   // 0-based position nps-jj+1
             setrad[slot[p2 - 1]] = -1.0;
             slot[p2 - 1] = slot[last];
             slot[last] = -1;
@@ -1301,19 +1370,40 @@ extern "C" int dl_coalesce(dl_ctx *c)
     for (auto &kv : setrad) { devs.push_back(kv.first); rads.push_back(kv.second); }
     int r = c->mixed ? coalesce_apply<float>(c, devs, rads) : coalesce_apply<double>(c, devs, rads);
     if (r) return r;
-    // new reference order of the survivors; deleted droplets get reference index -1
-    std::vector<int> rod(n, -1);
-    for (int q = 0; q < newn; q++) rod[slot[q]] = q;
-    DL_CUDA(c, cudaMemcpy(c->ref_of_dev, rod.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    // deleted droplets (radius -1) are dropped by a compacting re-sort
+    // renumbered survivors (new reference q < newn), deleted droplets (-1); the values kept
+    // by reference move from the old holder of q to its new one
+    std::vector<int> mdev, mref, psrc, pdst;
+    for (auto &kv : slot) {
+        const int q = kv.first, d = kv.second;
+        const auto del = setrad.find(d);
+        if (q < newn && d >= 0 && d != orig[q] && !(del != setrad.end() && del->second < 0.0)) {
+            mdev.push_back(d);
+            mref.push_back(q);
+            psrc.push_back(orig[q]);
+            pdst.push_back(d);
+        }
+    }
+    for (auto &kv : setrad)
+        if (kv.second < 0.0) { mdev.push_back(kv.first); mref.push_back(-1); }
+    r = c->mixed ? pert_keep<float>(c, psrc, pdst) : pert_keep<double>(c, psrc, pdst);
+    if (r) return r;
+    if (!mdev.empty()) {
+        const int k = (int)mdev.size();
+        int *d = nullptr;
+        DL_CUDA(c, cudaMallocAsync((void **)&d, sizeof(int) * 2 * k, c->stream));
+        DL_CUDA(c, cudaMemcpyAsync(d, mdev.data(), sizeof(int) * k, cudaMemcpyHostToDevice, c->stream));
+        DL_CUDA(c, cudaMemcpyAsync(d + k, mref.data(), sizeof(int) * k, cudaMemcpyHostToDevice, c->stream));
+        k_set_ref<<<dl_blocks(k, 256), 256, 0, c->stream>>>(k, d, d + k, c->ref_of_dev);
+        DL_CHECK_LAUNCH(c);
+        DL_CUDA(c, cudaFreeAsync(d, c->stream));
+        DL_CUDA(c, cudaStreamSynchronize(c->stream));   // the host vectors are temporaries
+    }
+    // deleted droplets (radius -1) are dropped by a compacting re-sort, which also rebuilds
+    // dev_of_ref from ref_of_dev
     c->has_dead = jj > 0;
     r = launch_brick_sort(c);
     if (r) return r;
     c->nps = newn;
-    if (c->pert[0]) {
-        r = c->mixed ? pert_io_t<float>(c, pert_by_ref.data(), 1) : pert_io_t<double>(c, pert_by_ref.data(), 1);
-        if (r) return r;
-    }
     return 0;
 }
 

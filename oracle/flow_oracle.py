@@ -26,8 +26,9 @@ import numpy as np
 
 
 class FlowOracle:
-    def __init__(self, n, nu, dt, forcing=0, force=(0.0, 0.0), iseedf=232300):
+    def __init__(self, n, nu, dt, forcing=0, force=(0.0, 0.0), iseedf=232300, workers=None):
         self.n, self.nu, self.dt, self.forcing = n, nu, dt, forcing
+        self.workers = workers   # None: numpy's FFT; an int: scipy.fft with that many workers
         self.force = tuple(force)
         nh = n // 2 + 1
         k1 = np.fft.fftfreq(n, 1.0 / n)
@@ -77,9 +78,15 @@ class FlowOracle:
         return self.dealias(self.symmetrize(v))
 
     def fwd(self, f):
+        if self.workers is not None:
+            import scipy.fft
+            return scipy.fft.rfftn(f, axes=(1, 2, 3), workers=self.workers) / self.n ** 3
         return np.fft.rfftn(f, axes=(1, 2, 3)) / self.n ** 3
 
     def inv(self, fh):
+        if self.workers is not None:
+            import scipy.fft
+            return scipy.fft.irfftn(fh, s=(self.n,) * 3, axes=(1, 2, 3), workers=self.workers) * self.n ** 3
         return np.fft.irfftn(fh, s=(self.n,) * 3, axes=(1, 2, 3)) * self.n ** 3
 
     # -- the reference's operations ---------------------------------------------------

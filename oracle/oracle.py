@@ -118,12 +118,17 @@ def _load():
     lib.orc_set_i.argtypes = [vp, C.c_char_p, C.c_int]
     lib.orc_set_d.argtypes = [vp, C.c_char_p, C.c_double]
     lib.orc_num_threads.restype = C.c_int
+    lib.orc_set_num_threads.argtypes = [C.c_int]
     _lib = lib
     return lib
 
 
 def num_threads() -> int:
     return _load().orc_num_threads()
+
+
+def set_num_threads(n: int) -> None:
+    _load().orc_set_num_threads(int(n))
 
 
 class RanPP:

@@ -547,6 +547,15 @@ int orc_num_threads(void)
 #endif
 }
 
+void orc_set_num_threads(int n)
+{
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
 /* ------------------------------------------------------------------------------------
  * COMPLETE_YPN, partlib.f90:761-838 (ghost j of slot jid is pindex(:,jid) of this rank)
  * ---------------------------------------------------------------------------------- */

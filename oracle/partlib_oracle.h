@@ -190,6 +190,7 @@ void orc_size_avg(orc_state *s, double *r_avg, double *r_max_avg);              
 void orc_update_step(orc_state *s, const double *vx, const double *vy, const double *vz,
                      long pitch_y, long pitch_z);
 int  orc_num_threads(void);
+void orc_set_num_threads(int n);   /* OpenMP threads of the update step (n > 0) */
 
 #ifdef __cplusplus
 }

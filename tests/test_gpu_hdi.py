@@ -149,3 +149,28 @@ def test_overlap_under_hdi_is_an_error():
     g.headlist(g.scalars().d_hdi)
     with pytest.raises(Exception, match="DL_E_OVERLAP_HDI"):
         g.nei_list_precomp()
+
+
+def test_hdi_coalescence_keeps_pertvel_by_reference():
+    """Growth mode with HDI: COALESCE renumbers droplets (swap-with-last) while pertvel stays
+    at its reference index (partlib.f90:3676-3728); droplet count, state and pertvel track
+    the FP64 oracle."""
+    f = smooth_field(32)
+    g, o = make_settled(hdi_params("fp64", npart=6000), f)
+    g.set_step(39998, 0.0)
+    o.seti("istep", 39998)
+    merged = 0
+    for step in range(6):
+        n0 = g.nps
+        g.particle_step()
+        o.particle_step(*f)
+        merged += n0 - g.nps
+        assert g.nps == o.nps, step
+        s = g.get_particles()
+        ref = o.yp[:o.nps]
+        assert np.array_equal(s["yp"][:, 6:8], ref[:, 6:8]), step
+        assert np.abs(s["yp"][:, :3] - ref[:, :3]).max() < 1e-12
+        pg = g.get_pertvel()
+        po = o.arr("pertvel")[:3 * o.nps].reshape(-1, 3)
+        assert np.linalg.norm(pg - po) <= 1e-9 * np.linalg.norm(po)
+    assert merged > 0
