@@ -246,6 +246,17 @@ __device__ __forceinline__ int lower_ix(const long long *re, int s, int e, int k
     return s;
 }
 
+// Cell start table: one warp per row, lanes over the x cells; each lane's lower-bound
+// search reads the row's entries, which the warp shares in L1.
+__global__ void k_cell_starts(int nrows, int ncd, const int *row_start, const long long *row_ent, int *cs)
+{
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= nrows) return;
+    const int rs = row_start[row], re = row_start[row + 1];
+    int *out = cs + (int64_t)row * (ncd + 1);
+    for (int ix = 1 + lane; ix <= ncd + 1; ix += 32) out[ix - 1] = lower_ix(row_ent, rs, re, ix);
+}
+
 // FINDINDEX, partlib.f90:1850-1885
 __device__ __forceinline__ void findindex(const DevConst &D, double r1, double r2, int &i1, int &i2)
 {
@@ -272,6 +283,7 @@ struct CollArgs {
     const Ghost *g;
     const int *row_start;
     const long long *row_ent;
+    const int *cell_start;
     const int *ref;
     const double *rad;
     const T *dm[3], *vo[3], *vn[3], *up[3];
@@ -348,7 +360,9 @@ __global__ void __launch_bounds__(128) k_collision(CollArgs<T> A)
             if (hi_raw > D.ncd) { rlo[nr] = 1; rhi[nr] = hi_raw - D.ncd; rsx[nr] = 1.0; nr++; }
             for (int q = 0; q < nr; q++) {
                 const double sx = rsx[q];
-                for (int s = lower_ix(A.row_ent, rs, re_, rlo[q]); s < re_; s++) {
+                int s0, s1;
+                cell_range(A.cell_start, row, D.ncd, rs, re_, rlo[q], rhi[q], s0, s1);
+                for (int s = s0; s < s1; s++) {
                     const long long ke = A.row_ent[s];
                     const int ix2 = (int)(ke >> 32);
                     if (ix2 > rhi[q]) break;
@@ -513,7 +527,8 @@ __global__ void k_accumulate(int nbinsz, const int *hi, const double *hd, int *a
 // OVERLAP_DET sweep (partlib.f90:2069-2156): per owned droplet, number of partners
 // (ypn index > ih1, 27 neighbour cells, half shell) within rcoll.
 __global__ void k_overlap(DevConst D, int nps, const double *px, const double *py, const double *pz, const Ghost *g,
-                          const int *row_start, const long long *row_ent, const int *ref, const double *rad,
+                          const int *row_start, const long long *row_ent, const int *cell_start, const int *ref,
+                          const double *rad,
                           int jmax, int kmax, int2 *hits, int cap, int *cnt)
 {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -538,7 +553,9 @@ __global__ void k_overlap(DevConst D, int nps, const double *px, const double *p
                 double sx = 0.0;
                 if (ix2 < 1) { ix2 = D.ncd + ix2; sx = -1.0; }
                 else if (ix2 > D.ncd) { ix2 = ix2 % D.ncd; sx = 1.0; }
-                for (int s = lower_ix(row_ent, rs, re_, ix2); s < re_; s++) {
+                int s0, s1;
+                cell_range(cell_start, row, D.ncd, rs, re_, ix2, ix2, s0, s1);
+                for (int s = s0; s < s1; s++) {
                     long long ke = row_ent[s];
                     if ((int)(ke >> 32) != ix2) break;
                     int e = (int)(ke & 0xffffffffLL);
@@ -946,6 +963,19 @@ int launch_headlist(dl_ctx *c, double dist)
             DL_CHECK_LAUNCH(c);
         }
     }
+    // per-cell entry starts (the searches of COLLISION_DET, OVERLAP_DET and the HDI walk)
+    const size_t cells = (size_t)c->nrows * (D.ncd + 1);
+    if (c->cell_start_cap < cells) {
+        if (c->cell_start) cudaFree(c->cell_start);
+        c->cell_start = nullptr;
+        c->cell_start_cap = 0;
+        if (cudaMalloc(&c->cell_start, sizeof(int) * cells) != cudaSuccess)
+            return dl_fail(c, DL_E_ALLOC, "HEADLIST: cudaMalloc of the cell start table failed");
+        c->cell_start_cap = cells;
+    }
+    k_cell_starts<<<(int)(((int64_t)c->nrows * 32 + 255) / 256), 256, 0, c->stream>>>(
+        c->nrows, D.ncd, c->row_start, (const long long *)c->row_ent, c->cell_start);
+    DL_CHECK_LAUNCH(c);
     c->hl_dist = dist;
     c->hl_valid = 1;
     return 0;
@@ -967,6 +997,7 @@ static int collision_t(dl_ctx *c, dl_coll_report *rep)
     A.g = c->ghosts;
     A.row_start = c->row_start;
     A.row_ent = (const long long *)c->row_ent;
+    A.cell_start = c->cell_start;
     A.ref = c->ref_of_dev;
     A.rad = c->rad;
     const int vnew = c->have_vnew ? c->vnew : c->vcur;
@@ -1063,7 +1094,8 @@ int launch_overlap_sweep(dl_ctx *c, std::vector<int2> &hits)
     if (c->nps > 0) {
         k_overlap<<<dl_blocks(c->nps, 128), 128, 0, c->stream>>>(
             D, c->nps, c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2], c->ghosts, c->row_start,
-            (const long long *)c->row_ent, c->ref_of_dev, c->rad, jmax, kmax, c->ovl_list, c->ovl_cap, c->ovl_cnt);
+            (const long long *)c->row_ent, c->cell_start, c->ref_of_dev, c->rad, jmax, kmax, c->ovl_list, c->ovl_cap,
+            c->ovl_cnt);
         DL_CHECK_LAUNCH(c);
     }
     int n = 0;

@@ -43,10 +43,18 @@ struct Grid {
 __device__ __forceinline__ void mode_of(const Grid &G, int64_t m, int &x, int &y, int &z, double &kx, double &ky,
                                         double &kz)
 {
-    x = (int)(m % G.nh);
-    const int64_t zy = m / G.nh;
-    y = (int)(zy % G.n);
-    z = (int)(zy / G.n);
+    if (G.M <= 0x7fffffff) {   // 32-bit index arithmetic (every grid up to 1024^3)
+        const unsigned mu = (unsigned)m, nh = (unsigned)G.nh, nn = (unsigned)G.n;
+        const unsigned zy = mu / nh;
+        x = (int)(mu - zy * nh);
+        z = (int)(zy / nn);
+        y = (int)(zy - (unsigned)z * nn);
+    } else {
+        x = (int)(m % G.nh);
+        const int64_t zy = m / G.nh;
+        y = (int)(zy % G.n);
+        z = (int)(zy / G.n);
+    }
     kx = (double)x;
     ky = (double)(y < G.n / 2 + 1 ? y : y - G.n);
     kz = (double)(z < G.n / 2 + 1 ? z : z - G.n);
@@ -122,15 +130,17 @@ __global__ void k_update(UpdArgs A)
             v[c].y = v[c].y + A.dt * a[1];
         }
     }
-    // projection onto divergence-free modes (turb.f90:669-672)
-    const double tr = (kx * v[0].x + ky * v[1].x + kz * v[2].x) / k2;
-    const double ti = (kx * v[0].y + ky * v[1].y + kz * v[2].y) / k2;
+    // projection onto divergence-free modes (turb.f90:669-672); one reciprocal each for
+    // k^2 and the Crank-Nicolson denominator
+    const double ik2 = 1.0 / k2;
+    const double tr = (kx * v[0].x + ky * v[1].x + kz * v[2].x) * ik2;
+    const double ti = (kx * v[0].y + ky * v[1].y + kz * v[2].y) * ik2;
     const double kk[3] = {kx, ky, kz};
-    const double den = 1.0 + A.nu * dth * k2;
+    const double iden = 1.0 / (1.0 + A.nu * dth * k2);
     for (int c = 0; c < 3; c++) {
         double2 w;
-        w.x = (v[c].x - kk[c] * tr) / den;
-        w.y = (v[c].y - kk[c] * ti) / den;
+        w.x = (v[c].x - kk[c] * tr) * iden;
+        w.y = (v[c].y - kk[c] * ti) * iden;
         A.u[c * A.G.M + m] = w;
     }
 }

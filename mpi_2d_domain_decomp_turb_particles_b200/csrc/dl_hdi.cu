@@ -64,17 +64,6 @@ __device__ __forceinline__ int nei_row(const DevConst &D, int iy, int iz)
     return (iz - (1 - D.nz_max)) * D.nyh + (iy - (1 - D.ny_max));
 }
 
-__device__ __forceinline__ int first_ix(const long long *re, int s, int e, int key)
-{
-    const long long k = (long long)key << 32;
-    while (s < e) {
-        const int m = (s + e) >> 1;
-        if (re[m] < k) s = m + 1;
-        else e = m;
-    }
-    return s;
-}
-
 // Stokes disturbance tensor of a sphere of radius arad at separation xd (partlib.f90:3318-3331)
 __device__ __forceinline__ void stokes_tensor(double arad, double dnij, const double *xd, double *c6)
 {
@@ -91,6 +80,13 @@ __device__ __forceinline__ void stokes_tensor(double arad, double dnij, const do
     c6[5] = gamma * (xd[2] * xd[2]) + beta;
 }
 
+// One neighbour entry as the walk finds it (scattered into the CSR afterwards).
+struct NeiApp {
+    int owner, partner;
+    unsigned long long key;
+    double coef[6];
+};
+
 struct NeiArgs {
     DevConst D;
     int nps;
@@ -99,34 +95,40 @@ struct NeiArgs {
     const Ghost *g;
     const int *row_start;
     const long long *row_ent;
-    int *cnt;                     // count pass: entries per owner
-    const int *start;             // fill pass: CSR offsets
-    int *fill;                    // fill pass: per-owner cursors
-    int *partner;                 // device index of the partner (its source droplet for ghosts)
-    unsigned long long *key;      // append-order key
-    double *coef;                 // 6 FP64 coefficients per entry
-    int *flag;                    // [0] overlapping owner + 1, [1] fill overflow
+    const int *cell_start;
+    int *cnt;                     // entries per owner
+    NeiApp *app;                  // appended entries
+    unsigned long long *napp;     // appended count (may exceed app_cap: then the walk is redone)
+    unsigned long long app_cap;
+    int *flag;                    // [0] overlapping owner + 1
 };
 
-template <bool FILL>
 __device__ __forceinline__ void nei_emit(const NeiArgs &A, int owner, int partner, unsigned long long key,
                                          double arad, double dnij, const double *xd)
 {
-    if (!FILL) {
-        atomicAdd(&A.cnt[owner], 1);
-        return;
-    }
-    const int slot = A.start[owner] + atomicAdd(&A.fill[owner], 1);
-    if (slot >= A.start[owner + 1]) {   // the count pass saw fewer: never expected
-        A.flag[1] = 1;
-        return;
-    }
-    A.partner[slot] = partner;
-    A.key[slot] = key;
-    stokes_tensor(arad, dnij, xd, A.coef + (int64_t)slot * 6);
+    atomicAdd(&A.cnt[owner], 1);
+    const unsigned long long slot = atomicAdd(A.napp, 1ull);
+    if (slot >= A.app_cap) return;
+    NeiApp &e = A.app[slot];
+    e.owner = owner;
+    e.partner = partner;
+    e.key = key;
+    stokes_tensor(arad, dnij, xd, e.coef);
 }
 
-template <bool FILL>
+// appended entries -> CSR slots of their owners (order fixed afterwards by k_nei_sort)
+__global__ void k_nei_scatter(int nnz, const NeiApp *app, const int *start, int *fill, int *partner,
+                              unsigned long long *key, double *coef)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnz) return;
+    const NeiApp &e = app[i];
+    const int slot = start[e.owner] + atomicAdd(&fill[e.owner], 1);
+    partner[slot] = e.partner;
+    key[slot] = e.key;
+    for (int t = 0; t < 6; t++) coef[(int64_t)slot * 6 + t] = e.coef[t];
+}
+
 __global__ void __launch_bounds__(128) k_nei_walk(NeiArgs A)
 {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -156,7 +158,9 @@ __global__ void __launch_bounds__(128) k_nei_walk(NeiArgs A)
             if (rs == re) continue;
             const int jrel = j - (iy - D.ny_max), krel = k - (iz - D.nz_max);
             for (int q = 0; q < nr; q++) {
-                for (int s = first_ix(A.row_ent, rs, re, rlo[q]); s < re; s++) {
+                int s0, s1;
+                cell_range(A.cell_start, row, D.ncd, rs, re, rlo[q], rhi[q], s0, s1);
+                for (int s = s0; s < s1; s++) {
                     const long long ke = A.row_ent[s];
                     const int ix2 = (int)(ke >> 32);
                     if (ix2 > rhi[q]) break;
@@ -190,11 +194,11 @@ __global__ void __launch_bounds__(128) k_nei_walk(NeiArgs A)
                         const unsigned cell = (unsigned)((irel * nj + jrel) * nk + krel);
                         const unsigned long long key = (1ull << 62) | ((unsigned long long)cell << 32) |
                                                        (unsigned long long)(0xffffffffu - (unsigned)ypn2);
-                        nei_emit<FILL>(A, a, src, key, rb, dnij, xd);
+                        nei_emit(A, a, src, key, rb, dnij, xd);
                     }
                     if (!ghost && dnij < trunc * ra) {
                         const double nxd[3] = {-xd[0], -xd[1], -xd[2]};
-                        nei_emit<FILL>(A, src, a, (unsigned long long)(refa + 1), ra, dnij, nxd);
+                        nei_emit(A, src, a, (unsigned long long)(refa + 1), ra, dnij, nxd);
                     }
                 }
             }
@@ -766,6 +770,13 @@ int launch_nei_list(dl_ctx *c)
         c->nei_valid = 1;
         return 0;
     }
+    if (!c->nei_app) {
+        c->nei_app_cap = std::max<size_t>(4096, (size_t)nps);
+        if (cudaMalloc(&c->nei_app, sizeof(NeiApp) * c->nei_app_cap + 16) != cudaSuccess)
+            return dl_fail(c, DL_E_ALLOC, "NEI_LIST_PRECOMP: cudaMalloc of the entry buffer failed");
+    }
+    unsigned long long *d_napp = reinterpret_cast<unsigned long long *>(
+        reinterpret_cast<char *>(c->nei_app) + sizeof(NeiApp) * c->nei_app_cap);
     NeiArgs A;
     A.D = c->dc;
     A.nps = nps;
@@ -775,22 +786,42 @@ int launch_nei_list(dl_ctx *c)
     A.g = c->ghosts;
     A.row_start = c->row_start;
     A.row_ent = (const long long *)c->row_ent;
+    A.cell_start = c->cell_start;
     A.cnt = c->nei_cnt;
-    A.start = c->nei_start;
-    A.fill = c->nei_fill;
-    A.partner = c->nei_idx;
-    A.key = c->nei_key;
-    A.coef = c->nei_coef64;
+    A.app = reinterpret_cast<NeiApp *>(c->nei_app);
+    A.napp = d_napp;
+    A.app_cap = c->nei_app_cap;
     A.flag = c->overlap_flag;
-    k_nei_walk<false><<<dl_blocks(nps, 128), 128, 0, c->stream>>>(A);
-    DL_CHECK_LAUNCH(c);
+    unsigned long long napp = 0;
+    for (int attempt = 0; attempt < 2; attempt++) {
+        // one walk finds every entry: counts per owner and the entries themselves
+        DL_CUDA(c, cudaMemsetAsync(d_napp, 0, sizeof(unsigned long long), c->stream));
+        if (attempt) DL_CUDA(c, cudaMemsetAsync(c->nei_cnt, 0, sizeof(int) * (m + 1), c->stream));
+        k_nei_walk<<<dl_blocks(nps, 128), 128, 0, c->stream>>>(A);
+        DL_CHECK_LAUNCH(c);
+        DL_CUDA(c, cudaMemcpyAsync(&napp, d_napp, sizeof(napp), cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaStreamSynchronize(c->stream));
+        if (napp <= c->nei_app_cap) break;
+        // more entries than the buffer holds: grow it and walk again
+        cudaFree(c->nei_app);
+        c->nei_app = nullptr;
+        c->nei_app_cap = napp + napp / 4;
+        if (cudaMalloc(&c->nei_app, sizeof(NeiApp) * c->nei_app_cap + 16) != cudaSuccess)
+            return dl_fail(c, DL_E_ALLOC, "NEI_LIST_PRECOMP: cudaMalloc of the entry buffer failed");
+        d_napp = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(c->nei_app) +
+                                                        sizeof(NeiApp) * c->nei_app_cap);
+        A.app = reinterpret_cast<NeiApp *>(c->nei_app);
+        A.napp = d_napp;
+        A.app_cap = c->nei_app_cap;
+    }
+    if (napp > c->nei_app_cap) return dl_fail(c, DL_E_STATE, "NEI_LIST_PRECOMP: entry buffer still too small");
     // CSR offsets and the capacity check (the reference allows nei_max = 100 per droplet)
     DL_CUDA(c, dl_scan_counts(c->stream, c->nei_cnt, c->nei_start, nps, c->nei_blk, c->overlap_flag + 2));
     c->launches += 3;
-    int hf[4] = {0, 0, 0, 0}, nnz = 0;
+    int hf[4] = {0, 0, 0, 0};
     DL_CUDA(c, cudaMemcpyAsync(hf, c->overlap_flag, sizeof(int) * 4, cudaMemcpyDeviceToHost, c->stream));
-    DL_CUDA(c, cudaMemcpyAsync(&nnz, c->nei_start + nps, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    const int nnz = (int)napp;
     if (hf[0]) {
         int ref = -1;
         DL_CUDA(c, cudaMemcpy(&ref, c->ref_of_dev + (hf[0] - 1), sizeof(int), cudaMemcpyDeviceToHost));
@@ -814,12 +845,10 @@ int launch_nei_list(dl_ctx *c)
             (c->mixed && cudaMalloc(&c->nei_coef, sizeof(float) * 6 * cap) != cudaSuccess))
             return dl_fail(c, DL_E_ALLOC, "NEI_LIST_PRECOMP: cudaMalloc of the neighbour lists failed");
         c->nei_cap = cap;
-        A.partner = c->nei_idx;
-        A.key = c->nei_key;
-        A.coef = c->nei_coef64;
     }
     if (nnz > 0) {
-        k_nei_walk<true><<<dl_blocks(nps, 128), 128, 0, c->stream>>>(A);
+        k_nei_scatter<<<dl_blocks(nnz, 256), 256, 0, c->stream>>>(nnz, A.app, c->nei_start, c->nei_fill, c->nei_idx,
+                                                                  c->nei_key, c->nei_coef64);
         DL_CHECK_LAUNCH(c);
         k_nei_sort<<<dl_blocks(nps, 128), 128, 0, c->stream>>>(nps, c->nei_start, c->nei_key, c->nei_idx,
                                                                c->nei_coef64);
@@ -830,10 +859,6 @@ int launch_nei_list(dl_ctx *c)
                                                                                          tp<float>(c->nei_coef));
             DL_CHECK_LAUNCH(c);
         }
-        int ovf = 0;
-        DL_CUDA(c, cudaMemcpyAsync(&ovf, c->overlap_flag + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-        DL_CUDA(c, cudaStreamSynchronize(c->stream));
-        if (ovf) return dl_fail(c, DL_E_STATE, "NEI_LIST_PRECOMP: count and fill passes disagree");
     }
     c->nnz = nnz;
     c->nei_valid = 1;

@@ -139,6 +139,8 @@ struct dl_ctx {
     int *row_start;              // nrows + 1
     int *row_fill;
     int64_t *row_ent;            // sorted (ix << 32 | entry) per row
+    int *cell_start;             // [nrows][ncd + 1]: first entry of cell ix (ix - 1), then the row end
+    size_t cell_start_cap;
     int nrows;
     int *long_rows;              // rows longer than the per-thread sort limit
     int *n_long;
@@ -197,6 +199,8 @@ struct dl_ctx {
     void *nei_coef;              // 6 FP32 coefficients per entry (mixed)
     double *nei_coef64;          // 6 FP64 coefficients per entry (reference arithmetic)
     size_t nei_cap;
+    void *nei_app;               // entries appended by the neighbour walk, before the CSR scatter
+    size_t nei_app_cap;
     int nnz, nei_valid;
     int *overlap_flag;           // [0] overlapping owner + 1, [1] fill overflow, [2] largest count
     // GMRES work
@@ -239,6 +243,15 @@ int dl_fail(dl_ctx *c, int code, const std::string &msg);
         (ctx)->launches++;                   \
         DL_CUDA(ctx, cudaGetLastError());    \
     } while (0)
+// Entries of cells lo..hi (x cell indices, 1-based) of one row of the cell list: [s0, s1).
+// Indices outside 1..ncd clamp to the row's ends, as a lower-bound search would.
+__device__ __forceinline__ void cell_range(const int *cs, int row, int ncd, int rs, int re, int lo, int hi, int &s0,
+                                           int &s1)
+{
+    const int64_t base = (int64_t)row * (ncd + 1);
+    s0 = lo <= 1 ? rs : (lo > ncd ? re : cs[base + lo - 1]);
+    s1 = hi >= ncd ? re : (hi < 1 ? rs : cs[base + hi]);
+}
 #define CHECK_INIT(c)                                                                   \
     do {                                                                                \
         if (!(c)) return DL_E_ARG;                                                      \
