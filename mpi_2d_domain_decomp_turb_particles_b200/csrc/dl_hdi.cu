@@ -331,15 +331,44 @@ __global__ void __launch_bounds__(kRedThreads) k_mgs(int64_t n, T *v, const T *q
 {
     __shared__ T sh[32];
     const T h = q_prev ? *h_prev : (T)0;
-    T s = (T)0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    // four independent elements per trip keep more loads in flight per thread
+    const int64_t st = (int64_t)gridDim.x * blockDim.x;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    T s4[4] = {(T)0, (T)0, (T)0, (T)0};
+    for (; i + 3 * st < n; i += 4 * st) {
+        T vi[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) vi[k] = v[i + k * st];
+        if (q_prev) {
+            T qp[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) qp[k] = q_prev[i + k * st];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                vi[k] = vi[k] - h * qp[k];
+                v[i + k * st] = vi[k];
+            }
+        }
+        if (q_next) {
+            T qn[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) qn[k] = q_next[i + k * st];
+#pragma unroll
+            for (int k = 0; k < 4; k++) s4[k] += qn[k] * vi[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) s4[k] += vi[k] * vi[k];
+        }
+    }
+    for (; i < n; i += st) {
         T vi = v[i];
         if (q_prev) {
             vi = vi - h * q_prev[i];
             v[i] = vi;
         }
-        s += q_next ? q_next[i] * vi : vi * vi;
+        s4[0] += q_next ? q_next[i] * vi : vi * vi;
     }
+    T s = (s4[0] + s4[1]) + (s4[2] + s4[3]);
     s = block_sum(s, sh);
     finish_reduction(s, partials, out, ticket, sh);
 }
@@ -349,9 +378,18 @@ template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_sumsq(int64_t n, const T *x, T *out, T *partials, unsigned *ticket)
 {
     __shared__ T sh[32];
-    T s = (T)0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        s += x[i] * x[i];
+    const int64_t st = (int64_t)gridDim.x * blockDim.x;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    T s4[4] = {(T)0, (T)0, (T)0, (T)0};
+    for (; i + 3 * st < n; i += 4 * st) {
+        T xv[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) xv[k] = x[i + k * st];
+#pragma unroll
+        for (int k = 0; k < 4; k++) s4[k] += xv[k] * xv[k];
+    }
+    for (; i < n; i += st) s4[0] += x[i] * x[i];
+    T s = (s4[0] + s4[1]) + (s4[2] + s4[3]);
     s = block_sum(s, sh);
     finish_reduction(s, partials, out, ticket, sh);
 }
@@ -360,7 +398,8 @@ template <typename T>
 __global__ void k_scale_div(int64_t n, const T *v, const T *h, T *q)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) q[i] = v[i] / *h;
+    const T inv = (T)1 / *h;
+    if (i < n) q[i] = v[i] * inv;
 }
 
 template <typename T>
