@@ -560,6 +560,33 @@ def cpu_baseline():
                            f"workers"}
 
 
+def run_only(args):
+    """One workload alone, for profilers (ncu launch lists and kernel captures): prints
+    a short JSON line with its device time; no baselines, no extra workloads."""
+    import torch
+    torch.cuda.set_device(0)
+    from mpi_2d_domain_decomp_turb_particles_b200.synthetic import spectral_field
+    out = {"only": args.only}
+    if args.only in ("update", "update-fp64"):
+        field = spectral_field(N_GRID, seed=1234, device="cuda:0")
+        g = _make("mixed" if args.only == "update" else "fp64", 0)
+        stream = torch.cuda.Stream()
+        g.set_stream(stream)
+        g.set_fields(*field)
+        g.sync()
+        ms, kms, launches = _time_update(g, stream, args.steps, args.warmup, torch)
+        out.update(ms_per_step=ms, kernel_ms=kms, launches=launches)
+        g.close()
+    elif args.only == "adjoint":
+        out.update(adjoint_bench(0, torch))
+    elif args.only == "full":
+        field = spectral_field(N_GRID, seed=1234, device="cuda:0")
+        out.update(full_step_bench(0, torch, field))
+    elif args.only == "config4":
+        out.update(config4_bench(0, torch))
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args):
     ws, rank, local = _dist()
     if rank != 0:
@@ -590,10 +617,14 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint workload")
     ap.add_argument("--no-full", action="store_true", help="skip the flow + HDI full-step workload")
     ap.add_argument("--no-config4", action="store_true", help="skip the 512^3 / 5M-droplet workload")
+    ap.add_argument("--only", choices=["update", "update-fp64", "adjoint", "full", "config4"],
+                    help="run one workload alone (for profilers)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         run_reference(args)
+    elif args.only:
+        run_only(args)
     else:
         run_ours(args)
 
