@@ -659,12 +659,23 @@ __global__ void k_scan_single(const int *cnt, int *start, int m)
     if (threadIdx.x == 0) start[m] = carry;
 }
 
+// Slots within a brick: lanes of a warp that share a brick take consecutive slots in lane
+// order (one atomic per brick per warp), so runs of droplets that stay in their brick
+// keep their relative order and the permutation gathers them in coalesced runs.
 __global__ void k_brick_scatter(int nps, const int *keys, const int *start, int *fill, int *perm)
 {
-    int d = blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= nps) return;
-    int k = keys[d];
-    perm[start[k] + atomicAdd(&fill[k], 1)] = d;
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = d < nps;
+    const int k = live ? keys[d] : -1;
+    const unsigned act = __ballot_sync(0xffffffffu, live);
+    if (!live) return;
+    const unsigned peers = __match_any_sync(act, k);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&fill[k], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    perm[start[k] + base + __popc(peers & ((1u << lane) - 1u))] = d;
 }
 
 template <typename E>
