@@ -44,6 +44,22 @@ def _dist():
     return ws, rank, local
 
 
+def max_over_ranks(values, ws, device="cpu"):
+    """Element-wise max of per-rank timings (the replica run's device times; every rank
+    takes this collective at the same point)."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def replica_value(ws, npart, ms_per_step):
+    """Whole-job particle-updates/s of ws replicas, each updating npart droplets per step."""
+    return ws * npart / (ms_per_step * 1e-3)
+
+
 def _clock_sampler(dev: int):
     cmd = ["nvidia-smi", f"--id={dev}",
            "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
@@ -157,11 +173,8 @@ def run_ours(args):
         dist.barrier()
     ms_step, kernel_ms, launches = _time_update(g, stream, args.steps, args.warmup, torch)
     clocks = _clock_summary(clk)
-    t = torch.tensor([ms_step, kernel_ms], device=f"cuda:{dev}", dtype=torch.float64)
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_step, kernel_ms = float(t[0]), float(t[1])
-    value = ws * N_PART / (ms_step * 1e-3)
+    ms_step, kernel_ms = max_over_ranks([ms_step, kernel_ms], ws, device=f"cuda:{dev}")
+    value = replica_value(ws, N_PART, ms_step)
 
     # ---- full particle substep (cell lists, collision detection and statistics) ----
     full = []
@@ -205,10 +218,8 @@ def run_ours(args):
     g64.sync()
     ms64, kms64, _ = _time_update(g64, stream, max(3, args.steps // 2), args.warmup, torch)
     g64.close()
-    t64 = torch.tensor([ms64], device=f"cuda:{dev}", dtype=torch.float64)
-    if ws > 1:
-        dist.all_reduce(t64, op=dist.ReduceOp.MAX)
-    value64 = ws * N_PART / (float(t64[0]) * 1e-3)
+    (ms64,) = max_over_ranks([ms64], ws, device=f"cuda:{dev}")
+    value64 = replica_value(ws, N_PART, ms64)
 
     errs = errors_bench(dev, torch, field)
     adj = adjoint_bench(dev, torch) if not args.no_adjoint else None
@@ -233,7 +244,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (positions f64)", "data": "synthetic (seeded spectrum field, uniform droplets)",
             "config": CONFIG,
-            "fp64_value": value64, "fp64_ms_per_step": float(t64[0]), "mixed_over_fp64": value / value64,
+            "fp64_value": value64, "fp64_ms_per_step": ms64, "mixed_over_fp64": value / value64,
             "full_step_ms": full_ms, "collision_ms": coll_ms,
             "collision_candidate_pairs_per_s": cand / (coll_ms * 1e-3) if coll_ms > 0 else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -591,7 +602,7 @@ def run_reference(args):
     ws, rank, local = _dist()
     if rank != 0:
         return
-    npart = 200_000
+    npart = args.ref_sample
     for _ in range(args.warmup):
         pass
     v, th, dt = _oracle_sample(npart, N_GRID, args.steps)
@@ -617,6 +628,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint workload")
     ap.add_argument("--no-full", action="store_true", help="skip the flow + HDI full-step workload")
     ap.add_argument("--no-config4", action="store_true", help="skip the 512^3 / 5M-droplet workload")
+    ap.add_argument("--ref-sample", type=int, default=200_000,
+                    help="droplets per step of the reference arm's CPU sample")
     ap.add_argument("--only", choices=["update", "update-fp64", "adjoint", "full", "config4"],
                     help="run one workload alone (for profilers)")
     args = ap.parse_args()
