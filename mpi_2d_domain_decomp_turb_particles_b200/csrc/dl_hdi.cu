@@ -43,7 +43,7 @@ constexpr int kMaxIter = 50;            // partlib.f90:2813
 constexpr double kMaxErr = 1.0e-6;      // partlib.f90:2814
 constexpr double kSmallRhs = 1.0e-5;    // partlib.f90:2853-2856: nothing to solve
 constexpr int kMaxRefine = 4;           // FP64 refinement sweeps of the mixed solve
-constexpr int kRedGrid = 296;           // reduction grid: 2 CTAs per SM
+constexpr int kRedGrid = 1184;          // reduction grid: 8 CTAs of 256 threads per SM
 constexpr int kRedThreads = 256;
 
 // ---------------------------------------------------------------------------------------

@@ -815,18 +815,22 @@ __global__ void k_update_pos(int nps, const double *px, const double *py, const 
 }
 
 // FP64 reference-layout field -> halo-padded copy in precision T (periodic images)
+// (grid: x in blocks of blockDim.x, one padded row (y, z) per blockIdx.y, blockIdx.z)
+__device__ __forceinline__ int wrap_pad(int p, int n)
+{
+    const int g = p - DL_PAD_LO;
+    return g < 0 ? g + n : (g >= n ? g - n : g);
+}
+
 template <typename T>
 __global__ void k_convert_field(const double *v, int64_t py, int64_t pz, int n, T *out, int64_t opy, int64_t opz)
 {
     const int e = n + DL_PAD_LO + DL_PAD_HI;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int64_t tot = (int64_t)e * e * e;
-    if (i >= tot) return;
-    int x = (int)(i % e);
-    int64_t yz = i / e;
-    int y = (int)(yz % e), z = (int)(yz / e);
-    int gx = wrapi(x - DL_PAD_LO, n), gy = wrapi(y - DL_PAD_LO, n), gz = wrapi(z - DL_PAD_LO, n);
-    out[x + opy * y + opz * z] = (T)v[gx + py * gy + pz * gz];
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= e) return;
+    const int y = blockIdx.y, z = blockIdx.z;
+    const double *src = v + py * wrap_pad(y, n) + pz * wrap_pad(z, n);
+    out[x + opy * y + opz * z] = (T)src[wrap_pad(x, n)];
 }
 
 // MEAN_VEL partial sums (partlib.f90:1910-1930) -> 11*nset doubles via FP64 atomics.
@@ -1163,17 +1167,16 @@ int launch_update_position(dl_ctx *c, int)
 int launch_convert_field(dl_ctx *c, int icpt)
 {
     const int n = c->dc.n, e = n + DL_PAD_LO + DL_PAD_HI;
-    int64_t tot = (int64_t)e * e * e;
-    const unsigned blocks = (unsigned)((tot + 255) / 256);
+    const dim3 grid((unsigned)((e + 127) / 128), (unsigned)e, (unsigned)e);
     const int k = icpt - 1;
     if (c->mixed)
-        k_convert_field<float><<<blocks, 256, 0, c->stream>>>(c->f64[k], c->fpy[k], c->fpz[k], n,
-                                                              (float *)c->fpad + (int64_t)k * c->fp_comp,
-                                                              c->fp_pitch, c->fp_plane);
+        k_convert_field<float><<<grid, 128, 0, c->stream>>>(c->f64[k], c->fpy[k], c->fpz[k], n,
+                                                             (float *)c->fpad + (int64_t)k * c->fp_comp,
+                                                             c->fp_pitch, c->fp_plane);
     else
-        k_convert_field<double><<<blocks, 256, 0, c->stream>>>(c->f64[k], c->fpy[k], c->fpz[k], n,
-                                                               (double *)c->fpad + (int64_t)k * c->fp_comp,
-                                                               c->fp_pitch, c->fp_plane);
+        k_convert_field<double><<<grid, 128, 0, c->stream>>>(c->f64[k], c->fpy[k], c->fpz[k], n,
+                                                              (double *)c->fpad + (int64_t)k * c->fp_comp,
+                                                              c->fp_pitch, c->fp_plane);
     DL_CHECK_LAUNCH(c);
     return 0;
 }
