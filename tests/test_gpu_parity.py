@@ -326,6 +326,7 @@ def test_coalescence_growth_mode_matches_oracle():
     g.set_step(39998, 0.0)
     o.seti("istep", 39998)
     merged = 0
+    mass0 = np.sum(g.get_particles()["yp"][:, 6] ** 3)
     for step in range(8):
         n0 = g.nps
         rep, _ = g.particle_step()
@@ -334,3 +335,5 @@ def test_coalescence_growth_mode_matches_oracle():
         assert g.nps == o.nps, f"step {step}"
         assert np.array_equal(gpu_state(g), oracle_state(o)), f"step {step}"
     assert merged > 0
+    # COALESCE conserves droplet mass: a^3 = a1^3 + a2^3 (partlib.f90:3684)
+    assert abs(np.sum(g.get_particles()["yp"][:, 6] ** 3) - mass0) <= 1e-12 * mass0
