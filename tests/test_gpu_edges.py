@@ -1,0 +1,103 @@
+"""Edge cases of the device path against the oracle: an empty population, a single
+droplet, droplets on the faces of the periodic box, and the capacity errors the library
+reports where the reference has no check (contact records, HDI neighbours)."""
+import numpy as np
+import pytest
+
+import oracle as orc
+from cases import dense_params, smooth_field
+from mpi_2d_domain_decomp_turb_particles_b200 import Partlib
+from mpi_2d_domain_decomp_turb_particles_b200._lib import DropletError
+
+pytestmark = pytest.mark.gpu
+
+
+def test_empty_population_runs_every_stage():
+    n = 32
+    f = smooth_field(n)
+    for hdi in (False, True):
+        p = dense_params(n=n, npart=0, hdi_included=hdi, nonoverlap=hdi)
+        g = Partlib(p)
+        g.part_init()
+        g.set_fields(*f)
+        assert g.nps == 0
+        g.update_step()
+        rep, gm = g.particle_step()
+        assert g.nps == 0 and rep.ncoll == 0 and rep.ncontact == 0 and gm.iterations == 0
+        assert g.get_particles()["yp"].shape == (0, 8)
+        assert len(g.contacts()[0]) == 0 and len(g.pairs()) == 0
+        assert not g.histograms(written=False)["nirbin"].any()
+        g.close()
+
+
+def test_single_droplet_matches_oracle():
+    n = 32
+    f = smooth_field(n)
+    p = dense_params(n=n, npart=1)
+    g = Partlib(p)
+    g.part_init()
+    o = orc.Oracle(**p.oracle_kwargs())
+    o.part_init()
+    g.set_fields(*f)
+    for _ in range(6):
+        g.particle_step()
+        o.particle_step(*f)
+    s = g.get_particles()
+    assert g.nps == o.nps == 1
+    assert np.array_equal(s["yp"], o.yp[:1])
+
+
+def test_droplets_on_box_faces_match_oracle():
+    """Positions 0 and just inside 2 pi on every axis: wrap, departure flags and the
+    PERIODIC order as the oracle has them."""
+    n = 32
+    f = smooth_field(n)
+    p = dense_params(n=n, npart=200)
+    g = Partlib(p)
+    g.part_init()
+    o = orc.Oracle(**p.oracle_kwargs())
+    o.part_init()
+    yp = o.yp[:o.nps].copy()
+    top = np.nextafter(2 * np.pi, 0.0)
+    for i, (ax, v) in enumerate([(0, 0.0), (1, 0.0), (2, 0.0), (0, top), (1, top), (2, top)] * 10):
+        yp[i, ax] = v
+    o.yp[:o.nps] = yp
+    g.set_particles(yp)
+    g.set_fields(*f)
+    for _ in range(5):
+        g.particle_step()
+        o.particle_step(*f)
+    assert g.nps == o.nps
+    assert np.array_equal(g.get_particles()["yp"], o.yp[:o.nps])
+
+
+def test_contact_capacity_is_an_error():
+    """Ten pairs placed inside the contact shell; a capacity of one contact record per
+    step must fail with DL_E_CAPACITY (the reference has no check)."""
+    n = 32
+    f = smooth_field(n)
+    g = Partlib(dense_params(n=n, npart=6000, mevent=1))
+    g.part_init()
+    g.set_fields(*f)
+    yp = g.get_particles()["yp"]
+    for i in range(10):
+        a, b = 2 * i, 2 * i + 1
+        yp[b, :3] = yp[a, :3]
+        yp[b, 0] = (yp[a, 0] + 1.001 * (yp[a, 6] + yp[b, 6])) % (2 * np.pi)
+    g.set_particles(yp)
+    with pytest.raises(DropletError, match="CAPACITY"):
+        g.particle_step()
+    g.close()
+
+
+def test_hdi_neighbour_capacity_is_an_error():
+    n = 32
+    p = dense_params(n=n, npart=6000, hdi_included=True, nonoverlap=True, hdi_trunc=30.0, nei_max=1)
+    g = Partlib(p)
+    g.part_init()
+    g.set_fields(*smooth_field(n))
+    g.periodic()
+    g.overlap_det()
+    with pytest.raises(DropletError, match="NEI_CAPACITY"):
+        g.particle_step()
+    g.close()
