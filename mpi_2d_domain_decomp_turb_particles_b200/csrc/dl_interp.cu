@@ -120,7 +120,7 @@ struct GlobalLoaderPad {
 template <typename T>
 struct InterpArgs {
     int n, nps;
-    double dx, pi2;
+    double dx, inv_dx, pi2;
     const double *px, *py, *pz;     // current positions
     const int *brick_start;
     int nbx, nby, nbricks;
@@ -219,12 +219,24 @@ __device__ __forceinline__ void advance_math(T a, const T *u, const T *f0, const
     T taup = tau2 * rad2;
     T dtau = dt / ((T)24.0 * taup) * fsn;
     T wp = sv * rad2;
+    if constexpr (sizeof(T) == 4) {
+        // FP32: one reciprocal for the three components' common denominator
+        const T inv_den = (T)1.0 / ((T)1.0 + (T)9.0 * dtau);
+        const T grav = dt * (wp / taup) * fsn;
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-        T unitv = (c == 0) ? (T)1.0 : (T)0.0;
-        T tempv = (T)19.0 * f0[c] - (T)5.0 * f1[c] + f2[c];
-        T tempd = (T)55.0 * d0[c] - (T)59.0 * d1[c] + (T)37.0 * d2[c] - (T)9.0 * d3[c];
-        vnew[c] = (f0[c] + dt * unitv * wp / taup * fsn - dtau * tempv + dtau * tempd) / ((T)1.0 + (T)9.0 * dtau);
+        for (int c = 0; c < 3; c++) {
+            T tempv = (T)19.0 * f0[c] - (T)5.0 * f1[c] + f2[c];
+            T tempd = (T)55.0 * d0[c] - (T)59.0 * d1[c] + (T)37.0 * d2[c] - (T)9.0 * d3[c];
+            vnew[c] = (f0[c] + (c == 0 ? grav : (T)0.0) - dtau * tempv + dtau * tempd) * inv_den;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            T unitv = (c == 0) ? (T)1.0 : (T)0.0;
+            T tempv = (T)19.0 * f0[c] - (T)5.0 * f1[c] + f2[c];
+            T tempd = (T)55.0 * d0[c] - (T)59.0 * d1[c] + (T)37.0 * d2[c] - (T)9.0 * d3[c];
+            vnew[c] = (f0[c] + dt * unitv * wp / taup * fsn - dtau * tempv + dtau * tempd) / ((T)1.0 + (T)9.0 * dtau);
+        }
     }
     T dtc = dt / (T)24.0;
 #pragma unroll
@@ -461,7 +473,16 @@ __global__ void __launch_bounds__((NG * GW + 1) * 32, 1) k_interp(const __grid_c
 #pragma unroll
                 for (int q3 = 0; q3 < 3; q3++) {
                     double z;
-                    node[q3] = node_frac(pos[q3], A.dx, &z);
+                    if constexpr (sizeof(T) == 8) {
+                        node[q3] = node_frac(pos[q3], A.dx, &z);   // the reference's division
+                    } else {
+                        // FP32 weights: a multiply by 1/dx (no FP64 division in the per-brick
+                        // critical path); a node that differs by one at a cell face gives the
+                        // same interpolant (z = 1 on node n is z = 0 on node n + 1)
+                        const double u = pos[q3] * A.inv_dx;
+                        node[q3] = (int)floor(u);
+                        z = u - (double)node[q3];
+                    }
                     if constexpr (sizeof(T) == 8) {
                         double w[6];
                         lagrange6(z, w);
@@ -979,6 +1000,7 @@ static int launch_interp_t(dl_ctx *c, int comp_lo, int ncomp, int fused)
     A.n = c->dc.n;
     A.nps = c->nps;
     A.dx = c->dc.dx;
+    A.inv_dx = 1.0 / c->dc.dx;
     A.pi2 = c->dc.pi2;
     A.px = c->pos[c->pcur][0]; A.py = c->pos[c->pcur][1]; A.pz = c->pos[c->pcur][2];
     A.brick_start = c->brick_start;
