@@ -306,7 +306,10 @@ static int alloc_dev(dl_ctx *c, void **p, size_t bytes)
     if (bytes == 0) bytes = 16;
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) return dl_fail(c, DL_E_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    cudaMemset(*p, 0, bytes);
+    // zeroed on the context's stream: the legacy stream is not ordered with a non-blocking
+    // stream, so a cudaMemset there could land after this stream's first writes
+    e = cudaMemsetAsync(*p, 0, bytes, c->stream);
+    if (e != cudaSuccess) return dl_fail(c, DL_E_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
     return 0;
 }
 #define ALLOC(ptr, bytes)                                   \
@@ -1135,8 +1138,8 @@ int dl_hist_boundary(dl_ctx *c)
             int hb = (pp[0] - 1) + nset * ((pp[1] - 1) + nset * ikk);
             if (hi[hb] != 0) hd[5 * nbz + hb] = hd[5 * nbz + hb] / (double)hi[hb];
         }
-    DL_CUDA(c, cudaMemcpy(c->out_i, hi.data(), sizeof(int) * nbz, cudaMemcpyHostToDevice));
-    DL_CUDA(c, cudaMemcpy(c->out_d, hd.data(), sizeof(double) * 7 * nbz, cudaMemcpyHostToDevice));
+    DL_CUDA(c, cudaMemcpyAsync(c->out_i, hi.data(), sizeof(int) * nbz, cudaMemcpyHostToDevice, c->stream));
+    DL_CUDA(c, cudaMemcpyAsync(c->out_d, hd.data(), sizeof(double) * 7 * nbz, cudaMemcpyHostToDevice, c->stream));
     DL_CUDA(c, cudaMemsetAsync(c->acc_i, 0, sizeof(int) * nbz, c->stream));
     DL_CUDA(c, cudaMemsetAsync(c->acc_d, 0, sizeof(double) * 7 * nbz, c->stream));
     return 0;

@@ -822,7 +822,9 @@ int aalloc(dl_adj *a, void **p, size_t bytes)
 {
     cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
     if (e != cudaSuccess) return afail(a, DL_E_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    cudaMemset(*p, 0, bytes ? bytes : 16);
+    // zeroed on the context's stream (the legacy stream is not ordered with it)
+    e = cudaMemsetAsync(*p, 0, bytes ? bytes : 16, a->stream);
+    if (e != cudaSuccess) return afail(a, DL_E_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
     return 0;
 }
 template <typename T>
@@ -961,7 +963,7 @@ int find_pairs(dl_adj *a)
         std::sort(h.begin(), h.end(), [&](const int2 &u, const int2 &v) {
             return pm[u.x] != pm[v.x] ? pm[u.x] < pm[v.x] : pm[u.y] < pm[v.y];
         });
-        ACUDA(a, cudaMemcpy(a->pairs, h.data(), sizeof(int2) * np2, cudaMemcpyHostToDevice));
+        ACUDA(a, cudaMemcpyAsync(a->pairs, h.data(), sizeof(int2) * np2, cudaMemcpyHostToDevice, a->stream));
     }
     return 0;
 }
@@ -1234,10 +1236,10 @@ extern "C" int dl_adj_set_droplets(dl_adj *a, const double *x0, const double *ta
         st[q] = ht[i];
         sr[q] = hr[i];
     }
-    ACUDA(a, cudaMemcpy(a->x0, sx.data(), sizeof(double) * 3 * np, cudaMemcpyHostToDevice));
-    ACUDA(a, cudaMemcpy(a->tau, st.data(), sizeof(double) * np, cudaMemcpyHostToDevice));
-    ACUDA(a, cudaMemcpy(a->rad, sr.data(), sizeof(double) * np, cudaMemcpyHostToDevice));
-    ACUDA(a, cudaMemcpy(a->perm, order.data(), sizeof(int) * np, cudaMemcpyHostToDevice));
+    ACUDA(a, cudaMemcpyAsync(a->x0, sx.data(), sizeof(double) * 3 * np, cudaMemcpyHostToDevice, a->stream));
+    ACUDA(a, cudaMemcpyAsync(a->tau, st.data(), sizeof(double) * np, cudaMemcpyHostToDevice, a->stream));
+    ACUDA(a, cudaMemcpyAsync(a->rad, sr.data(), sizeof(double) * np, cudaMemcpyHostToDevice, a->stream));
+    ACUDA(a, cudaMemcpyAsync(a->perm, order.data(), sizeof(int) * np, cudaMemcpyHostToDevice, a->stream));
     // pair cells at least as wide as the largest cutoff
     const double rmax = *std::max_element(hr.begin(), hr.end());
     const double cut = a->p.pair_factor * 2.0 * rmax;
