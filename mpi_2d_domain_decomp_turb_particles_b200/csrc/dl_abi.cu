@@ -824,6 +824,34 @@ extern "C" int dl_set_field(dl_ctx *c, int icpt, const double *v, int64_t pitch_
     return 0;
 }
 
+// For a producer that writes the padded field itself (the device flow step): the buffer,
+// its geometry and element type.  dl_field_written then marks all three components set.
+int dl_field_target(dl_ctx *c, void **fpad, int64_t *pitch, int64_t *plane, int64_t *comp, int *is_f32)
+{
+    if (!c || !c->initialized) return DL_E_STATE;
+    if (!c->fpad_own) ALLOC(c->fpad_own, c->esz * 3 * c->fp_comp);
+    if (c->fpad != c->fpad_own) c->fpad_valid = 0;
+    c->fpad = c->fpad_own;
+    *fpad = c->fpad_own;
+    *pitch = c->fp_pitch;
+    *plane = c->fp_plane;
+    *comp = c->fp_comp;
+    *is_f32 = c->mixed;
+    return 0;
+}
+
+int dl_field_written(dl_ctx *c, const double *const u[3], int64_t pitch_y, int64_t pitch_z)
+{
+    for (int k = 0; k < 3; k++) {
+        c->f64[k] = u[k];
+        c->fpy[k] = pitch_y;
+        c->fpz[k] = pitch_z;
+        c->field_set[k] = 1;
+    }
+    c->fpad_valid = 7;
+    return 0;
+}
+
 extern "C" int dl_set_field_padded(dl_ctx *c, const void *dev_ptr)
 {
     if (!c || !dev_ptr) return DL_E_ARG;

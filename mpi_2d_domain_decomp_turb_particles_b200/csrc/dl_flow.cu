@@ -86,6 +86,50 @@ __global__ void k_cross(int64_t n3, double *phys)
     wz[i] = ux * oy - uy * ox;
 }
 
+// k_cross for a step that feeds a droplet context: also writes the context's halo-padded
+// copy of u (precision T, DL_PAD_LO cells of periodic images below and DL_PAD_HI above in
+// every direction) while u is in registers, so the field is not read again for the
+// conversion.  Grid: x in blocks, one (y, z) row per blockIdx.y, blockIdx.z.
+// the second padded index of grid index p (its periodic image in the halo), or -1
+__device__ __forceinline__ int pad_image(int p, int n)
+{
+    return p < DL_PAD_HI ? p + DL_PAD_LO + n : (p >= n - DL_PAD_LO ? p + DL_PAD_LO - n : -1);
+}
+
+template <typename T>
+__global__ void k_cross_emit(int n, double *phys, T *fp, int64_t py, int64_t pz, int64_t pc)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= n) return;
+    const int y = blockIdx.y, z = blockIdx.z;
+    const int64_t n3 = (int64_t)n * n * n;
+    const int64_t i = ((int64_t)z * n + y) * n + x;
+    double *wx = phys, *wy = phys + n3, *wz = phys + 2 * n3;
+    const double *vx = phys + 3 * n3, *vy = phys + 4 * n3, *vz = phys + 5 * n3;
+    const double ox = wx[i], oy = wy[i], oz = wz[i];
+    const double ux = vx[i], uy = vy[i], uz = vz[i];
+    wx[i] = uy * oz - uz * oy;
+    wy[i] = uz * ox - ux * oz;
+    wz[i] = ux * oy - uy * ox;
+    const T u[3] = {(T)ux, (T)uy, (T)uz};
+    const int X0 = x + DL_PAD_LO, Y0 = y + DL_PAD_LO, Z0 = z + DL_PAD_LO;
+    {
+        T *d = fp + pz * Z0 + py * Y0 + X0;
+        d[0] = u[0]; d[pc] = u[1]; d[2 * pc] = u[2];
+    }
+    // periodic images in the halo (points within DL_PAD_* cells of a face; few threads)
+    const int xi = pad_image(x, n), yi = pad_image(y, n), zi = pad_image(z, n);
+    if (xi >= 0 || yi >= 0 || zi >= 0) {
+#pragma unroll
+        for (int m = 1; m < 8; m++) {
+            const int X = (m & 1) ? xi : X0, Y = (m & 2) ? yi : Y0, Z = (m & 4) ? zi : Z0;
+            if (X < 0 || Y < 0 || Z < 0) continue;
+            T *d = fp + pz * Z + py * Y + X;
+            d[0] = u[0]; d[pc] = u[1]; d[2 * pc] = u[2];
+        }
+    }
+}
+
 struct UpdArgs {
     Grid G;
     double2 *u;           // spectral velocity [3][M]
@@ -623,23 +667,37 @@ extern "C" int dl_flow_step(dl_flow *f, dl_ctx *droplets)
     if (!f->state_set) return ffail(f, DL_E_STATE, "dl_flow_step: set the velocity first");
     const int n = f->G.n;
     const int64_t n3 = (int64_t)n * n * n;
+    void *fpad = nullptr;
+    int64_t fpy = 0, fpz = 0, fpc = 0;
+    int f32 = 0;
+    if (droplets) {
+        if (droplets->dc.n != n) return ffail(f, DL_E_ARG, "dl_flow_step: droplet grid differs from the flow's");
+        const int r = dl_field_target(droplets, &fpad, &fpy, &fpz, &fpc, &f32);
+        if (r) return ffail(f, r, std::string("dl_flow_step: ") + dl_last_error(droplets));
+        // the droplet work queued so far (the last step's interpolation reads the padded
+        // field) completes before this step writes it
+        FCUDA(f, cudaEventRecord(f->ev_used, droplets->stream));
+        FCUDA(f, cudaStreamWaitEvent(f->stream, f->ev_used, 0));
+    }
     // omega and u in physical space
     FFT(f, cufftExecZ2D(f->c2r, reinterpret_cast<cufftDoubleComplex *>(f->work), f->phys));
     f->phys_valid = 1;
     if (droplets) {
-        // the droplet context converts the velocity on its own stream: order it after the
-        // inverse transform, and order this flow's next writes after the conversion
+        // u x omega, and the droplet context's padded copy of u from the same pass
+        const dim3 grid((unsigned)((n + 127) / 128), (unsigned)n, (unsigned)n);
+        if (f32)
+            k_cross_emit<float><<<grid, 128, 0, f->stream>>>(n, f->phys, (float *)fpad, fpy, fpz, fpc);
+        else
+            k_cross_emit<double><<<grid, 128, 0, f->stream>>>(n, f->phys, (double *)fpad, fpy, fpz, fpc);
+        FCUDA(f, cudaGetLastError());
         FCUDA(f, cudaEventRecord(f->ev_ready, f->stream));
         FCUDA(f, cudaStreamWaitEvent(droplets->stream, f->ev_ready, 0));
-        for (int c = 0; c < 3; c++) {
-            const int r = dl_set_field(droplets, c + 1, f->phys + (3 + c) * n3, n, (int64_t)n * n, 1);
-            if (r) return ffail(f, r, std::string("dl_flow_step: dl_set_field: ") + dl_last_error(droplets));
-        }
-        FCUDA(f, cudaEventRecord(f->ev_used, droplets->stream));
-        FCUDA(f, cudaStreamWaitEvent(f->stream, f->ev_used, 0));
+        const double *u[3] = {f->phys + 3 * n3, f->phys + 4 * n3, f->phys + 5 * n3};
+        dl_field_written(droplets, u, n, (int64_t)n * n);
+    } else {
+        k_cross<<<blocks(n3, 256), 256, 0, f->stream>>>(n3, f->phys);
+        FCUDA(f, cudaGetLastError());
     }
-    k_cross<<<blocks(n3, 256), 256, 0, f->stream>>>(n3, f->phys);
-    FCUDA(f, cudaGetLastError());
     FFT(f, cufftExecD2Z(f->r2c, f->phys, reinterpret_cast<cufftDoubleComplex *>(f->work)));
     UpdArgs A;
     A.G = f->G;

@@ -272,6 +272,9 @@ int launch_update_position(dl_ctx *c, int track_leave);
 int launch_convert_field(dl_ctx *c, int icpt);
 int launch_mean_vel(dl_ctx *c, double *host_out);
 int launch_interp_scalar(dl_ctx *c, const double *v, int64_t pitch_y, int64_t pitch_z, double *out);
+// dl_abi.cu: the padded field written directly by a producer (the device flow step)
+int dl_field_target(dl_ctx *c, void **fpad, int64_t *pitch, int64_t *plane, int64_t *comp, int *is_f32);
+int dl_field_written(dl_ctx *c, const double *const u[3], int64_t pitch_y, int64_t pitch_z);
 // dl_cells.cu
 int launch_headlist(dl_ctx *c, double dist);
 int launch_collision(dl_ctx *c, dl_coll_report *rep);
