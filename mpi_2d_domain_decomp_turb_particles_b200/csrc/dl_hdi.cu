@@ -32,6 +32,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <vector>
 
 namespace {
@@ -464,6 +465,418 @@ __global__ void k_uncopy3(int nps, const S *s, int64_t ld, D *d0, D *d1, D *d2)
 }
 
 // ---------------------------------------------------------------------------------------
+// Fused FP32 Arnoldi: the inner solve of the mixed context.  One iteration is three
+// launches over a fixed grid and no host round trip:
+//   k_arn_spmv    q_k = w / s (w the unnormalised vector the previous iteration left,
+//                 s its norm), v = N q_k, h1_j = <q_j, v> for j = 1..k and
+//                 ||v||^2; the last CTA decides whether a second projection is needed
+//                 (||v - Q h1||^2 = ||v||^2 - ||h1||^2 below half of ||v||^2, the
+//                 Daniel-Gragg-Kaufman-Stewart criterion with eta = 1/sqrt(2));
+//   k_arn_cgs<2>  v -= Q h1, then h2_j = <q_j, v> when projecting again, else ||v||^2
+//                 and the least-squares update below;
+//   k_arn_cgs<3>  (second projection only) v -= Q h2, ||v||^2 and the least-squares
+//                 update: the last CTA writes the Hessenberg column H(j, k) = h1_j
+//                 (+ h2_j) (+ 1 for j = k), H(k+1, k) = ||v|| and one of its warps
+//                 runs the Givens update, the back substitution, the residual estimate and the
+//                 tolerance schedule of partlib.f90:2888-2970 in FP64.  Convergence
+//                 raises a done flag: launches already queued for later iterations
+//                 return at entry, so the host checks the state only every few
+//                 iterations.
+// The basis is built from N rather than I + N (the same Krylov space; the identity
+// only adds 1 to the diagonal of H), so the projection does not first cancel the
+// identity part of v and the second pass is rarely needed.
+// Classical Gram-Schmidt with selective reorthogonalisation keeps the basis as
+// orthogonal as the reference's modified Gram-Schmidt with one or two reductions per
+// iteration instead of k + 1; the FP64 refinement around this solve sets the accuracy
+// of the result.  All sums run in a fixed order over a fixed grid, so the solve is
+// deterministic.
+// ---------------------------------------------------------------------------------------
+constexpr int kArnThreads = 256;                  // one tile of 256 droplets per CTA trip
+constexpr int kArnWarps = kArnThreads / 32;
+constexpr int kArnSlots = (kMaxIter + kArnWarps - 1) / kArnWarps;   // basis vectors per warp in the dots
+constexpr int kArnCtasPerSm = 4;
+constexpr int kM1 = kMaxIter + 1;
+
+struct ArnState {
+    int done, iters, converged, reorth;
+    double res, maxerr, norm_b, norm_rhs, stop_abs;
+    double bn[kM1], y[kMaxIter];
+    double H[kM1 * kMaxIter], QN[kM1 * kM1], RN[kM1 * kM1];
+};
+
+// the head of ArnState the host reads after each batch of iterations
+struct ArnStatus {
+    int done, iters, converged, reorth;
+    double res, maxerr;
+};
+
+struct ArnArgs {
+    int nps;
+    int64_t ld, qld;
+    const int *start, *partner;
+    const float *coef;
+    float *Q;             // Krylov basis, column j at Q + j * qld
+    ArnState *st;
+    float *part;          // [kMaxIter + 1][gridDim.x] partial sums
+    float *h1, *h2;       // [kMaxIter] projections of the two passes
+    float *s;             // [0] norm of the vector the next k_arn_spmv normalises
+    unsigned *ticket;
+};
+
+__device__ __forceinline__ float warp_sum_f(float v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// acc[m] += <q_j, v> over one tile for the basis vectors j = warp + m * kArnWarps < k;
+// the tile's v is in sv (zero past nps)
+__device__ __forceinline__ void arn_tile_dots(const ArnArgs &A, int k, int base, const float (*sv)[kArnThreads],
+                                              float *acc)
+{
+    constexpr int kPer = kArnThreads / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int cnt = min(kArnThreads, A.nps - base);
+    if (cnt == kArnThreads) {
+        // full tile: all 3 x kPer loads of a lane in flight before the sums
+#pragma unroll
+        for (int m = 0; m < kArnSlots; m++) {
+            const int j = w + m * kArnWarps;
+            if (j < k) {
+                const float *q = A.Q + (int64_t)j * A.qld + base + lane;
+                float qv[3][kPer];
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+#pragma unroll
+                    for (int t = 0; t < kPer; t++) qv[c][t] = q[c * A.ld + 32 * t];
+                float s = 0.0f;
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+#pragma unroll
+                    for (int t = 0; t < kPer; t++) s = __fmaf_rn(qv[c][t], sv[c][lane + 32 * t], s);
+                acc[m] += s;
+            }
+        }
+        return;
+    }
+#pragma unroll
+    for (int m = 0; m < kArnSlots; m++) {
+        const int j = w + m * kArnWarps;
+        if (j < k) {
+            const float *q = A.Q + (int64_t)j * A.qld + base;
+            float s = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                for (int t = lane; t < cnt; t += 32) s = __fmaf_rn(q[c * A.ld + t], sv[c][t], s);
+            acc[m] += s;
+        }
+    }
+}
+
+// CTA sum of one float per thread, valid in thread 0
+__device__ __forceinline__ float arn_cta_sum(float v)
+{
+    __shared__ float sw[kArnWarps];
+    v = warp_sum_f(v);
+    if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = v;
+    __syncthreads();
+    float t = 0.0f;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < kArnWarps; i++) t += sw[i];
+    return t;
+}
+
+// Every thread of the CTA calls this after writing its partial sums: true in the CTA
+// that finishes last, which then sees all partials.
+__device__ __forceinline__ bool arn_last_cta(const ArnArgs &A)
+{
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(A.ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+// per-CTA dots -> part; the last CTA sums them in CTA order into out[0..k).  With
+// NORM, nrm is this thread's share of ||v||^2 and the last CTA also sets the
+// reorthogonalisation flag from ||v||^2 - ||out||^2.
+template <bool NORM>
+__device__ __forceinline__ void arn_finish_dots(const ArnArgs &A, int k, const float *acc, float *out, float nrm)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int G = gridDim.x;
+#pragma unroll
+    for (int m = 0; m < kArnSlots; m++) {
+        const int j = w + m * kArnWarps;
+        if (j < k) {
+            const float s = warp_sum_f(acc[m]);
+            if (lane == 0) A.part[(int64_t)j * G + blockIdx.x] = s;
+        }
+    }
+    if (NORM) {
+        const float t = arn_cta_sum(nrm);
+        if (threadIdx.x == 0) A.part[(int64_t)kMaxIter * G + blockIdx.x] = t;
+    }
+    if (!arn_last_cta(A)) return;
+#pragma unroll
+    for (int m = 0; m < kArnSlots; m++) {
+        const int j = w + m * kArnWarps;
+        if (j < k) {
+            float s = 0.0f;
+            for (int b = lane; b < G; b += 32) s += __ldcg(A.part + (int64_t)j * G + b);
+            s = warp_sum_f(s);
+            if (lane == 0) out[j] = s;
+        }
+    }
+    if (NORM) {
+        float t = 0.0f;
+        if (w == 0) {
+            for (int b = lane; b < G; b += 32) t += __ldcg(A.part + (int64_t)kMaxIter * G + b);
+            t = warp_sum_f(t);
+        }
+        __syncthreads();   // out[] of every warp written
+        if (threadIdx.x == 0) {
+            double hh = 0.0;
+            for (int j = 0; j < k; j++) hh += (double)out[j] * (double)out[j];
+            A.st->reorth = ((double)t - hh) < 0.5 * (double)t;
+        }
+    }
+    if (threadIdx.x == 0) *A.ticket = 0u;
+}
+
+__global__ void k_arn_init(ArnState *st, double norm_b, double norm_rhs, double stop_abs, float *s)
+{
+    double *p = reinterpret_cast<double *>(st);
+    const int nd = (int)(sizeof(ArnState) / sizeof(double));
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nd; i += gridDim.x * blockDim.x) {
+        double v = 0.0;
+        if (i == (int)(offsetof(ArnState, maxerr) / sizeof(double))) v = kMaxErr;
+        if (i == (int)(offsetof(ArnState, norm_b) / sizeof(double))) v = norm_b;
+        if (i == (int)(offsetof(ArnState, norm_rhs) / sizeof(double))) v = norm_rhs;
+        if (i == (int)(offsetof(ArnState, stop_abs) / sizeof(double))) v = stop_abs;
+        p[i] = v;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) s[0] = (float)norm_rhs;
+}
+
+__global__ void __launch_bounds__(kArnThreads, kArnCtasPerSm) k_arn_spmv(ArnArgs A, int k, const float *w, float *v)
+{
+    if (A.st->done) return;
+    __shared__ float sv[3][kArnThreads];
+    const float inv = 1.0f / A.s[0];
+    float *qk = A.Q + (int64_t)(k - 1) * A.qld;
+    float acc[kArnSlots];
+#pragma unroll
+    for (int m = 0; m < kArnSlots; m++) acc[m] = 0.0f;
+    float nrm = 0.0f;
+    for (int base = blockIdx.x * kArnThreads; base < A.nps; base += gridDim.x * kArnThreads) {
+        const int a = base + threadIdx.x;
+        float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
+        if (a < A.nps) {
+            float r0 = 0.0f, r1 = 0.0f, r2 = 0.0f;
+            const int e1 = A.start[a + 1];
+            for (int e = A.start[a]; e < e1; e++) {
+                const int p = A.partner[e];
+                const float x1 = w[p], x2 = w[A.ld + p], x3 = w[2 * A.ld + p];
+                const float *n = A.coef + (int64_t)e * 6;
+                r0 = __fmaf_rn(n[0], x1, __fmaf_rn(n[1], x2, __fmaf_rn(n[2], x3, r0)));
+                r1 = __fmaf_rn(n[1], x1, __fmaf_rn(n[3], x2, __fmaf_rn(n[4], x3, r1)));
+                r2 = __fmaf_rn(n[2], x1, __fmaf_rn(n[4], x2, __fmaf_rn(n[5], x3, r2)));
+            }
+            const float w0 = w[a], w1 = w[A.ld + a], w2 = w[2 * A.ld + a];
+            v0 = r0 * inv;
+            v1 = r1 * inv;
+            v2 = r2 * inv;
+            qk[a] = w0 * inv;
+            qk[A.ld + a] = w1 * inv;
+            qk[2 * A.ld + a] = w2 * inv;
+            v[a] = v0;
+            v[A.ld + a] = v1;
+            v[2 * A.ld + a] = v2;
+            nrm = __fmaf_rn(v0, v0, __fmaf_rn(v1, v1, __fmaf_rn(v2, v2, nrm)));
+        }
+        sv[0][threadIdx.x] = v0;
+        sv[1][threadIdx.x] = v1;
+        sv[2][threadIdx.x] = v2;
+        __syncthreads();   // also makes this CTA's q_k stores visible to its dot loads
+        arn_tile_dots(A, k, base, sv, acc);
+        __syncthreads();
+    }
+    arn_finish_dots<true>(A, k, acc, A.h1, nrm);
+}
+
+// Givens update of the least-squares problem, back substitution, residual estimate and
+// tolerance schedule (partlib.f90:2888-2970) after iteration k; one warp, FP64.
+__device__ void arn_lsq(const ArnArgs &A, int k, float nrm2, bool two)
+{
+    __shared__ double sy[kMaxIter];
+    ArnState *S = A.st;
+    const int lane = threadIdx.x & 31;
+    const double norm_rhs = S->norm_rhs;
+    double *H = S->H, *QN = S->QN, *RN = S->RN, *bn = S->bn;
+    auto HH = [H](int r, int col) -> double & { return H[(col - 1) * kM1 + (r - 1)]; };
+    auto Q_ = [QN](int r, int col) -> double & { return QN[(col - 1) * kM1 + (r - 1)]; };
+    auto R_ = [RN](int r, int col) -> double & { return RN[(col - 1) * kM1 + (r - 1)]; };
+    for (int i = lane; i < k; i += 32)
+        HH(i + 1, k) = (double)A.h1[i] + (two ? (double)A.h2[i] : 0.0) + (i == k - 1 ? 1.0 : 0.0);
+    const double hn = sqrt((double)nrm2);
+    if (lane == 0) {
+        HH(k + 1, k) = hn;
+        A.s[0] = (float)hn;
+    }
+    __syncwarp();
+    if (k == 1) {
+        if (lane == 0) {
+            const double nrm = sqrt(HH(1, 1) * HH(1, 1) + HH(2, 1) * HH(2, 1));
+            const double q1a = HH(1, 1) / nrm, q1b = HH(2, 1) / nrm;
+            Q_(1, 1) = q1a; Q_(2, 1) = q1b;
+            Q_(1, 2) = q1b; Q_(2, 2) = -q1a;
+            R_(1, 1) = nrm;
+            bn[0] = q1a * norm_rhs;
+            sy[0] = bn[0] / R_(1, 1);
+        }
+        __syncwarp();
+    } else {
+        for (int i = 1 + lane; i <= k; i += 32) {
+            double acc = 0.0;
+            for (int j = 1; j <= k; j++) acc = acc + Q_(i, j) * HH(j, k);
+            R_(i, k) = acc;
+        }
+        __syncwarp();
+        const double aa = R_(k, k), bb = HH(k + 1, k);
+        const double dd = sqrt(aa * aa + bb * bb);
+        const double cc = aa / dd, ss = bb / dd;
+        __syncwarp();
+        if (lane == 0) R_(k, k) = dd;
+        for (int j = 1 + lane; j <= k + 1; j += 32) {
+            const double qv = j <= k ? Q_(k, j) : 0.0;
+            Q_(k, j) = j <= k ? cc * qv : ss;
+            Q_(k + 1, j) = j <= k ? -ss * qv : cc;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            bn[k - 2] = Q_(k - 1, 1) * norm_rhs;
+            bn[k - 1] = Q_(k, 1) * norm_rhs;
+            sy[k - 1] = bn[k - 1] / R_(k, k);
+        }
+        __syncwarp();
+        for (int i = k - 1; i >= 1; i--) {
+            double d = 0.0;
+            for (int j = i + 1 + lane; j <= k; j += 32) d = d + sy[j - 1] * R_(i, j);
+            d = warp_sum_d(d);
+            if (lane == 0) sy[i - 1] = (bn[i - 1] - d) / R_(i, i);
+            __syncwarp();
+        }
+    }
+    // residual estimate ||H y - norm_rhs e1||
+    double xc = 0.0;
+    for (int i = 1 + lane; i <= k + 1; i += 32) {
+        double acc = 0.0;
+        for (int j = 1; j <= k; j++) acc = acc + HH(i, j) * sy[j - 1];
+        if (i == 1) acc = acc - norm_rhs;
+        xc = xc + acc * acc;
+    }
+    xc = warp_sum_d(xc);
+    for (int j = lane; j < k; j += 32) S->y[j] = sy[j];
+    if (lane == 0) {
+        const double res = sqrt(xc) / S->norm_b;
+        S->res = res;
+        S->iters = k;
+        if (res < S->maxerr || (S->stop_abs > 0.0 && sqrt(xc) < S->stop_abs)) {
+            S->converged = 1;
+            S->done = 1;
+        } else {
+            if (k == kMaxIter / 2) S->maxerr = S->maxerr * 10;
+            if (k >= kMaxIter - 2) S->maxerr = S->maxerr * 10;
+            if (k >= kMaxIter) S->done = 1;
+        }
+    }
+}
+
+// PASS 2: v -= Q h1, then h2 = Q^T v (second projection) or ||v||^2 and the
+// least-squares update.  PASS 3 (second projection only): v -= Q h2, ||v||^2 and the
+// least-squares update.
+template <int PASS>
+__global__ void __launch_bounds__(kArnThreads, kArnCtasPerSm) k_arn_cgs(ArnArgs A, int k, float *v)
+{
+    if (A.st->done) return;
+    const bool again = A.st->reorth != 0;
+    if (PASS == 3 && !again) return;
+    const bool dots = PASS == 2 && again;
+    __shared__ float sv[3][kArnThreads];
+    __shared__ float sh[kMaxIter];
+    const float *hs = PASS == 2 ? A.h1 : A.h2;
+    for (int i = threadIdx.x; i < k; i += kArnThreads) sh[i] = hs[i];
+    __syncthreads();
+    float acc[kArnSlots];
+#pragma unroll
+    for (int m = 0; m < kArnSlots; m++) acc[m] = 0.0f;
+    float nrm = 0.0f;
+    for (int base = blockIdx.x * kArnThreads; base < A.nps; base += gridDim.x * kArnThreads) {
+        const int a = base + threadIdx.x;
+        float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
+        if (a < A.nps) {
+            v0 = v[a];
+            v1 = v[A.ld + a];
+            v2 = v[2 * A.ld + a];
+            const float *q = A.Q + a;
+#pragma unroll 4
+            for (int j = 0; j < k; j++, q += A.qld) {
+                const float h = sh[j];
+                v0 = __fmaf_rn(-h, q[0], v0);
+                v1 = __fmaf_rn(-h, q[A.ld], v1);
+                v2 = __fmaf_rn(-h, q[2 * A.ld], v2);
+            }
+            v[a] = v0;
+            v[A.ld + a] = v1;
+            v[2 * A.ld + a] = v2;
+            nrm = __fmaf_rn(v0, v0, __fmaf_rn(v1, v1, __fmaf_rn(v2, v2, nrm)));
+        }
+        if (dots) {   // CTA-uniform
+            sv[0][threadIdx.x] = v0;
+            sv[1][threadIdx.x] = v1;
+            sv[2][threadIdx.x] = v2;
+            __syncthreads();
+            arn_tile_dots(A, k, base, sv, acc);
+            __syncthreads();
+        }
+    }
+    if (dots) {
+        arn_finish_dots<false>(A, k, acc, A.h2, 0.0f);
+        return;
+    }
+    const float t0 = arn_cta_sum(nrm);
+    if (threadIdx.x == 0) A.part[blockIdx.x] = t0;
+    if (!arn_last_cta(A)) return;
+    const int lane = threadIdx.x & 31;
+    if ((threadIdx.x >> 5) != 0) return;
+    float t = 0.0f;
+    for (int b = lane; b < (int)gridDim.x; b += 32) t += __ldcg(A.part + b);
+    t = warp_sum_f(t);
+    arn_lsq(A, k, t, PASS == 3);
+    if (lane == 0) *A.ticket = 0u;
+}
+
+// x += Q y over the iterations the state reports
+__global__ void k_arn_xupdate(int64_t n, const ArnState *st, const float *Q, int64_t qld, double *x)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int it = st->iters;
+    double acc = 0.0;
+    for (int j = 0; j < it; j++) acc = acc + (double)Q[(int64_t)j * qld + i] * st->y[j];
+    x[i] = x[i] + acc;
+}
+
+// ---------------------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------------------
 int grow(dl_ctx *c, void **p, size_t bytes, size_t *have)
@@ -476,6 +889,41 @@ int grow(dl_ctx *c, void **p, size_t bytes, size_t *have)
     if (e != cudaSuccess) return dl_fail(c, DL_E_ALLOC, std::string("HDI buffers: ") + cudaGetErrorString(e));
     *have = bytes;
     return 0;
+}
+
+// Layout of c->arn: the least-squares state, then [kMaxIter + 1][grid] partial sums,
+// h1[kMaxIter], h2[kMaxIter], the norm slot and the ticket.
+int arn_grid(const dl_ctx *c, int nps)
+{
+    return std::max(1, std::min((nps + kArnThreads - 1) / kArnThreads, c->num_sms * kArnCtasPerSm));
+}
+
+size_t arn_bytes(const dl_ctx *c)
+{
+    const size_t st = (sizeof(ArnState) + 255) / 256 * 256;
+    return st + sizeof(float) * ((size_t)(kMaxIter + 1) * c->num_sms * kArnCtasPerSm + 2 * kMaxIter + 4) + 16;
+}
+
+ArnArgs arn_args(dl_ctx *c)
+{
+    ArnArgs A;
+    char *base = static_cast<char *>(c->arn);
+    const size_t st = (sizeof(ArnState) + 255) / 256 * 256;
+    const size_t gmax = (size_t)c->num_sms * kArnCtasPerSm;
+    A.nps = c->nps;
+    A.ld = c->nps;
+    A.qld = 3 * (int64_t)c->msize;
+    A.start = c->nei_start;
+    A.partner = c->nei_idx;
+    A.coef = tp<float>(c->nei_coef);
+    A.Q = tp<float>(c->kry);
+    A.st = reinterpret_cast<ArnState *>(base);
+    A.part = reinterpret_cast<float *>(base + st);
+    A.h1 = A.part + (size_t)(kMaxIter + 1) * gmax;
+    A.h2 = A.h1 + kMaxIter;
+    A.s = A.h2 + kMaxIter;
+    A.ticket = reinterpret_cast<unsigned *>(A.s + 4);
+    return A;
 }
 
 // The Krylov space, the reduction scratch and the FP64 vectors (allocated on first use).
@@ -495,6 +943,11 @@ int gmres_buffers(dl_ctx *c)
             return dl_fail(c, DL_E_ALLOC, "HDI_GMRES: cudaMalloc failed");
         c->rf32 = (float *)p;
         DL_CUDA(c, cudaMemsetAsync(c->dots, 0, sizeof(double) * (kRedGrid + 2 * (kMaxIter + 4)) + 64, c->stream));
+    }
+    if (c->mixed && !c->arn) {
+        const size_t bytes = arn_bytes(c);
+        if (cudaMalloc(&c->arn, bytes) != cudaSuccess) return dl_fail(c, DL_E_ALLOC, "HDI_GMRES: cudaMalloc failed");
+        DL_CUDA(c, cudaMemsetAsync(c->arn, 0, bytes, c->stream));
     }
     return 0;
 }
@@ -718,6 +1171,45 @@ int gmres_fp64(dl_ctx *c, dl_gmres_report *rep)
     return g.converged ? 0 : DL_W_GMRES_NOT_CONVERGED;
 }
 
+// The FP32 correction solve of the mixed context: (I + N) d = r from d0 = 0, r = c->rf32
+// of norm nf, by the fused Arnoldi kernels, then x += d.  The iterations are queued in
+// batches (the first as long as this sweep's previous solve, then two at a time) and the
+// host reads the state once per batch.
+int arnoldi_f32(dl_ctx *c, int sweep, double norm_b, double nf, double stop_abs, double *x, int &iters)
+{
+    const int64_t n3 = 3 * (int64_t)c->nps;
+    const ArnArgs A = arn_args(c);
+    const int G = arn_grid(c, c->nps);
+    k_arn_init<<<8, 256, 0, c->stream>>>(A.st, norm_b, nf, stop_abs, A.s);
+    DL_CHECK_LAUNCH(c);
+    float *buf[2] = {tp<float>(c->wv), tp<float>(c->xt)};
+    int &guess = c->arn_guess[std::min(sweep, 7)];
+    int batch = guess > 0 ? guess : 4;
+    ArnStatus hs{};
+    int k = 0;
+    while (k < kMaxIter) {
+        const int kend = std::min(kMaxIter, k + batch);
+        while (k < kend) {
+            k++;
+            const float *w = k == 1 ? c->rf32 : buf[(k - 1) & 1];
+            float *v = buf[k & 1];
+            k_arn_spmv<<<G, kArnThreads, 0, c->stream>>>(A, k, w, v);
+            k_arn_cgs<2><<<G, kArnThreads, 0, c->stream>>>(A, k, v);
+            k_arn_cgs<3><<<G, kArnThreads, 0, c->stream>>>(A, k, v);
+            DL_CHECK_LAUNCH(c);
+        }
+        DL_CUDA(c, cudaMemcpyAsync(&hs, A.st, sizeof(hs), cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaStreamSynchronize(c->stream));
+        if (hs.done) break;
+        batch = 2;
+    }
+    iters = hs.iters;
+    guess = hs.iters;
+    k_arn_xupdate<<<(int)((n3 + 255) / 256), 256, 0, c->stream>>>(n3, A.st, A.Q, A.qld, x);
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}
+
 // HDI_GMRES of a mixed context: FP32 GMRES corrections inside FP64 residual refinement.
 int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
 {
@@ -725,7 +1217,6 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
     const int64_t ld = nps, n3 = 3 * (int64_t)nps;
     const int bs = dl_blocks(nps, 256);
     double *x = c->xg, *b = c->bg64, *r64 = c->rg;
-    float *Q0 = tp<float>(c->kry);
     k_copy3<float, double><<<bs, 256, 0, c->stream>>>(nps, tp<float>(c->pert[0]), tp<float>(c->pert[1]),
                                                       tp<float>(c->pert[2]), ld, x);
     DL_CHECK_LAUNCH(c);
@@ -763,17 +1254,15 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
         if (sweep > 0 && rep->residual < kMaxErr) { converged = true; break; }
         if (sweep == kMaxRefine) break;
         // FP32 correction: (I + N) d = r, d0 = 0
-        DL_CUDA(c, cudaMemcpyAsync(Q0, c->rf32, sizeof(float) * n3, cudaMemcpyDeviceToDevice, c->stream));
         double nf2 = 0.0;
-        if ((r = sumsq<float>(c, Q0, n3, &nf2))) return r;
+        if ((r = sumsq<float>(c, c->rf32, n3, &nf2))) return r;
         const double nf = std::sqrt(nf2);
         if (!(nf > 0.0)) { converged = true; break; }
-        GmresResult g;
         // stop the FP32 solve at a tenth of the FP64 target, or at FP32 resolution of r
         const double stop_abs = std::max(0.1 * kMaxErr * norm_b, 1.0e-5 * nf);
-        if ((r = gmres_iterate<float, float>(c, tp<float>(c->nei_coef), norm_b, nf, stop_abs, g))) return r;
-        rep->iterations += g.iters;
-        if ((r = x_update<float>(c, g, x, x))) return r;
+        int iters = 0;
+        if ((r = arnoldi_f32(c, sweep, norm_b, nf, stop_abs, x, iters))) return r;
+        rep->iterations += iters;
     }
     k_uncopy3<double, float><<<bs, 256, 0, c->stream>>>(nps, x, ld, tp<float>(c->pert[0]), tp<float>(c->pert[1]),
                                                         tp<float>(c->pert[2]));
@@ -790,7 +1279,6 @@ int launch_nei_list(dl_ctx *c)
     if (!c->hl_valid) return dl_fail(c, DL_E_STATE, "NEI_LIST_PRECOMP: call HEADLIST first");
     const int nps = c->nps;
     const size_t m = (size_t)c->msize;
-    int r;
     if (!c->nei_cnt) {
         if (cudaMalloc(&c->nei_cnt, sizeof(int) * (m + 1)) != cudaSuccess ||
             cudaMalloc(&c->nei_start, sizeof(int) * (m + 1)) != cudaSuccess ||

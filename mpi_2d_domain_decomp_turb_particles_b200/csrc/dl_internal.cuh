@@ -210,6 +210,8 @@ struct dl_ctx {
     void *wv, *xt;               // T vectors (3*msize)
     float *rf32;                 // FP32 copy of the FP64 residual (mixed)
     double *dots;                // reduction scratch
+    void *arn;                   // fused FP32 Arnoldi: least-squares state, partial dots, scalars
+    int arn_guess[8];            // iterations of the previous FP32 solve of each refinement sweep
     int gmres_iters, gmres_refine;
     double gmres_res, gmres_norm_rhs;
 
