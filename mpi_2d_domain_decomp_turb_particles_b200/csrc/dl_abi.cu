@@ -477,7 +477,8 @@ extern "C" int dl_destroy(dl_ctx *c)
     F(c->ovl_list); F(c->ovl_cnt); F(c->fpad_own);
     F(c->nei_cnt); F(c->nei_start); F(c->nei_idx); F(c->nei_coef); F(c->nei_coef64); F(c->overlap_flag);
     F(c->kry); F(c->xg); F(c->rg); F(c->bg64); F(c->tmp64); F(c->wv); F(c->xt); F(c->dots); F(c->arn);
-    F(c->nei_fill); F(c->nei_blk); F(c->nei_key); F(c->rf32); F(c->nei_app); F(c->cell_start);
+    F(c->red_pos); F(c->red_list); F(c->red_start); F(c->red_partner); F(c->red_rhs);
+    F(c->nei_fill); F(c->nei_blk); F(c->nei_key); F(c->rf32); F(c->nei_app); F(c->cell_start); F(c->pk_x); F(c->pk_id);
     F(c->scal[0]); F(c->scal[1]); F(c->gr_part); F(c->gr_bins); F(c->gr_mdens); F(c->scal_field);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);

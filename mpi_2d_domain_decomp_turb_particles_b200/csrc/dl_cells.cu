@@ -246,15 +246,41 @@ __device__ __forceinline__ int lower_ix(const long long *re, int s, int e, int k
     return s;
 }
 
-// Cell start table: one warp per row, lanes over the x cells; each lane's lower-bound
-// search reads the row's entries, which the warp shares in L1.
-__global__ void k_cell_starts(int nrows, int ncd, const int *row_start, const long long *row_ent, int *cs)
+// Cell start table: per row, the first entry of each bucket of 2^shift x cells and the
+// row end; one thread per (row, bucket), a lower-bound search in the row's entries.
+__global__ void k_cell_starts(int nrows, int nb, int shift, const int *row_start, const long long *row_ent, int *cs)
 {
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (row >= nrows) return;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)nrows * (nb + 1)) return;
+    const int row = (int)(i / (nb + 1)), b = (int)(i - (int64_t)row * (nb + 1));
     const int rs = row_start[row], re = row_start[row + 1];
-    int *out = cs + (int64_t)row * (ncd + 1);
-    for (int ix = 1 + lane; ix <= ncd + 1; ix += 32) out[ix - 1] = lower_ix(row_ent, rs, re, ix);
+    cs[i] = b == nb ? re : lower_ix(row_ent, rs, re, 1 + (b << shift));
+}
+
+// Cell-ordered copy of what the neighbour searches read of each sorted entry: (x, y, z,
+// radius) with a ghost's y/z shift applied, and (source droplet, ypn index - 1, ix,
+// ghost slot or 0).  A search then streams the entries of a cell range instead of
+// gathering them through the entry index.
+__global__ void k_pack_entries(int ne, int nps, const long long *row_ent, const double *px, const double *py,
+                               const double *pz, const double *rad, const int *ref, const Ghost *g, double4 *pk_x,
+                               int4 *pk_id)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ne) return;
+    const long long ke = row_ent[s];
+    const int e = (int)(ke & 0xffffffffLL), ix = (int)(ke >> 32);
+    int src, key, jid;
+    double y, z;
+    if (e < nps) {
+        src = e; key = ref[e]; jid = 0;
+        y = py[e]; z = pz[e];
+    } else {
+        const Ghost gh = g[e - nps];
+        src = gh.src; key = e; jid = gh.jid;   // ghosts follow the owned droplets in ypn order
+        y = gh.y; z = gh.z;
+    }
+    pk_x[s] = make_double4(px[src], y, z, rad[src]);
+    pk_id[s] = make_int4(src, key, ix, jid);
 }
 
 // FINDINDEX, partlib.f90:1850-1885
@@ -278,14 +304,11 @@ __device__ __forceinline__ double dot3(const double *a, const double *b)
 template <typename T>
 struct CollArgs {
     DevConst D;
-    int nps;
-    const double *px, *py, *pz;
-    const Ghost *g;
-    const int *row_start;
-    const long long *row_ent;
+    int nps, ne;                 // droplets, sorted entries (droplets + ghosts)
+    const double4 *pk_x;         // packed sorted entries (HEADLIST)
+    const int4 *pk_id;
     const int *cell_start;
     const int *ref;
-    const double *rad;
     const T *dm[3], *vo[3], *vn[3], *up[3];
     int imax, jmax, kmax;
     int nbinsz;
@@ -302,41 +325,31 @@ struct CollArgs {
     int remove_cap;
 };
 
+// COLLISION_DET body for one owned droplet ih1 (partlib.f90:1233-1590), the droplet of
+// sorted entry sa; returns the candidates it visited.
 template <typename T>
-__device__ __forceinline__ void load_entry(const CollArgs<T> &A, int e, double *x, int &src, int &jid)
+__device__ __forceinline__ unsigned collision_owner(const CollArgs<T> &A, int sa)
 {
-    if (e < A.nps) {
-        src = e; jid = 0;
-        x[0] = A.px[e]; x[1] = A.py[e]; x[2] = A.pz[e];
-    } else {
-        const Ghost &gh = A.g[e - A.nps];
-        src = gh.src; jid = gh.jid;
-        x[0] = A.px[src]; x[1] = gh.y; x[2] = gh.z;
-    }
-}
-
-// COLLISION_DET body for one owned droplet ih1 (partlib.f90:1233-1590)
-template <typename T>
-__global__ void __launch_bounds__(128) k_collision(CollArgs<T> A)
-{
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= A.nps) return;
+    const int4 ida = A.pk_id[sa];
+    if (ida.w != 0) return 0u;   // a ghost owns no search
+    const double4 pa = A.pk_x[sa];
+    const int a = ida.x;
     const DevConst &D = A.D;
     const int nset = D.nset;
-    double xa[3] = {A.px[a], A.py[a], A.pz[a]}, xan[3], va[3], van[3], ua[3];
+    double xa[3] = {pa.x, pa.y, pa.z}, xan[3], va[3], van[3], ua[3];
     for (int i = 0; i < 3; i++) {
         xan[i] = xa[i] + (double)A.dm[i][a];
         va[i] = (double)A.vo[i][a];
         van[i] = (double)A.vn[i][a];
         ua[i] = (double)A.up[i][a];
     }
-    const double ra = A.rad[a];
-    const int refa = A.ref[a];
+    const double ra = pa.w;
+    const int refa = ida.y;
     const double dma[3] = {(double)A.dm[0][a], (double)A.dm[1][a], (double)A.dm[2][a]};
     int ix, iy, iz;
     own_cell(D, xa[0], xa[1], xa[2], ix, iy, iz);
     int ncollip1 = 0;
-    unsigned long long ncand = 0;
+    unsigned ncand = 0;
     const int nj = 2 * A.jmax + 1, nk = 2 * A.kmax + 1;
 
     for (int jj = -A.jmax; jj <= A.jmax; jj++) {
@@ -348,29 +361,33 @@ __global__ void __launch_bounds__(128) k_collision(CollArgs<T> A)
             if (iz2 < 1) continue;
             if (iz2 <= D.ncd && iy2 < 1) continue;
             const int row = row_of(D, iy2, iz2);
-            const int rs = A.row_start[row], re_ = A.row_start[row + 1];
-            if (rs == re_) continue;
-            // up to three x ranges: [lo, hi] with shift sx
-            int lo_raw = ix - A.imax, hi_raw = ix + A.imax;
-            int rlo[3], rhi[3];
-            double rsx[3];
-            int nr = 0;
-            rlo[nr] = max(1, lo_raw); rhi[nr] = min(D.ncd, hi_raw); rsx[nr] = 0.0; nr++;
-            if (lo_raw < 1) { rlo[nr] = lo_raw + D.ncd; rhi[nr] = D.ncd; rsx[nr] = -1.0; nr++; }
-            if (hi_raw > D.ncd) { rlo[nr] = 1; rhi[nr] = hi_raw - D.ncd; rsx[nr] = 1.0; nr++; }
-            for (int q = 0; q < nr; q++) {
-                const double sx = rsx[q];
+            // up to three x ranges: [lo, hi] inside the box and the wrapped parts, with shift sx
+            const int lo_raw = ix - A.imax, hi_raw = ix + A.imax;
+#pragma unroll 1
+            for (int q = 0; q < 3; q++) {
+                int lo, hi;
+                double sx;
+                if (q == 0) {
+                    lo = max(1, lo_raw); hi = min(D.ncd, hi_raw); sx = 0.0;
+                } else if (q == 1) {
+                    if (lo_raw >= 1) continue;
+                    lo = lo_raw + D.ncd; hi = D.ncd; sx = -1.0;
+                } else {
+                    if (hi_raw <= D.ncd) continue;
+                    lo = 1; hi = hi_raw - D.ncd; sx = 1.0;
+                }
                 int s0, s1;
-                cell_range(A.cell_start, row, D.ncd, rs, re_, rlo[q], rhi[q], s0, s1);
+                cell_range(A.cell_start, D, row, lo, hi, s0, s1);
                 for (int s = s0; s < s1; s++) {
-                    const long long ke = A.row_ent[s];
-                    const int ix2 = (int)(ke >> 32);
-                    if (ix2 > rhi[q]) break;
-                    const int e = (int)(ke & 0xffffffffLL);
-                    double xb0[3];
-                    int src, jid;
-                    load_entry(A, e, xb0, src, jid);
-                    if (jid == 0 && A.ref[src] <= refa) continue;   // ih2 <= ih1
+                    const int4 idb = A.pk_id[s];
+                    const int ix2 = idb.z;
+                    if (ix2 < lo) continue;
+                    if (ix2 > hi) break;
+                    const int src = idb.x, jid = idb.w;
+                    if (jid == 0 && idb.y <= refa) continue;   // ih2 <= ih1
+                    const int e = jid == 0 ? src : idb.y;      // entry index (ghosts: nps + slot order)
+                    const double4 pb = A.pk_x[s];
+                    const double xb0[3] = {pb.x, pb.y, pb.z};
                     const int ii = (sx == 0.0) ? ix2 - ix : (sx < 0.0 ? ix2 - D.ncd - ix : ix2 + D.ncd - ix);
                     ncand++;
                     double xb[3], xbn[3], vb[3], xd[3];
@@ -384,7 +401,7 @@ __global__ void __launch_bounds__(128) k_collision(CollArgs<T> A)
                         xd[i] = xa[i] - xb[i];
                     }
                     const double dnij0 = sqrt(xd[0] * xd[0] + xd[1] * xd[1] + xd[2] * xd[2]);
-                    const double rb = A.rad[src];
+                    const double rb = pb.w;
                     const double rcoll = ra + rb;
                     const double rcolla = D.hdi ? rcoll : rcoll * (1.0 - D.st / 100.0);
                     const double rcollb = rcoll * (1.0 + D.st / 100.0);
@@ -514,7 +531,19 @@ __global__ void __launch_bounds__(128) k_collision(CollArgs<T> A)
         if (rs2 < A.remove_cap) A.remove[rs2] = refa + 1;
         else A.counts[6] = 1;
     }
-    if (ncand) atomicAdd(A.cand, ncand);
+    return ncand;
+}
+
+// One thread per sorted entry that is an owned droplet: consecutive threads own
+// neighbouring droplets of one cell row and stream overlapping ranges of the packed
+// entries.  The candidate count takes one atomic per warp.
+template <typename T>
+__global__ void __launch_bounds__(128) k_collision(CollArgs<T> A)
+{
+    const int sa = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned ncand = sa < A.ne ? collision_owner(A, sa) : 0u;
+    const unsigned tot = __reduce_add_sync(0xffffffffu, ncand);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(A.cand, (unsigned long long)tot);
 }
 
 __global__ void k_accumulate(int nbinsz, const int *hi, const double *hd, int *acc_i, double *acc_d)
@@ -525,16 +554,19 @@ __global__ void k_accumulate(int nbinsz, const int *hi, const double *hd, int *a
 }
 
 // OVERLAP_DET sweep (partlib.f90:2069-2156): per owned droplet, number of partners
-// (ypn index > ih1, 27 neighbour cells, half shell) within rcoll.
-__global__ void k_overlap(DevConst D, int nps, const double *px, const double *py, const double *pz, const Ghost *g,
-                          const int *row_start, const long long *row_ent, const int *cell_start, const int *ref,
-                          const double *rad,
+// (ypn index > ih1, 27 neighbour cells, half shell) within rcoll.  One thread per sorted
+// entry that is an owned droplet, streaming the packed entries.
+__global__ void k_overlap(DevConst D, int nps, int ne, const double4 *pk_x, const int4 *pk_id, const int *cell_start,
                           int jmax, int kmax, int2 *hits, int cap, int *cnt)
 {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= nps) return;
-    const double xa[3] = {px[a], py[a], pz[a]};
-    const int refa = ref[a];
+    const int sa = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sa >= ne) return;
+    const int4 ida = pk_id[sa];
+    if (ida.w != 0) return;   // ghost
+    const double4 pa = pk_x[sa];
+    const double xa[3] = {pa.x, pa.y, pa.z};
+    const double ra = pa.w;
+    const int refa = ida.y;
     int ix, iy, iz;
     own_cell(D, xa[0], xa[1], xa[2], ix, iy, iz);
     int nov = 0;
@@ -547,32 +579,32 @@ __global__ void k_overlap(DevConst D, int nps, const double *px, const double *p
             if (iz2 < 1) continue;
             if (iz2 <= D.ncd && iy2 < 1) continue;
             const int row = row_of(D, iy2, iz2);
-            const int rs = row_start[row], re_ = row_start[row + 1];
-            for (int ii = -1; ii <= 1; ii++) {
-                int ix2 = ix + ii;
-                double sx = 0.0;
-                if (ix2 < 1) { ix2 = D.ncd + ix2; sx = -1.0; }
-                else if (ix2 > D.ncd) { ix2 = ix2 % D.ncd; sx = 1.0; }
+            // x cells ix - 1 .. ix + 1: the part inside the box, then the wrapped cell
+#pragma unroll 1
+            for (int q = 0; q < 3; q++) {
+                int lo, hi;
+                double sx;
+                if (q == 0) {
+                    lo = max(1, ix - 1); hi = min(D.ncd, ix + 1); sx = 0.0;
+                } else if (q == 1) {
+                    if (ix - 1 >= 1) continue;
+                    lo = D.ncd; hi = D.ncd; sx = -1.0;
+                } else {
+                    if (ix + 1 <= D.ncd) continue;
+                    lo = 1; hi = 1; sx = 1.0;
+                }
                 int s0, s1;
-                cell_range(cell_start, row, D.ncd, rs, re_, ix2, ix2, s0, s1);
+                cell_range(cell_start, D, row, lo, hi, s0, s1);
                 for (int s = s0; s < s1; s++) {
-                    long long ke = row_ent[s];
-                    if ((int)(ke >> 32) != ix2) break;
-                    int e = (int)(ke & 0xffffffffLL);
-                    double xb[3];
-                    int src;
-                    if (e < nps) {
-                        src = e;
-                        if (ref[src] <= refa) continue;
-                        xb[1] = py[e]; xb[2] = pz[e];
-                    } else {
-                        src = g[e - nps].src;
-                        xb[1] = g[e - nps].y; xb[2] = g[e - nps].z;
-                    }
-                    xb[0] = px[src] + sx * D.hx;
+                    const int4 idb = pk_id[s];
+                    if (idb.z < lo) continue;
+                    if (idb.z > hi) break;
+                    if (idb.w == 0 && idb.y <= refa) continue;
+                    const double4 pb = pk_x[s];
+                    const double xb[3] = {pb.x + sx * D.hx, pb.y, pb.z};
                     double xd[3] = {xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2]};
                     double dnij = sqrt(xd[0] * xd[0] + xd[1] * xd[1] + xd[2] * xd[2]);
-                    double rcoll = rad[a] + rad[src];
+                    double rcoll = ra + pb.w;
                     if (dnij <= rcoll) nov++;
                 }
             }
@@ -963,8 +995,16 @@ int launch_headlist(dl_ctx *c, double dist)
             DL_CHECK_LAUNCH(c);
         }
     }
-    // per-cell entry starts (the searches of COLLISION_DET, OVERLAP_DET and the HDI walk)
-    const size_t cells = (size_t)c->nrows * (D.ncd + 1);
+    // bucketed cell starts (the searches of COLLISION_DET, OVERLAP_DET and the HDI walk):
+    // buckets of about half an entry on average, at most 32 cells
+    {
+        const double occ = (double)ne / ((double)c->nrows * (double)D.ncd);
+        int shift = 0;
+        while (shift < 5 && 2.0 * (double)(1 << (shift + 1)) * occ <= 1.0) shift++;
+        c->dc.cs_shift = shift;
+        c->dc.cs_nb = ((D.ncd - 1) >> shift) + 1;
+    }
+    const size_t cells = (size_t)c->nrows * (c->dc.cs_nb + 1);
     if (c->cell_start_cap < cells) {
         if (c->cell_start) cudaFree(c->cell_start);
         c->cell_start = nullptr;
@@ -973,9 +1013,26 @@ int launch_headlist(dl_ctx *c, double dist)
             return dl_fail(c, DL_E_ALLOC, "HEADLIST: cudaMalloc of the cell start table failed");
         c->cell_start_cap = cells;
     }
-    k_cell_starts<<<(int)(((int64_t)c->nrows * 32 + 255) / 256), 256, 0, c->stream>>>(
-        c->nrows, D.ncd, c->row_start, (const long long *)c->row_ent, c->cell_start);
+    k_cell_starts<<<(int)((cells + 255) / 256), 256, 0, c->stream>>>(
+        c->nrows, c->dc.cs_nb, c->dc.cs_shift, c->row_start, (const long long *)c->row_ent, c->cell_start);
     DL_CHECK_LAUNCH(c);
+    if ((size_t)ne > c->pk_cap) {
+        cudaFree(c->pk_x);
+        cudaFree(c->pk_id);
+        c->pk_x = nullptr;
+        c->pk_id = nullptr;
+        c->pk_cap = 0;
+        const size_t cap = std::max<size_t>((size_t)ne + ne / 4, 4096);
+        if (cudaMalloc(&c->pk_x, sizeof(double4) * cap) != cudaSuccess ||
+            cudaMalloc(&c->pk_id, sizeof(int4) * cap) != cudaSuccess)
+            return dl_fail(c, DL_E_ALLOC, "HEADLIST: cudaMalloc of the packed entries failed");
+        c->pk_cap = cap;
+    }
+    if (ne > 0) {
+        k_pack_entries<<<dl_blocks(ne, t), t, 0, c->stream>>>(ne, nps, (const long long *)c->row_ent, P[0], P[1], P[2],
+                                                              c->rad, c->ref_of_dev, c->ghosts, c->pk_x, c->pk_id);
+        DL_CHECK_LAUNCH(c);
+    }
     c->hl_dist = dist;
     c->hl_valid = 1;
     return 0;
@@ -993,13 +1050,11 @@ static int collision_t(dl_ctx *c, dl_coll_report *rep)
     memset(&A, 0, sizeof(A));
     A.D = D;
     A.nps = c->nps;
-    A.px = c->pos[c->pcur][0]; A.py = c->pos[c->pcur][1]; A.pz = c->pos[c->pcur][2];
-    A.g = c->ghosts;
-    A.row_start = c->row_start;
-    A.row_ent = (const long long *)c->row_ent;
+    A.ne = c->nps + c->nghost;
+    A.pk_x = c->pk_x;
+    A.pk_id = c->pk_id;
     A.cell_start = c->cell_start;
     A.ref = c->ref_of_dev;
-    A.rad = c->rad;
     const int vnew = c->have_vnew ? c->vnew : c->vcur;
     for (int k = 0; k < 3; k++) {
         A.dm[k] = tp<T>(c->dmv[k]);
@@ -1028,7 +1083,7 @@ static int collision_t(dl_ctx *c, dl_coll_report *rep)
     DL_CUDA(c, cudaMemsetAsync(c->counts, 0, sizeof(int) * ncount, c->stream));
     DL_CUDA(c, cudaMemsetAsync(c->cand, 0, sizeof(unsigned long long), c->stream));
     if (c->nps > 0) {
-        k_collision<T><<<dl_blocks(c->nps, t), t, 0, c->stream>>>(A);
+        k_collision<T><<<dl_blocks(A.ne, t), t, 0, c->stream>>>(A);
         DL_CHECK_LAUNCH(c);
     }
     k_accumulate<<<dl_blocks(7 * nbz, 256), 256, 0, c->stream>>>(nbz, c->hist_i, c->hist_d, c->acc_i, c->acc_d);
@@ -1092,10 +1147,9 @@ int launch_overlap_sweep(dl_ctx *c, std::vector<int2> &hits)
     const int kmax = 1 + (int)(d_overl * (double)D.ncd / D.hz);
     DL_CUDA(c, cudaMemsetAsync(c->ovl_cnt, 0, sizeof(int), c->stream));
     if (c->nps > 0) {
-        k_overlap<<<dl_blocks(c->nps, 128), 128, 0, c->stream>>>(
-            D, c->nps, c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2], c->ghosts, c->row_start,
-            (const long long *)c->row_ent, c->cell_start, c->ref_of_dev, c->rad, jmax, kmax, c->ovl_list, c->ovl_cap,
-            c->ovl_cnt);
+        const int ne = c->nps + c->nghost;
+        k_overlap<<<dl_blocks(ne, 128), 128, 0, c->stream>>>(D, c->nps, ne, c->pk_x, c->pk_id, c->cell_start, jmax, kmax,
+                                                             c->ovl_list, c->ovl_cap, c->ovl_cnt);
         DL_CHECK_LAUNCH(c);
     }
     int n = 0;

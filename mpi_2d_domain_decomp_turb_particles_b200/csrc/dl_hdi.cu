@@ -5,9 +5,10 @@
 // lists of the (2 nx_max + 1)(2 ny_max + 1)(2 nz_max + 1) cells around it, visits the
 // droplets ih2 > ih1 (ypn order) and appends a Stokes-disturbance tensor to ih1's list
 // (partner radius) and, for an owned ih2, to ih2's list (own radius).  Here one thread per
-// owned droplet walks the row-sorted cell list twice (count, then fill into a CSR over
-// the device order) and each owner's entries are then sorted by a key that reproduces
-// the reference's append order:
+// owned droplet, in cell order, streams the packed row-sorted cell list once, appending
+// each entry with its owner; the entries are scattered into a CSR over the device order
+// and each owner's entries are then sorted by a key that reproduces the reference's
+// append order:
 //   entries appended while an earlier ih1 was processed come first, by that ih1;
 //   then the owner's own walk: cell loop order (i, j, k), inside a cell descending ypn
 //   index (the head/list chain order).
@@ -90,31 +91,45 @@ struct NeiApp {
 
 struct NeiArgs {
     DevConst D;
-    int nps;
-    const double *px, *py, *pz, *rad;
-    const int *ref;
-    const Ghost *g;
-    const int *row_start;
-    const long long *row_ent;
+    int nps, ne;                  // droplets, sorted entries (droplets + ghosts)
+    const double4 *pk_x;          // packed sorted entries (HEADLIST)
+    const int4 *pk_id;
     const int *cell_start;
     int *cnt;                     // entries per owner
     NeiApp *app;                  // appended entries
     unsigned long long *napp;     // appended count (may exceed app_cap: then the walk is redone)
+    const double *rmax;           // largest radius of the current droplets
     unsigned long long app_cap;
     int *flag;                    // [0] overlapping owner + 1
 };
 
+// The lanes that emit together take consecutive slots with one atomic on the shared
+// counter (a single counter taking one atomic per entry serialises the walk).
 __device__ __forceinline__ void nei_emit(const NeiArgs &A, int owner, int partner, unsigned long long key,
                                          double arad, double dnij, const double *xd)
 {
     atomicAdd(&A.cnt[owner], 1);
-    const unsigned long long slot = atomicAdd(A.napp, 1ull);
+    const unsigned m = __activemask();
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(A.napp, (unsigned long long)__popc(m));
+    base = __shfl_sync(m, base, leader);
+    const unsigned long long slot = base + (unsigned)__popc(m & ((1u << lane) - 1u));
     if (slot >= A.app_cap) return;
     NeiApp &e = A.app[slot];
     e.owner = owner;
     e.partner = partner;
     e.key = key;
     stokes_tensor(arad, dnij, xd, e.coef);
+}
+
+// largest radius (positive doubles order like their bit patterns)
+__global__ void k_rad_max(int n, const double *rad, unsigned long long *out)
+{
+    double m = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = fmax(m, rad[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
 
 // appended entries -> CSR slots of their owners (order fixed afterwards by k_nei_sort)
@@ -130,77 +145,106 @@ __global__ void k_nei_scatter(int nnz, const NeiApp *app, const int *start, int 
     for (int t = 0; t < 6; t++) coef[(int64_t)slot * 6 + t] = e.coef[t];
 }
 
+// Cells of the search box that can hold a droplet within distance r of coordinate v
+// (cell index 1 + floor(v / h) as HEADLIST assigns it, widened by a millionth of a cell
+// against rounding at the faces).
+__device__ __forceinline__ int cell_below(double v, double r, double h)
+{
+    return (int)floor((v - r) / h - 1.0e-6) + 1;
+}
+__device__ __forceinline__ int cell_above(double v, double r, double h)
+{
+    return (int)floor((v + r) / h + 1.0e-6) + 1;
+}
+
+// One thread per sorted entry that is an owned droplet: consecutive threads own
+// neighbouring droplets of one cell row and stream overlapping entry ranges.  Of the
+// reference's (2 nx_max + 1)(2 ny_max + 1)(2 nz_max + 1) cells only those within
+// hdi_trunc * radmax of the owner are read: every entry (distance below hdi_trunc times
+// a radius) and every overlap (below the sum of two radii) lies there, and the entries
+// keep the keys of the full box.  The reach uses the largest radius of the current
+// droplets (coalescence can grow droplets past the largest initial radius).
 __global__ void __launch_bounds__(128) k_nei_walk(NeiArgs A)
 {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= A.nps) return;
+    const int sa = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sa >= A.ne) return;
+    const int4 ida = A.pk_id[sa];
+    if (ida.y >= A.nps) return;   // a ghost owns no list
     const DevConst &D = A.D;
-    const double xa[3] = {A.px[a], A.py[a], A.pz[a]};
-    const double ra = A.rad[a];
-    const int refa = A.ref[a];
+    const double4 pa = A.pk_x[sa];
+    const int a = ida.x, refa = ida.y;
+    const double xa[3] = {pa.x, pa.y, pa.z};
+    const double ra = pa.w;
     int ix, iy, iz;
     nei_cell(D, xa[0], xa[1], xa[2], ix, iy, iz);
     const int jlo = max(iy - D.ny_max, 1 - D.ny_max), jhi = min(iy + D.ny_max, D.ncd + D.ny_max);
     const int klo = max(iz - D.nz_max, 1 - D.nz_max), khi = min(iz + D.nz_max, D.ncd + D.nz_max);
     const int nj = 2 * D.ny_max + 1, nk = 2 * D.nz_max + 1;
     const int lo_raw = ix - D.nx_max, hi_raw = ix + D.nx_max;
-    // x ranges: [lo, hi] of cell indices ii with the shift sx and the unwrapped i = ii + ish
-    int rlo[3], rhi[3], ish[3];
-    double rsx[3];
-    int nr = 0;
-    rlo[nr] = max(1, lo_raw); rhi[nr] = min(D.ncd, hi_raw); rsx[nr] = 0.0; ish[nr] = 0; nr++;
-    if (lo_raw < 1) { rlo[nr] = lo_raw + D.ncd; rhi[nr] = D.ncd; rsx[nr] = -1.0; ish[nr] = -D.ncd; nr++; }
-    if (hi_raw > D.ncd) { rlo[nr] = 1; rhi[nr] = hi_raw - D.ncd; rsx[nr] = 1.0; ish[nr] = D.ncd; nr++; }
     const double trunc = D.hdi_trunc;
-    for (int j = jlo; j <= jhi; j++) {
-        for (int k = klo; k <= khi; k++) {
+    // one candidate droplet of cell (ix2 + ish, j, k) of the search box, shifted by sx * hx
+    auto visit = [=](int s, double sx, int ish, int jrel, int krel) {
+        const int4 idb = A.pk_id[s];
+        const bool ghost = idb.y >= A.nps;
+        if (!ghost && idb.y <= refa) return;   // ih2 <= ih1
+        const int src = idb.x, ypn2 = idb.y + 1, ix2 = idb.z;
+        const double4 pb = A.pk_x[s];
+        const double xb[3] = {pb.x + sx * D.hx, pb.y, pb.z};
+        double xd[3] = {xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2]};
+        const double dnij = sqrt(xd[0] * xd[0] + xd[1] * xd[1] + xd[2] * xd[2]);
+        const double rb = pb.w;
+        if (dnij < ra + rb) {                 // partlib.f90:3294-3299
+            atomicCAS(&A.flag[0], 0, a + 1);
+            return;
+        }
+        if (dnij < trunc * rb) {
+            const int irel = ix2 + ish - lo_raw;
+            const unsigned cell = (unsigned)((irel * nj + jrel) * nk + krel);
+            const unsigned long long key = (1ull << 62) | ((unsigned long long)cell << 32) |
+                                           (unsigned long long)(0xffffffffu - (unsigned)ypn2);
+            nei_emit(A, a, src, key, rb, dnij, xd);
+        }
+        if (!ghost && dnij < trunc * ra) {
+            const double nxd[3] = {-xd[0], -xd[1], -xd[2]};
+            nei_emit(A, src, a, (unsigned long long)(refa + 1), ra, dnij, nxd);
+        }
+    };
+    // the window of the box within reach (unwrapped x cell indices)
+    const double reach = fmax(trunc, 2.0) * *A.rmax;
+    const double cx = D.hx / D.ncd, cy = D.hy / D.ncd, cz = D.hz / D.ncd;
+    const int wlo = max(lo_raw, cell_below(xa[0], reach, cx)), whi = min(hi_raw, cell_above(xa[0], reach, cx));
+    const int j0 = max(jlo, cell_below(xa[1], reach, cy)), j1 = min(jhi, cell_above(xa[1], reach, cy));
+    const int k0 = max(klo, cell_below(xa[2], reach, cz)), k1 = min(khi, cell_above(xa[2], reach, cz));
+    const int mlo = max(1, wlo), mhi = min(D.ncd, whi);   // the part inside 1..ncd
+    for (int j = j0; j <= j1; j++) {
+        for (int k = k0; k <= k1; k++) {
             const int row = nei_row(D, j, k);
-            const int rs = A.row_start[row], re = A.row_start[row + 1];
-            if (rs == re) continue;
             const int jrel = j - (iy - D.ny_max), krel = k - (iz - D.nz_max);
-            for (int q = 0; q < nr; q++) {
+            if (mlo <= mhi) {
                 int s0, s1;
-                cell_range(A.cell_start, row, D.ncd, rs, re, rlo[q], rhi[q], s0, s1);
+                cell_range(A.cell_start, D, row, mlo, mhi, s0, s1);
                 for (int s = s0; s < s1; s++) {
-                    const long long ke = A.row_ent[s];
-                    const int ix2 = (int)(ke >> 32);
-                    if (ix2 > rhi[q]) break;
-                    const int e = (int)(ke & 0xffffffffLL);
-                    int src, ypn2;
-                    double xb[3];
-                    bool ghost = e >= A.nps;
-                    if (!ghost) {
-                        src = e;
-                        if (A.ref[src] <= refa) continue;   // ih2 <= ih1
-                        ypn2 = A.ref[src] + 1;
-                        xb[1] = A.py[src];
-                        xb[2] = A.pz[src];
-                    } else {
-                        const Ghost &gh = A.g[e - A.nps];
-                        src = gh.src;
-                        ypn2 = e + 1;                     // ghosts are stored in ypn order
-                        xb[1] = gh.y;
-                        xb[2] = gh.z;
-                    }
-                    xb[0] = A.px[src] + rsx[q] * D.hx;
-                    double xd[3] = {xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2]};
-                    const double dnij = sqrt(xd[0] * xd[0] + xd[1] * xd[1] + xd[2] * xd[2]);
-                    const double rb = A.rad[src];
-                    if (dnij < ra + rb) {                 // partlib.f90:3294-3299
-                        atomicCAS(&A.flag[0], 0, a + 1);
-                        continue;
-                    }
-                    if (dnij < trunc * rb) {
-                        const int irel = ix2 + ish[q] - lo_raw;
-                        const unsigned cell = (unsigned)((irel * nj + jrel) * nk + krel);
-                        const unsigned long long key = (1ull << 62) | ((unsigned long long)cell << 32) |
-                                                       (unsigned long long)(0xffffffffu - (unsigned)ypn2);
-                        nei_emit(A, a, src, key, rb, dnij, xd);
-                    }
-                    if (!ghost && dnij < trunc * ra) {
-                        const double nxd[3] = {-xd[0], -xd[1], -xd[2]};
-                        nei_emit(A, src, a, (unsigned long long)(refa + 1), ra, dnij, nxd);
-                    }
+                    const int ix2 = A.pk_id[s].z;
+                    if (ix2 < mlo) continue;
+                    if (ix2 > mhi) break;
+                    visit(s, 0.0, 0, jrel, krel);
+                }
+            }
+            // the parts that wrap around x (owners within reach of an x face)
+            if (wlo < 1) {
+                const int lo = wlo + D.ncd;
+                int s0, s1;
+                cell_range(A.cell_start, D, row, lo, D.ncd, s0, s1);
+                for (int s = s0; s < s1; s++)
+                    if (A.pk_id[s].z >= lo) visit(s, -1.0, -D.ncd, jrel, krel);
+            }
+            if (whi > D.ncd) {
+                const int hi = whi - D.ncd;
+                int s0, s1;
+                cell_range(A.cell_start, D, row, 1, hi, s0, s1);
+                for (int s = s0; s < s1; s++) {
+                    if (A.pk_id[s].z > hi) break;
+                    visit(s, 1.0, D.ncd, jrel, krel);
                 }
             }
         }
@@ -685,6 +729,7 @@ __global__ void __launch_bounds__(kArnThreads, kArnCtasPerSm) k_arn_spmv(ArnArgs
             const int e1 = A.start[a + 1];
             for (int e = A.start[a]; e < e1; e++) {
                 const int p = A.partner[e];
+                if (p < 0) continue;   // partner outside the coupled rows
                 const float x1 = w[p], x2 = w[A.ld + p], x3 = w[2 * A.ld + p];
                 const float *n = A.coef + (int64_t)e * 6;
                 r0 = __fmaf_rn(n[0], x1, __fmaf_rn(n[1], x2, __fmaf_rn(n[2], x3, r0)));
@@ -865,15 +910,83 @@ __global__ void __launch_bounds__(kArnThreads, kArnCtasPerSm) k_arn_cgs(ArnArgs 
     if (lane == 0) *A.ticket = 0u;
 }
 
-// x += Q y over the iterations the state reports
-__global__ void k_arn_xupdate(int64_t n, const ArnState *st, const float *Q, int64_t qld, double *x)
+// ---------------------------------------------------------------------------------------
+// Coupled rows.  A droplet without neighbour entries has an identity row in (I + N) and
+// a zero right-hand side, so the correction solve (I + N) d = r splits: d_U = r_U on
+// those rows exactly, and (I + N_CC) d_C = r_C - N_CU r_U on the rows with entries (a
+// few per cent of the droplets at HDI truncations of tens of radii).  The Arnoldi
+// kernels run on the coupled rows only, packed in device order (component c of coupled
+// row i at c * nc + i).
+// ---------------------------------------------------------------------------------------
+__global__ void k_red_flag(int nps, const int *start, int *flag)
 {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int it = st->iters;
-    double acc = 0.0;
-    for (int j = 0; j < it; j++) acc = acc + (double)Q[(int64_t)j * qld + i] * st->y[j];
-    x[i] = x[i] + acc;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < nps) flag[a] = start[a + 1] > start[a] ? 1 : 0;
+}
+
+// pos = exclusive scan of the flags: list[pos[a]] = a and the packed row starts (the
+// entries themselves stay where they are: the coupled rows keep their CSR segments)
+__global__ void k_red_rows(int nps, const int *start, const int *pos, int *list, int *rstart)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nps) return;
+    if (a == 0) rstart[pos[nps]] = start[nps];
+    if (start[a + 1] > start[a]) {
+        list[pos[a]] = a;
+        rstart[pos[a]] = start[a];
+    }
+}
+
+// partner -> its packed row, or -1 for an uncoupled partner
+__global__ void k_red_partner(int nnz, const int *partner, const int *pos, int *rpartner)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    const int p = partner[e];
+    rpartner[e] = pos[p + 1] > pos[p] ? pos[p] : -1;
+}
+
+// r_C - N_CU r_U, packed
+__global__ void k_red_rhs(int nc, int64_t ld, const int *list, const int *rstart, const int *partner,
+                          const int *rpartner, const float *coef, const float *rf, float *rc)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nc) return;
+    const int a = list[i];
+    float r0 = rf[a], r1 = rf[ld + a], r2 = rf[2 * ld + a];
+    const int e1 = rstart[i + 1];
+    for (int e = rstart[i]; e < e1; e++) {
+        if (rpartner[e] >= 0) continue;
+        const int p = partner[e];
+        const float x1 = rf[p], x2 = rf[ld + p], x3 = rf[2 * ld + p];
+        const float *n = coef + (int64_t)e * 6;
+        r0 = r0 - (n[0] * x1 + n[1] * x2 + n[2] * x3);
+        r1 = r1 - (n[1] * x1 + n[3] * x2 + n[4] * x3);
+        r2 = r2 - (n[2] * x1 + n[4] * x2 + n[5] * x3);
+    }
+    rc[i] = r0;
+    rc[nc + i] = r1;
+    rc[2 * nc + i] = r2;
+}
+
+// x += d: Q y on the coupled rows (when solved), r on the others
+__global__ void k_red_xupdate(int nps, const int *pos, const ArnState *st, int solved, const float *Q, int64_t qld,
+                              const double *r64, double *x)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 3 * (int64_t)nps) return;
+    const int comp = (int)(e / nps), a = (int)(e - (int64_t)comp * nps);
+    const int i0 = pos[a];
+    if (pos[a + 1] > i0) {
+        if (!solved) return;
+        const int64_t off = (int64_t)comp * pos[nps] + i0;
+        const int it = st->iters;
+        double acc = 0.0;
+        for (int j = 0; j < it; j++) acc = acc + (double)Q[(int64_t)j * qld + off] * st->y[j];
+        x[e] = x[e] + acc;
+    } else {
+        x[e] = x[e] + r64[e];
+    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -904,17 +1017,17 @@ size_t arn_bytes(const dl_ctx *c)
     return st + sizeof(float) * ((size_t)(kMaxIter + 1) * c->num_sms * kArnCtasPerSm + 2 * kMaxIter + 4) + 16;
 }
 
-ArnArgs arn_args(dl_ctx *c)
+ArnArgs arn_args(dl_ctx *c, int nc)
 {
     ArnArgs A;
     char *base = static_cast<char *>(c->arn);
     const size_t st = (sizeof(ArnState) + 255) / 256 * 256;
     const size_t gmax = (size_t)c->num_sms * kArnCtasPerSm;
-    A.nps = c->nps;
-    A.ld = c->nps;
+    A.nps = nc;
+    A.ld = nc;
     A.qld = 3 * (int64_t)c->msize;
-    A.start = c->nei_start;
-    A.partner = c->nei_idx;
+    A.start = c->red_start;
+    A.partner = c->red_partner;
     A.coef = tp<float>(c->nei_coef);
     A.Q = tp<float>(c->kry);
     A.st = reinterpret_cast<ArnState *>(base);
@@ -946,8 +1059,21 @@ int gmres_buffers(dl_ctx *c)
     }
     if (c->mixed && !c->arn) {
         const size_t bytes = arn_bytes(c);
-        if (cudaMalloc(&c->arn, bytes) != cudaSuccess) return dl_fail(c, DL_E_ALLOC, "HDI_GMRES: cudaMalloc failed");
+        const size_t m = (size_t)c->msize;
+        if (cudaMalloc(&c->arn, bytes) != cudaSuccess || cudaMalloc(&c->red_pos, sizeof(int) * (m + 1)) != cudaSuccess ||
+            cudaMalloc(&c->red_list, sizeof(int) * (m + 1)) != cudaSuccess ||
+            cudaMalloc(&c->red_start, sizeof(int) * (m + 1)) != cudaSuccess ||
+            cudaMalloc(&c->red_rhs, sizeof(float) * 3 * m) != cudaSuccess)
+            return dl_fail(c, DL_E_ALLOC, "HDI_GMRES: cudaMalloc failed");
         DL_CUDA(c, cudaMemsetAsync(c->arn, 0, bytes, c->stream));
+    }
+    if (c->mixed && c->red_partner_cap < c->nei_cap) {
+        cudaFree(c->red_partner);
+        c->red_partner = nullptr;
+        c->red_partner_cap = 0;
+        if (cudaMalloc(&c->red_partner, sizeof(int) * c->nei_cap) != cudaSuccess)
+            return dl_fail(c, DL_E_ALLOC, "HDI_GMRES: cudaMalloc failed");
+        c->red_partner_cap = c->nei_cap;
     }
     return 0;
 }
@@ -1171,15 +1297,33 @@ int gmres_fp64(dl_ctx *c, dl_gmres_report *rep)
     return g.converged ? 0 : DL_W_GMRES_NOT_CONVERGED;
 }
 
-// The FP32 correction solve of the mixed context: (I + N) d = r from d0 = 0, r = c->rf32
-// of norm nf, by the fused Arnoldi kernels, then x += d.  The iterations are queued in
-// batches (the first as long as this sweep's previous solve, then two at a time) and the
-// host reads the state once per batch.
-int arnoldi_f32(dl_ctx *c, int sweep, double norm_b, double nf, double stop_abs, double *x, int &iters)
+// The coupled rows of the current neighbour lists; nc = their count.
+int reduce_rows(dl_ctx *c, int &nc)
 {
-    const int64_t n3 = 3 * (int64_t)c->nps;
-    const ArnArgs A = arn_args(c);
-    const int G = arn_grid(c, c->nps);
+    const int nps = c->nps;
+    k_red_flag<<<dl_blocks(nps, 256), 256, 0, c->stream>>>(nps, c->nei_start, c->red_list);
+    DL_CHECK_LAUNCH(c);
+    DL_CUDA(c, dl_scan_counts(c->stream, c->red_list, c->red_pos, nps, c->nei_blk, nullptr));
+    k_red_rows<<<dl_blocks(nps, 256), 256, 0, c->stream>>>(nps, c->nei_start, c->red_pos, c->red_list, c->red_start);
+    DL_CHECK_LAUNCH(c);
+    if (c->nnz > 0) {
+        k_red_partner<<<dl_blocks(c->nnz, 256), 256, 0, c->stream>>>(c->nnz, c->nei_idx, c->red_pos, c->red_partner);
+        DL_CHECK_LAUNCH(c);
+    }
+    nc = 0;
+    DL_CUDA(c, cudaMemcpyAsync(&nc, c->red_pos + nps, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+// The FP32 solve of the coupled rows: (I + N_CC) d_C = c->red_rhs (norm nf) from d0 = 0
+// by the fused Arnoldi kernels; the coefficients stay in the state for the x update.
+// The iterations are queued in batches (the first as long as this sweep's previous
+// solve, then two at a time) and the host reads the state once per batch.
+int arnoldi_f32(dl_ctx *c, int sweep, int nc, double norm_b, double nf, double stop_abs, int &iters)
+{
+    const ArnArgs A = arn_args(c, nc);
+    const int G = arn_grid(c, nc);
     k_arn_init<<<8, 256, 0, c->stream>>>(A.st, norm_b, nf, stop_abs, A.s);
     DL_CHECK_LAUNCH(c);
     float *buf[2] = {tp<float>(c->wv), tp<float>(c->xt)};
@@ -1191,7 +1335,7 @@ int arnoldi_f32(dl_ctx *c, int sweep, double norm_b, double nf, double stop_abs,
         const int kend = std::min(kMaxIter, k + batch);
         while (k < kend) {
             k++;
-            const float *w = k == 1 ? c->rf32 : buf[(k - 1) & 1];
+            const float *w = k == 1 ? c->red_rhs : buf[(k - 1) & 1];
             float *v = buf[k & 1];
             k_arn_spmv<<<G, kArnThreads, 0, c->stream>>>(A, k, w, v);
             k_arn_cgs<2><<<G, kArnThreads, 0, c->stream>>>(A, k, v);
@@ -1205,8 +1349,6 @@ int arnoldi_f32(dl_ctx *c, int sweep, double norm_b, double nf, double stop_abs,
     }
     iters = hs.iters;
     guess = hs.iters;
-    k_arn_xupdate<<<(int)((n3 + 255) / 256), 256, 0, c->stream>>>(n3, A.st, A.Q, A.qld, x);
-    DL_CHECK_LAUNCH(c);
     return 0;
 }
 
@@ -1226,10 +1368,12 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
                                                  tp<float>(c->vel[vs][2]), tp<float>(dl_vp_ptr(c, 0)),
                                                  tp<float>(dl_vp_ptr(c, 1)), tp<float>(dl_vp_ptr(c, 2)), ld, b);
     DL_CHECK_LAUNCH(c);
-    int r;
+    int r, nc = 0;
+    if ((r = reduce_rows(c, nc))) return r;
     double nb2 = 0.0;
     if ((r = sumsq<double>(c, b, n3, &nb2))) return r;
     const double norm_b = std::sqrt(nb2);
+    const ArnArgs A = arn_args(c, nc);
     rep->iterations = 0;
     rep->refinements = 0;
     rep->residual = 0.0;
@@ -1253,16 +1397,28 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
         rep->residual = norm_b > 0.0 ? nr / norm_b : 0.0;
         if (sweep > 0 && rep->residual < kMaxErr) { converged = true; break; }
         if (sweep == kMaxRefine) break;
-        // FP32 correction: (I + N) d = r, d0 = 0
-        double nf2 = 0.0;
-        if ((r = sumsq<float>(c, c->rf32, n3, &nf2))) return r;
-        const double nf = std::sqrt(nf2);
-        if (!(nf > 0.0)) { converged = true; break; }
-        // stop the FP32 solve at a tenth of the FP64 target, or at FP32 resolution of r
-        const double stop_abs = std::max(0.1 * kMaxErr * norm_b, 1.0e-5 * nf);
-        int iters = 0;
-        if ((r = arnoldi_f32(c, sweep, norm_b, nf, stop_abs, x, iters))) return r;
-        rep->iterations += iters;
+        // correction (I + N) d = r: d_U = r_U, FP32 GMRES for d_C from d0 = 0
+        double nf = 0.0;
+        if (nc > 0) {
+            k_red_rhs<<<dl_blocks(nc, 256), 256, 0, c->stream>>>(nc, ld, c->red_list, c->red_start, c->nei_idx,
+                                                                 c->red_partner, tp<float>(c->nei_coef), c->rf32,
+                                                                 c->red_rhs);
+            DL_CHECK_LAUNCH(c);
+            double nf2 = 0.0;
+            if ((r = sumsq<float>(c, c->red_rhs, 3 * (int64_t)nc, &nf2))) return r;
+            nf = std::sqrt(nf2);
+        }
+        const bool solve = nf > 0.0;
+        if (solve) {
+            // stop the FP32 solve at a tenth of the FP64 target, or at FP32 resolution of r
+            const double stop_abs = std::max(0.1 * kMaxErr * norm_b, 1.0e-5 * nf);
+            int iters = 0;
+            if ((r = arnoldi_f32(c, sweep, nc, norm_b, nf, stop_abs, iters))) return r;
+            rep->iterations += iters;
+        }
+        k_red_xupdate<<<(int)((n3 + 255) / 256), 256, 0, c->stream>>>(nps, c->red_pos, A.st, solve ? 1 : 0, A.Q,
+                                                                      A.qld, r64, x);
+        DL_CHECK_LAUNCH(c);
     }
     k_uncopy3<double, float><<<bs, 256, 0, c->stream>>>(nps, x, ld, tp<float>(c->pert[0]), tp<float>(c->pert[1]),
                                                         tp<float>(c->pert[2]));
@@ -1307,12 +1463,9 @@ int launch_nei_list(dl_ctx *c)
     NeiArgs A;
     A.D = c->dc;
     A.nps = nps;
-    A.px = c->pos[c->pcur][0]; A.py = c->pos[c->pcur][1]; A.pz = c->pos[c->pcur][2];
-    A.rad = c->rad;
-    A.ref = c->ref_of_dev;
-    A.g = c->ghosts;
-    A.row_start = c->row_start;
-    A.row_ent = (const long long *)c->row_ent;
+    A.ne = nps + c->nghost;
+    A.pk_x = c->pk_x;
+    A.pk_id = c->pk_id;
     A.cell_start = c->cell_start;
     A.cnt = c->nei_cnt;
     A.app = reinterpret_cast<NeiApp *>(c->nei_app);
@@ -1322,9 +1475,12 @@ int launch_nei_list(dl_ctx *c)
     unsigned long long napp = 0;
     for (int attempt = 0; attempt < 2; attempt++) {
         // one walk finds every entry: counts per owner and the entries themselves
-        DL_CUDA(c, cudaMemsetAsync(d_napp, 0, sizeof(unsigned long long), c->stream));
+        DL_CUDA(c, cudaMemsetAsync(d_napp, 0, 2 * sizeof(unsigned long long), c->stream));
+        A.rmax = reinterpret_cast<const double *>(d_napp + 1);
+        k_rad_max<<<std::min(dl_blocks(nps, 256), 4 * c->num_sms), 256, 0, c->stream>>>(nps, c->rad, d_napp + 1);
+        DL_CHECK_LAUNCH(c);
         if (attempt) DL_CUDA(c, cudaMemsetAsync(c->nei_cnt, 0, sizeof(int) * (m + 1), c->stream));
-        k_nei_walk<<<dl_blocks(nps, 128), 128, 0, c->stream>>>(A);
+        k_nei_walk<<<dl_blocks(A.ne, 128), 128, 0, c->stream>>>(A);
         DL_CHECK_LAUNCH(c);
         DL_CUDA(c, cudaMemcpyAsync(&napp, d_napp, sizeof(napp), cudaMemcpyDeviceToHost, c->stream));
         DL_CUDA(c, cudaStreamSynchronize(c->stream));

@@ -25,6 +25,7 @@ struct DevConst {
     int nx_coll, ny_coll, nz_coll;   // collision search half-widths in cells
     int nx_max, ny_max, nz_max;      // halo depth of the cell grid (partlib.f90:137-151)
     int nyh, nzh;                    // rows of the cell grid including halo cells
+    int cs_shift, cs_nb;             // cell start table: buckets of 2^cs_shift x cells, cs_nb per row
     double dt, rnu, pi2, hx, hy, hz, dx;   // dx = pi2 / n (partlib.f90:315-317)
     double tau2, sv;                 // tau_CLOUD_const2, Sv_const
     double st, radmax;
@@ -139,8 +140,11 @@ struct dl_ctx {
     int *row_start;              // nrows + 1
     int *row_fill;
     int64_t *row_ent;            // sorted (ix << 32 | entry) per row
-    int *cell_start;             // [nrows][ncd + 1]: first entry of cell ix (ix - 1), then the row end
+    int *cell_start;             // [nrows][cs_nb + 1]: first entry of each bucket of x cells, then the row end
     size_t cell_start_cap;
+    double4 *pk_x;               // per sorted entry: x, y, z (ghost shift applied), radius
+    int4 *pk_id;                 // per sorted entry: source droplet, ypn index - 1, ix, ghost slot
+    size_t pk_cap;
     int nrows;
     int *long_rows;              // rows longer than the per-thread sort limit
     int *n_long;
@@ -212,6 +216,9 @@ struct dl_ctx {
     double *dots;                // reduction scratch
     void *arn;                   // fused FP32 Arnoldi: least-squares state, partial dots, scalars
     int arn_guess[8];            // iterations of the previous FP32 solve of each refinement sweep
+    int *red_pos, *red_list, *red_start, *red_partner;   // coupled rows of the mixed solve
+    size_t red_partner_cap;
+    float *red_rhs;              // right-hand side of the coupled rows (3 x coupled count)
     int gmres_iters, gmres_refine;
     double gmres_res, gmres_norm_rhs;
 
@@ -245,14 +252,15 @@ int dl_fail(dl_ctx *c, int code, const std::string &msg);
         (ctx)->launches++;                   \
         DL_CUDA(ctx, cudaGetLastError());    \
     } while (0)
-// Entries of cells lo..hi (x cell indices, 1-based) of one row of the cell list: [s0, s1).
-// Indices outside 1..ncd clamp to the row's ends, as a lower-bound search would.
-__device__ __forceinline__ void cell_range(const int *cs, int row, int ncd, int rs, int re, int lo, int hi, int &s0,
-                                           int &s1)
+// Entries of the x cells lo..hi (1 <= lo <= hi <= ncd) of one row of the cell list, as
+// the superset [s0, s1) of whole buckets of 2^cs_shift cells from the cell start table:
+// the entries of cells below lo (at the front) and above hi (at the back) are the
+// caller's to skip.
+__device__ __forceinline__ void cell_range(const int *cs, const DevConst &D, int row, int lo, int hi, int &s0, int &s1)
 {
-    const int64_t base = (int64_t)row * (ncd + 1);
-    s0 = lo <= 1 ? rs : (lo > ncd ? re : cs[base + lo - 1]);
-    s1 = hi >= ncd ? re : (hi < 1 ? rs : cs[base + hi]);
+    const int *c = cs + (int64_t)row * (D.cs_nb + 1);
+    s0 = c[(lo - 1) >> D.cs_shift];
+    s1 = c[min(D.cs_nb, ((hi - 1) >> D.cs_shift) + 1)];
 }
 #define CHECK_INIT(c)                                                                   \
     do {                                                                                \
