@@ -6,6 +6,7 @@
 // list) run here on the few affected droplets; everything proportional to the droplet
 // count runs in the kernels of dl_interp.cu, dl_cells.cu and dl_hdi.cu.
 #include "dl_internal.cuh"
+#include "dl_scan.cuh"
 
 #include <algorithm>
 #include <unordered_map>
@@ -86,43 +87,6 @@ double dl_ranff2(int *idum, int *iv, int *iy, int *idum2)
 // Small device helpers
 // ---------------------------------------------------------------------------------------
 namespace {
-
-__global__ void k_scan_blocks(const int *cnt, int *start, int m, int *carry_io)
-{
-    // one CTA, sequential chunks of 1024 (m is at most a few hundred thousand here)
-    __shared__ int ws[32];
-    __shared__ int carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int base = 0; base < m; base += blockDim.x) {
-        int i = base + threadIdx.x;
-        int v = i < m ? cnt[i] : 0;
-        int incl = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        if (lane == 31) ws[w] = incl;
-        __syncthreads();
-        if (w == 0) {
-            int s = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0, si = s;
-            for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_up_sync(0xffffffffu, si, o);
-                if (lane >= o) si += y;
-            }
-            ws[lane] = si - s;
-        }
-        __syncthreads();
-        int excl = carry + ws[w] + incl - v;
-        if (i < m) start[i] = excl;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) start[m] = carry;
-    (void)carry_io;
-}
 
 template <typename T>
 __global__ void k_upload(int nps, const double *yp, const double *fvp, const double *fdp, double *px, double *py,
@@ -288,9 +252,33 @@ __global__ void k_collist_gather(int m, int nps, int nghost, const int *ent, con
 
 int dl_scan(dl_ctx *c, const int *cnt, int *start, int m)
 {
-    k_scan_blocks<<<1, 1024, 0, c->stream>>>(cnt, start, m, nullptr);
-    DL_CHECK_LAUNCH(c);
+    const size_t need = 2 * ((size_t)m / 1024 + 2);
+    if (need > c->scan_cap) {
+        cudaFree(c->scan_buf);
+        c->scan_buf = nullptr;
+        c->scan_cap = 0;
+        if (cudaMalloc(&c->scan_buf, sizeof(int) * (need + need / 2)) != cudaSuccess)
+            return dl_fail(c, DL_E_ALLOC, "cudaMalloc of the scan scratch failed");
+        c->scan_cap = need + need / 2;
+    }
+    DL_CUDA(c, dl_scan_counts(c->stream, cnt, start, m, c->scan_buf, nullptr));
+    c->launches += 3;
     return 0;
+}
+
+// Device scratch of COALESCE, kept between calls (grown on demand; every use ends with a
+// synchronisation of the context's stream, so a grown buffer replaces an idle one).
+static void *co_scratch(dl_ctx *c, size_t bytes)
+{
+    if (bytes > c->co_cap) {
+        cudaFree(c->co_buf);
+        c->co_buf = nullptr;
+        c->co_cap = 0;
+        const size_t cap = std::max<size_t>(bytes + bytes / 2, 4096);
+        if (cudaMalloc(&c->co_buf, cap) != cudaSuccess) return nullptr;
+        c->co_cap = cap;
+    }
+    return c->co_buf;
 }
 
 void *dl_vp_ptr(dl_ctx *c, int k)
@@ -476,7 +464,7 @@ extern "C" int dl_destroy(dl_ctx *c)
     F(c->counts); F(c->cand); F(c->pairs); F(c->contacts); F(c->remove_dev); F(c->pair_buf); F(c->pair_ibuf); F(c->mv_acc);
     F(c->ovl_list); F(c->ovl_cnt); F(c->fpad_own);
     F(c->nei_cnt); F(c->nei_start); F(c->nei_idx); F(c->nei_coef); F(c->nei_coef64); F(c->overlap_flag);
-    F(c->kry); F(c->xg); F(c->rg); F(c->bg64); F(c->tmp64); F(c->wv); F(c->xt); F(c->dots); F(c->arn);
+    F(c->kry); F(c->xg); F(c->rg); F(c->bg64); F(c->tmp64); F(c->wv); F(c->xt); F(c->dots); F(c->arn); F(c->co_buf); F(c->scan_buf);
     F(c->red_pos); F(c->red_list); F(c->red_start); F(c->red_partner); F(c->red_rhs);
     F(c->nei_fill); F(c->nei_blk); F(c->nei_key); F(c->rf32); F(c->nei_app); F(c->cell_start); F(c->pk_x); F(c->pk_id);
     F(c->scal[0]); F(c->scal[1]); F(c->gr_part); F(c->gr_bins); F(c->gr_mdens); F(c->scal_field);
@@ -1327,10 +1315,10 @@ static int pert_keep(dl_ctx *c, const std::vector<int> &src, const std::vector<i
 {
     const int m = (int)src.size();
     if (m == 0 || !c->pert[0]) return 0;
-    int *d_idx = nullptr;
-    E *tmp = nullptr;
-    DL_CUDA(c, cudaMallocAsync((void **)&d_idx, sizeof(int) * 2 * m, c->stream));
-    DL_CUDA(c, cudaMallocAsync((void **)&tmp, sizeof(E) * 3 * m, c->stream));
+    char *buf = static_cast<char *>(co_scratch(c, sizeof(int) * 2 * m + 16 + sizeof(E) * 3 * m));
+    if (!buf) return dl_fail(c, DL_E_ALLOC, "COALESCE: cudaMalloc failed");
+    int *d_idx = reinterpret_cast<int *>(buf);
+    E *tmp = reinterpret_cast<E *>(buf + (sizeof(int) * 2 * m + 15) / 16 * 16);
     DL_CUDA(c, cudaMemcpyAsync(d_idx, src.data(), sizeof(int) * m, cudaMemcpyHostToDevice, c->stream));
     DL_CUDA(c, cudaMemcpyAsync(d_idx + m, dst.data(), sizeof(int) * m, cudaMemcpyHostToDevice, c->stream));
     E *P[3] = {tp<E>(c->pert[0]), tp<E>(c->pert[1]), tp<E>(c->pert[2])};
@@ -1338,8 +1326,6 @@ static int pert_keep(dl_ctx *c, const std::vector<int> &src, const std::vector<i
         k_move_by_ref<E><<<dl_blocks(m, 256), 256, 0, c->stream>>>(m, d_idx, d_idx + m, P[0], P[1], P[2], tmp, gather);
         DL_CHECK_LAUNCH(c);
     }
-    DL_CUDA(c, cudaFreeAsync(tmp, c->stream));
-    DL_CUDA(c, cudaFreeAsync(d_idx, c->stream));
     DL_CUDA(c, cudaStreamSynchronize(c->stream));   // the index vectors are host temporaries
     return 0;
 }
@@ -1371,13 +1357,12 @@ extern "C" int dl_coalesce(dl_ctx *c)
     const int m = (int)need.size();
     std::vector<int> got(m);
     {
-        int *d = nullptr;
-        DL_CUDA(c, cudaMallocAsync((void **)&d, sizeof(int) * 2 * m, c->stream));
+        int *d = static_cast<int *>(co_scratch(c, sizeof(int) * 2 * m));
+        if (!d) return dl_fail(c, DL_E_ALLOC, "COALESCE: cudaMalloc failed");
         DL_CUDA(c, cudaMemcpyAsync(d, need.data(), sizeof(int) * m, cudaMemcpyHostToDevice, c->stream));
         k_gather_int<<<dl_blocks(m, 256), 256, 0, c->stream>>>(m, d, c->dev_of_ref, d + m);
         DL_CHECK_LAUNCH(c);
         DL_CUDA(c, cudaMemcpyAsync(got.data(), d + m, sizeof(int) * m, cudaMemcpyDeviceToHost, c->stream));
-        DL_CUDA(c, cudaFreeAsync(d, c->stream));
         DL_CUDA(c, cudaStreamSynchronize(c->stream));
     }
     std::unordered_map<int, int> orig, slot;   // reference position -> device droplet (slot mutated by swaps)
@@ -1421,13 +1406,12 @@ extern "C" int dl_coalesce(dl_ctx *c)
     if (r) return r;
     if (!mdev.empty()) {
         const int k = (int)mdev.size();
-        int *d = nullptr;
-        DL_CUDA(c, cudaMallocAsync((void **)&d, sizeof(int) * 2 * k, c->stream));
+        int *d = static_cast<int *>(co_scratch(c, sizeof(int) * 2 * k));
+        if (!d) return dl_fail(c, DL_E_ALLOC, "COALESCE: cudaMalloc failed");
         DL_CUDA(c, cudaMemcpyAsync(d, mdev.data(), sizeof(int) * k, cudaMemcpyHostToDevice, c->stream));
         DL_CUDA(c, cudaMemcpyAsync(d + k, mref.data(), sizeof(int) * k, cudaMemcpyHostToDevice, c->stream));
         k_set_ref<<<dl_blocks(k, 256), 256, 0, c->stream>>>(k, d, d + k, c->ref_of_dev);
         DL_CHECK_LAUNCH(c);
-        DL_CUDA(c, cudaFreeAsync(d, c->stream));
         DL_CUDA(c, cudaStreamSynchronize(c->stream));   // the host vectors are temporaries
     }
     // deleted droplets (radius -1) are dropped by a compacting re-sort, which also rebuilds

@@ -178,25 +178,37 @@ __global__ void k_row_scatter(int ne, const int *ent_row, const int *ent_ix, con
 }
 
 // Sort each row by (ix, entry).  Rows hold tens of entries for uniformly spread droplets;
-// a thread sorts a row of up to kShortRow entries, longer rows are handed to k_row_sort_long.
+// a warp sorts a row of up to kShortRow entries (each lane ranks its one or two keys
+// against the row's, the keys being distinct), longer rows are handed to k_row_sort_long.
 constexpr int kShortRow = 64;
 constexpr int kLongRowMax = 4096;   // entries a CTA can sort in (static) shared memory
 
 __global__ void k_row_sort(int nrows, const int *row_start, long long *row_ent, int *long_rows, int *n_long)
 {
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= nrows) return;
-    int s = row_start[r], e = row_start[r + 1];
-    if (e - s > kShortRow) {
-        long_rows[atomicAdd(n_long, 1)] = r;
+    const int r = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (r >= nrows) return;   // the whole warp
+    const int s = row_start[r], len = row_start[r + 1] - s;
+    if (len <= 1) return;
+    if (len > kShortRow) {
+        if (lane == 0) long_rows[atomicAdd(n_long, 1)] = r;
         return;
     }
-    for (int i = s + 1; i < e; i++) {
-        long long v = row_ent[i];
-        int j = i - 1;
-        while (j >= s && row_ent[j] > v) { row_ent[j + 1] = row_ent[j]; j--; }
-        row_ent[j + 1] = v;
+    const long long v0 = lane < len ? row_ent[s + lane] : LLONG_MAX;
+    const long long v1 = lane + 32 < len ? row_ent[s + 32 + lane] : LLONG_MAX;
+    int r0 = 0, r1 = 0;
+    for (int i = 0; i < min(len, 32); i++) {
+        const long long u = __shfl_sync(0xffffffffu, v0, i);
+        r0 += u < v0;
+        r1 += u < v1;
     }
+    for (int i = 32; i < len; i++) {
+        const long long u = __shfl_sync(0xffffffffu, v1, i - 32);
+        r0 += u < v0;
+        r1 += u < v1;
+    }
+    __syncwarp();
+    if (lane < len) row_ent[s + r0] = v0;
+    if (lane + 32 < len) row_ent[s + r1] = v1;
 }
 
 // One CTA per long row: bitonic sort in shared memory (length padded to a power of two).
@@ -974,8 +986,8 @@ int launch_headlist(dl_ctx *c, double dist)
                                                              (long long *)c->row_ent);
         DL_CHECK_LAUNCH(c);
         DL_CUDA(c, cudaMemsetAsync(c->n_long, 0, sizeof(int), c->stream));
-        k_row_sort<<<dl_blocks(c->nrows, t), t, 0, c->stream>>>(c->nrows, c->row_start, (long long *)c->row_ent,
-                                                                c->long_rows, c->n_long);
+        k_row_sort<<<(int)(((int64_t)c->nrows * 32 + t - 1) / t), t, 0, c->stream>>>(
+            c->nrows, c->row_start, (long long *)c->row_ent, c->long_rows, c->n_long);
         DL_CHECK_LAUNCH(c);
         int nl = 0;
         DL_CUDA(c, cudaMemcpyAsync(&nl, c->n_long, sizeof(int), cudaMemcpyDeviceToHost, c->stream));

@@ -973,9 +973,9 @@ __global__ void k_red_rhs(int nc, int64_t ld, const int *list, const int *rstart
 __global__ void k_red_xupdate(int nps, const int *pos, const ArnState *st, int solved, const float *Q, int64_t qld,
                               const double *r64, double *x)
 {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= 3 * (int64_t)nps) return;
-    const int comp = (int)(e / nps), a = (int)(e - (int64_t)comp * nps);
+    const int a = blockIdx.x * blockDim.x + threadIdx.x, comp = blockIdx.y;
+    if (a >= nps) return;
+    const int64_t e = (int64_t)comp * nps + a;
     const int i0 = pos[a];
     if (pos[a + 1] > i0) {
         if (!solved) return;
@@ -1304,6 +1304,7 @@ int reduce_rows(dl_ctx *c, int &nc)
     k_red_flag<<<dl_blocks(nps, 256), 256, 0, c->stream>>>(nps, c->nei_start, c->red_list);
     DL_CHECK_LAUNCH(c);
     DL_CUDA(c, dl_scan_counts(c->stream, c->red_list, c->red_pos, nps, c->nei_blk, nullptr));
+    c->launches += 3;
     k_red_rows<<<dl_blocks(nps, 256), 256, 0, c->stream>>>(nps, c->nei_start, c->red_pos, c->red_list, c->red_start);
     DL_CHECK_LAUNCH(c);
     if (c->nnz > 0) {
@@ -1341,6 +1342,7 @@ int arnoldi_f32(dl_ctx *c, int sweep, int nc, double norm_b, double nf, double s
             k_arn_cgs<2><<<G, kArnThreads, 0, c->stream>>>(A, k, v);
             k_arn_cgs<3><<<G, kArnThreads, 0, c->stream>>>(A, k, v);
             DL_CHECK_LAUNCH(c);
+            c->launches += 2;
         }
         DL_CUDA(c, cudaMemcpyAsync(&hs, A.st, sizeof(hs), cudaMemcpyDeviceToHost, c->stream));
         DL_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -1416,8 +1418,8 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
             if ((r = arnoldi_f32(c, sweep, nc, norm_b, nf, stop_abs, iters))) return r;
             rep->iterations += iters;
         }
-        k_red_xupdate<<<(int)((n3 + 255) / 256), 256, 0, c->stream>>>(nps, c->red_pos, A.st, solve ? 1 : 0, A.Q,
-                                                                      A.qld, r64, x);
+        k_red_xupdate<<<dim3(dl_blocks(nps, 256), 3), 256, 0, c->stream>>>(nps, c->red_pos, A.st, solve ? 1 : 0, A.Q,
+                                                                             A.qld, r64, x);
         DL_CHECK_LAUNCH(c);
     }
     k_uncopy3<double, float><<<bs, 256, 0, c->stream>>>(nps, x, ld, tp<float>(c->pert[0]), tp<float>(c->pert[1]),

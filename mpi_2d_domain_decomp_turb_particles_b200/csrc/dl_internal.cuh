@@ -216,6 +216,10 @@ struct dl_ctx {
     double *dots;                // reduction scratch
     void *arn;                   // fused FP32 Arnoldi: least-squares state, partial dots, scalars
     int arn_guess[8];            // iterations of the previous FP32 solve of each refinement sweep
+    void *co_buf;                // COALESCE scratch (index lists, pertvel values), grown on demand
+    size_t co_cap;
+    int *scan_buf;               // multi-block scan scratch
+    size_t scan_cap;
     int *red_pos, *red_list, *red_start, *red_partner;   // coupled rows of the mixed solve
     size_t red_partner_cap;
     float *red_rhs;              // right-hand side of the coupled rows (3 x coupled count)
