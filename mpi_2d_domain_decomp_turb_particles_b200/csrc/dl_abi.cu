@@ -213,7 +213,7 @@ template <typename T>
 __global__ void k_collist_gather(int m, int nps, int nghost, const int *ent, const Ghost *g, const int *ref,
                                  const double *px, const double *py, const double *pz, const T *vx, const T *vy,
                                  const T *vz, const double *rad, const double *gid, int *out_ref, int *out_ypn,
-                                 double *rows)
+                                 int *out_jid, double *rows)
 {
     __shared__ int cnt;
     const int j = blockIdx.x;
@@ -238,6 +238,7 @@ __global__ void k_collist_gather(int m, int nps, int nghost, const int *ent, con
     if (threadIdx.x == 0) {
         out_ref[j] = ref[src] + 1;
         out_ypn[j] = ghost ? nps + cnt + 1 : ref[src] + 1;
+        out_jid[j] = ghost ? g[e - nps].jid : 0;
         double *r = rows + 8 * j;
         r[0] = px[src];
         r[1] = ghost ? g[e - nps].y : py[src];
@@ -248,7 +249,51 @@ __global__ void k_collist_gather(int m, int nps, int nghost, const int *ent, con
     }
 }
 
+// cell-list entries of the detected pairs: (a, b) per pair
+__global__ void k_pairs_ent(int np, const PairRec *pr, int *ent)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    ent[2 * i] = pr[i].a;
+    ent[2 * i + 1] = pr[i].b;
+}
+
+// statistics of a 5-step boundary: accumulated sums -> written copies, with thetabin
+// normalised by nirbin for the set pairs (1,1), (1,2), (2,2) (partlib.f90:1692-1697)
+__global__ void k_hist_boundary(int nbz, int nset, const int *acc_i, const double *acc_d, int *out_i, double *out_d)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 7 * nbz) return;
+    if (i < nbz) out_i[i] = acc_i[i];
+    double v = acc_d[i];
+    if (i >= 5 * nbz && i < 6 * nbz) {
+        const int hb = i - 5 * nbz;
+        const int s1 = hb % nset + 1, s2 = (hb / nset) % nset + 1;
+        const bool listed = (s1 == 1 && s2 == 1) || (s1 == 1 && s2 == 2) || (s1 == 2 && s2 == 2);
+        if (listed && acc_i[hb] != 0) v = v / (double)acc_i[hb];
+    }
+    out_d[i] = v;
+}
+
 }  // namespace
+
+// Pinned host staging for the small device -> host reads of a step (grown on demand),
+// so that the copies of one step go out together and one synchronisation collects them.
+void *dl_host_stage(dl_ctx *c, size_t bytes)
+{
+    if (bytes > c->hstage_cap) {
+        if (c->hstage) cudaFreeHost(c->hstage);
+        c->hstage = nullptr;
+        c->hstage_cap = 0;
+        const size_t cap = std::max<size_t>(bytes + bytes / 2, 1 << 16);
+        if (cudaHostAlloc(&c->hstage, cap, cudaHostAllocDefault) != cudaSuccess) {
+            c->hstage = nullptr;
+            return nullptr;
+        }
+        c->hstage_cap = cap;
+    }
+    return c->hstage;
+}
 
 int dl_scan(dl_ctx *c, const int *cnt, int *start, int m)
 {
@@ -429,7 +474,7 @@ static int allocate_state(dl_ctx *c)
     c->remove_cap = 2 * c->pair_cap + 16;
     ALLOC(c->remove_dev, sizeof(int) * c->remove_cap);
     ALLOC(c->pair_buf, sizeof(double) * 16 * c->pair_cap);
-    ALLOC(c->pair_ibuf, sizeof(int) * 6 * c->pair_cap);
+    ALLOC(c->pair_ibuf, sizeof(int) * 8 * c->pair_cap);
     ALLOC(c->mv_acc, sizeof(double) * (11 * 10 + 16));
     c->ovl_cap = std::max(4096, c->msize / 16);
     ALLOC(c->ovl_list, sizeof(int2) * c->ovl_cap);
@@ -465,6 +510,8 @@ extern "C" int dl_destroy(dl_ctx *c)
     F(c->ovl_list); F(c->ovl_cnt); F(c->fpad_own);
     F(c->nei_cnt); F(c->nei_start); F(c->nei_idx); F(c->nei_coef); F(c->nei_coef64); F(c->overlap_flag);
     F(c->kry); F(c->xg); F(c->rg); F(c->bg64); F(c->tmp64); F(c->wv); F(c->xt); F(c->dots); F(c->arn); F(c->co_buf); F(c->scan_buf);
+    if (c->hpin) cudaFreeHost(c->hpin);
+    if (c->hstage) cudaFreeHost(c->hstage);
     F(c->red_pos); F(c->red_list); F(c->red_start); F(c->red_partner); F(c->red_rhs);
     F(c->nei_fill); F(c->nei_blk); F(c->nei_key); F(c->rf32); F(c->nei_app); F(c->cell_start); F(c->pk_x); F(c->pk_id);
     F(c->scal[0]); F(c->scal[1]); F(c->gr_part); F(c->gr_bins); F(c->gr_mdens); F(c->scal_field);
@@ -1076,38 +1123,37 @@ static int collist_gather_t(dl_ctx *c, int m)
 {
     const int yv = c->have_vnew ? c->vnew : c->vcur;
     int *ent = c->pair_ibuf, *oref = c->pair_ibuf + 2 * c->pair_cap, *oypn = c->pair_ibuf + 4 * c->pair_cap;
+    int *ojid = c->pair_ibuf + 6 * c->pair_cap;
     k_collist_gather<T><<<m, 256, 0, c->stream>>>(m, c->nps, c->nghost, ent, c->ghosts, c->ref_of_dev,
                                                   c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2],
                                                   tp<T>(c->vel[yv][0]), tp<T>(c->vel[yv][1]),
-                                                  tp<T>(c->vel[yv][2]), c->rad, c->gid, oref, oypn, c->pair_buf);
+                                                  tp<T>(c->vel[yv][2]), c->rad, c->gid, oref, oypn, ojid,
+                                                  c->pair_buf);
     DL_CHECK_LAUNCH(c);
     return 0;
 }
 
+// Queues, for the np detected pairs in c->pairs, the gather of both droplets' collist
+// rows, reference and ypn indices and ghost slots into c->pair_ibuf / c->pair_buf.
+int dl_pairs_gather(dl_ctx *c, int np)
+{
+    if (np == 0) return 0;
+    if (np > c->pair_cap) return dl_fail(c, DL_E_CAPACITY, "COLLISION_DET: pair buffer full");
+    k_pairs_ent<<<dl_blocks(np, 256), 256, 0, c->stream>>>(np, c->pairs, c->pair_ibuf);
+    DL_CHECK_LAUNCH(c);
+    return c->mixed ? collist_gather_t<float>(c, 2 * np) : collist_gather_t<double>(c, 2 * np);
+}
+
 // Puts the detected pairs into the reference's detection order and builds collist
 // (partlib.f90:1557-1562): ih1 ascending, then the (i, j, k) cell loop, then the chain
-// order of the head/list cell (descending ypn index).
-int dl_pairs_to_host(dl_ctx *c, std::vector<PairRec> &pr)
+// order of the head/list cell (descending ypn index).  Inputs are the host copies of
+// the pair records and of what dl_pairs_gather produced (2 entries per pair).
+int dl_pairs_to_host(dl_ctx *c, const PairRec *pr, int np, const int *oref, const int *oypn, const int *ojid,
+                     const double *rows)
 {
-    const int np = (int)pr.size();
     c->pairs_host.clear();
     c->collist.clear();
     if (np == 0) return 0;
-    if (np > c->pair_cap) return dl_fail(c, DL_E_CAPACITY, "COLLISION_DET: pair buffer full");
-    std::vector<int> ent(2 * np);
-    for (int i = 0; i < np; i++) { ent[2 * i] = pr[i].a; ent[2 * i + 1] = pr[i].b; }
-    DL_CUDA(c, cudaMemcpyAsync(c->pair_ibuf, ent.data(), sizeof(int) * 2 * np, cudaMemcpyHostToDevice, c->stream));
-    int r = c->mixed ? collist_gather_t<float>(c, 2 * np) : collist_gather_t<double>(c, 2 * np);
-    if (r) return r;
-    std::vector<int> oref(2 * np), oypn(2 * np);
-    std::vector<double> rows(16 * (size_t)np);
-    DL_CUDA(c, cudaMemcpyAsync(oref.data(), c->pair_ibuf + 2 * c->pair_cap, sizeof(int) * 2 * np,
-                               cudaMemcpyDeviceToHost, c->stream));
-    DL_CUDA(c, cudaMemcpyAsync(oypn.data(), c->pair_ibuf + 4 * c->pair_cap, sizeof(int) * 2 * np,
-                               cudaMemcpyDeviceToHost, c->stream));
-    DL_CUDA(c, cudaMemcpyAsync(rows.data(), c->pair_buf, sizeof(double) * 16 * np, cudaMemcpyDeviceToHost,
-                               c->stream));
-    DL_CUDA(c, cudaStreamSynchronize(c->stream));
     std::vector<int> order(np);
     for (int i = 0; i < np; i++) order[i] = i;
     std::sort(order.begin(), order.end(), [&](int x, int y) {
@@ -1116,16 +1162,9 @@ int dl_pairs_to_host(dl_ctx *c, std::vector<PairRec> &pr)
         return oypn[2 * x + 1] > oypn[2 * y + 1];
     });
     for (int q : order) {
-        const bool ghost = pr[q].b >= c->nps;
-        int jid = 0;
-        if (ghost) {
-            Ghost g;
-            DL_CUDA(c, cudaMemcpy(&g, c->ghosts + (pr[q].b - c->nps), sizeof(Ghost), cudaMemcpyDeviceToHost));
-            jid = g.jid;
-        }
         c->pairs_host.push_back(oref[2 * q]);
         c->pairs_host.push_back(oref[2 * q + 1]);
-        c->pairs_host.push_back(jid);
+        c->pairs_host.push_back(ojid[2 * q + 1]);
         c->pairs_host.push_back(pr[q].type);
         double cl[20];
         for (int k = 0; k < 8; k++) cl[k] = rows[16 * (size_t)q + k];
@@ -1141,22 +1180,10 @@ int dl_pairs_to_host(dl_ctx *c, std::vector<PairRec> &pr)
 
 int dl_hist_boundary(dl_ctx *c)
 {
-    const int nbz = c->nbinsz, nset = c->dc.nset;
-    DL_CUDA(c, cudaStreamSynchronize(c->stream));
-    std::vector<int> hi(nbz);
-    std::vector<double> hd(7 * nbz);
-    DL_CUDA(c, cudaMemcpy(hi.data(), c->acc_i, sizeof(int) * nbz, cudaMemcpyDeviceToHost));
-    DL_CUDA(c, cudaMemcpy(hd.data(), c->acc_d, sizeof(double) * 7 * nbz, cudaMemcpyDeviceToHost));
-    // thetabin / nirbin for set pairs (1,1), (1,2), (2,2) (partlib.f90:1692-1697)
-    const int pairs_[3][2] = {{1, 1}, {1, 2}, {2, 2}};
-    for (int ikk = 0; ikk < DL_NBIN; ikk++)
-        for (auto &pp : pairs_) {
-            if (pp[1] > nset) continue;
-            int hb = (pp[0] - 1) + nset * ((pp[1] - 1) + nset * ikk);
-            if (hi[hb] != 0) hd[5 * nbz + hb] = hd[5 * nbz + hb] / (double)hi[hb];
-        }
-    DL_CUDA(c, cudaMemcpyAsync(c->out_i, hi.data(), sizeof(int) * nbz, cudaMemcpyHostToDevice, c->stream));
-    DL_CUDA(c, cudaMemcpyAsync(c->out_d, hd.data(), sizeof(double) * 7 * nbz, cudaMemcpyHostToDevice, c->stream));
+    const int nbz = c->nbinsz;
+    k_hist_boundary<<<dl_blocks(7 * nbz, 256), 256, 0, c->stream>>>(nbz, c->dc.nset, c->acc_i, c->acc_d, c->out_i,
+                                                                    c->out_d);
+    DL_CHECK_LAUNCH(c);
     DL_CUDA(c, cudaMemsetAsync(c->acc_i, 0, sizeof(int) * nbz, c->stream));
     DL_CUDA(c, cudaMemsetAsync(c->acc_d, 0, sizeof(double) * 7 * nbz, c->stream));
     return 0;

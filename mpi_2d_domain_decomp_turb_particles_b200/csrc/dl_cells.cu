@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstring>
 
 namespace {
 
@@ -1100,32 +1101,67 @@ static int collision_t(dl_ctx *c, dl_coll_report *rep)
     }
     k_accumulate<<<dl_blocks(7 * nbz, 256), 256, 0, c->stream>>>(nbz, c->hist_i, c->hist_d, c->acc_i, c->acc_d);
     DL_CHECK_LAUNCH(c);
-    std::vector<int> cnt(ncount);
-    unsigned long long cand = 0;
-    DL_CUDA(c, cudaMemcpyAsync(cnt.data(), c->counts, sizeof(int) * ncount, cudaMemcpyDeviceToHost, c->stream));
-    DL_CUDA(c, cudaMemcpyAsync(&cand, c->cand, sizeof(cand), cudaMemcpyDeviceToHost, c->stream));
+    // counts and the candidate total, then everything the host bookkeeping needs in one
+    // batch of copies into pinned staging
+    char *hs = static_cast<char *>(dl_host_stage(c, sizeof(int) * ncount + 16));
+    if (!hs) return dl_fail(c, DL_E_ALLOC, "cudaHostAlloc of the staging buffer failed");
+    DL_CUDA(c, cudaMemcpyAsync(hs, c->cand, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    DL_CUDA(c, cudaMemcpyAsync(hs + 16, c->counts, sizeof(int) * ncount, cudaMemcpyDeviceToHost, c->stream));
     DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    unsigned long long cand;
+    memcpy(&cand, hs, sizeof(cand));
+    std::vector<int> cnt(ncount);
+    memcpy(cnt.data(), hs + 16, sizeof(int) * ncount);
     if (cnt[6]) return dl_fail(c, DL_E_CAPACITY, "COLLISION_DET: pair, contact or removal buffer full");
     const int npairs = cnt[3], ncontact = cnt[4], nremove = cnt[5];
     if (npairs > c->p.ncollmax)
         return dl_fail(c, DL_E_CAPACITY, "COLLISION_DET: more collided pairs than ncollmax (collist capacity)");
-    // removal list: sort (hpsort, partlib.f90:1631)
-    c->removepart.resize(nremove);
-    if (nremove)
-        DL_CUDA(c, cudaMemcpy(c->removepart.data(), c->remove_dev, sizeof(int) * nremove, cudaMemcpyDeviceToHost));
-    std::sort(c->removepart.begin(), c->removepart.end());
-    // pairs in the reference's detection order -> collist and the pair rows
-    std::vector<PairRec> pr(npairs);
-    if (npairs) DL_CUDA(c, cudaMemcpy(pr.data(), c->pairs, sizeof(PairRec) * npairs, cudaMemcpyDeviceToHost));
     c->last_npairs = npairs;
     c->last_ncontact = ncontact;
     c->last_ntotpair = npairs;
-    int r = dl_pairs_to_host(c, pr);
-    if (r) return r;
+    c->removepart.resize(nremove);
+    c->pairs_host.clear();
+    c->collist.clear();
+    if (nremove || npairs) {
+        int r = dl_pairs_gather(c, npairs);
+        if (r) return r;
+        // staging layout: removal list | pair records | oref | oypn | jid | rows (8-byte aligned)
+        const size_t o_rem = 0, o_pr = (sizeof(int) * nremove + 15) / 16 * 16;
+        const size_t o_ref = o_pr + sizeof(PairRec) * npairs, o_ypn = o_ref + sizeof(int) * 2 * npairs;
+        const size_t o_jid = o_ypn + sizeof(int) * 2 * npairs;
+        const size_t o_rows = (o_jid + sizeof(int) * 2 * npairs + 15) / 16 * 16;
+        char *st = static_cast<char *>(dl_host_stage(c, o_rows + sizeof(double) * 16 * npairs + 16));
+        if (!st) return dl_fail(c, DL_E_ALLOC, "cudaHostAlloc of the staging buffer failed");
+        if (nremove)
+            DL_CUDA(c, cudaMemcpyAsync(st + o_rem, c->remove_dev, sizeof(int) * nremove, cudaMemcpyDeviceToHost,
+                                       c->stream));
+        if (npairs) {
+            const int *ib = c->pair_ibuf;
+            DL_CUDA(c, cudaMemcpyAsync(st + o_pr, c->pairs, sizeof(PairRec) * npairs, cudaMemcpyDeviceToHost,
+                                       c->stream));
+            DL_CUDA(c, cudaMemcpyAsync(st + o_ref, ib + 2 * c->pair_cap, sizeof(int) * 2 * npairs,
+                                       cudaMemcpyDeviceToHost, c->stream));
+            DL_CUDA(c, cudaMemcpyAsync(st + o_ypn, ib + 4 * c->pair_cap, sizeof(int) * 2 * npairs,
+                                       cudaMemcpyDeviceToHost, c->stream));
+            DL_CUDA(c, cudaMemcpyAsync(st + o_jid, ib + 6 * c->pair_cap, sizeof(int) * 2 * npairs,
+                                       cudaMemcpyDeviceToHost, c->stream));
+            DL_CUDA(c, cudaMemcpyAsync(st + o_rows, c->pair_buf, sizeof(double) * 16 * npairs,
+                                       cudaMemcpyDeviceToHost, c->stream));
+        }
+        DL_CUDA(c, cudaStreamSynchronize(c->stream));
+        // removal list: sort (hpsort, partlib.f90:1631)
+        memcpy(c->removepart.data(), st + o_rem, sizeof(int) * nremove);
+        std::sort(c->removepart.begin(), c->removepart.end());
+        // pairs in the reference's detection order -> collist and the pair rows
+        r = dl_pairs_to_host(c, reinterpret_cast<const PairRec *>(st + o_pr), npairs,
+                             reinterpret_cast<const int *>(st + o_ref), reinterpret_cast<const int *>(st + o_ypn),
+                             reinterpret_cast<const int *>(st + o_jid), reinterpret_cast<const double *>(st + o_rows));
+        if (r) return r;
+    }
     // histograms: 5-step boundary (partlib.f90:1659-1718)
     c->last_written = 0;
     if ((c->istep + 1) % 5 == 0) {
-        r = dl_hist_boundary(c);
+        const int r = dl_hist_boundary(c);
         if (r) return r;
         c->last_written = 1;
     }

@@ -152,16 +152,23 @@ __global__ void k_update(UpdArgs A)
     const bool alias = ik2_of(kx * kx + ky * ky + kz * kz) > A.G.nek;
     const double dth = 0.5 * A.dt, dtr = 1.5 * A.dt;
     const double lin = 1.0 - A.nu * dth * k2;
-    double2 v[3];
+    // all nine loads first: the stores to nold may alias the next component's loads as
+    // far as the compiler knows, which would serialise the three components
+    double2 nh[3], no[3], uu[3], v[3];
+#pragma unroll
     for (int c = 0; c < 3; c++) {
-        double2 nn = A.nh[c * A.G.M + m];
+        nh[c] = A.nh[c * A.G.M + m];
+        no[c] = A.nold[c * A.G.M + m];
+        uu[c] = A.u[c * A.G.M + m];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        double2 nn = nh[c];
         nn.x *= A.inv_n3;
         nn.y *= A.inv_n3;
         if (alias) nn = make_double2(0.0, 0.0);
-        const double2 no = A.nold[c * A.G.M + m];
-        const double2 uu = A.u[c * A.G.M + m];
-        v[c].x = uu.x * lin + dtr * nn.x - dth * no.x;
-        v[c].y = uu.y * lin + dtr * nn.y - dth * no.y;
+        v[c].x = uu[c].x * lin + dtr * nn.x - dth * no[c].x;
+        v[c].y = uu[c].y * lin + dtr * nn.y - dth * no[c].y;
         A.nold[c * A.G.M + m] = nn;
     }
     // stochastic forcing on the modes kx <= 2, |ky|, |kz| <= 2 (flowlib.f90:522-560)

@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
+#include <cstring>
 #include <vector>
 
 namespace {
@@ -969,24 +970,28 @@ __global__ void k_red_rhs(int nc, int64_t ld, const int *list, const int *rstart
     rc[2 * nc + i] = r2;
 }
 
-// x += d: Q y on the coupled rows (when solved), r on the others
-__global__ void k_red_xupdate(int nps, const int *pos, const ArnState *st, int solved, const float *Q, int64_t qld,
-                              const double *r64, double *x)
+// x += d: r on the uncoupled rows (the first blocks, one thread per droplet), Q y on the
+// coupled rows when solved (the remaining blocks, one thread per coupled row)
+__global__ void k_red_xupdate(int nps, int nc, const int *pos, const int *list, const ArnState *st, int solved,
+                              const float *Q, int64_t qld, const double *r64, double *x)
 {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x, comp = blockIdx.y;
-    if (a >= nps) return;
-    const int64_t e = (int64_t)comp * nps + a;
-    const int i0 = pos[a];
-    if (pos[a + 1] > i0) {
-        if (!solved) return;
-        const int64_t off = (int64_t)comp * pos[nps] + i0;
-        const int it = st->iters;
-        double acc = 0.0;
-        for (int j = 0; j < it; j++) acc = acc + (double)Q[(int64_t)j * qld + off] * st->y[j];
-        x[e] = x[e] + acc;
-    } else {
+    const int comp = blockIdx.y, nbu = (nps + 255) / 256;
+    if ((int)blockIdx.x < nbu) {
+        const int a = blockIdx.x * 256 + threadIdx.x;
+        if (a >= nps || pos[a + 1] > pos[a]) return;
+        const int64_t e = (int64_t)comp * nps + a;
         x[e] = x[e] + r64[e];
+        return;
     }
+    if (!solved) return;
+    const int i = (blockIdx.x - nbu) * 256 + threadIdx.x;
+    if (i >= nc) return;
+    const int it = st->iters;
+    const float *q = Q + (int64_t)comp * nc + i;
+    double acc = 0.0;
+    for (int j = 0; j < it; j++) acc = acc + (double)q[(int64_t)j * qld] * st->y[j];
+    const int64_t e = (int64_t)comp * nps + list[i];
+    x[e] = x[e] + acc;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1108,6 +1113,45 @@ int sumsq(dl_ctx *c, const T *x, int64_t n, double *out)
     DL_CUDA(c, cudaStreamSynchronize(c->stream));
     *out = (double)v;
     return 0;
+}
+
+// Result slots for reductions whose values the host reads together (8 bytes each, after
+// the reduction scratch in c->dots), and the pinned host buffer they are read into.
+constexpr int kSlot0 = kRedGrid + kMaxIter + 4;
+
+int pinned(dl_ctx *c)
+{
+    if (!c->hpin && cudaHostAlloc(&c->hpin, 256, cudaHostAllocDefault) != cudaSuccess) {
+        c->hpin = nullptr;
+        return dl_fail(c, DL_E_ALLOC, "cudaHostAlloc of 256 bytes failed");
+    }
+    return 0;
+}
+
+template <typename T>
+int sumsq_to_slot(dl_ctx *c, const T *x, int64_t n, int slot)
+{
+    Red<T> R = red_of<T>(c);
+    k_sumsq<T><<<kRedGrid, kRedThreads, 0, c->stream>>>(n, x, reinterpret_cast<T *>(c->dots + kSlot0 + slot),
+                                                        R.partials, R.ticket);
+    DL_CHECK_LAUNCH(c);
+    return 0;
+}
+
+// slots [0, n) -> c->hpin (as 8-byte words), after whatever else was queued to c->hpin
+int read_slots(dl_ctx *c, int n)
+{
+    DL_CUDA(c, cudaMemcpyAsync(c->hpin, c->dots + kSlot0, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+template <typename T>
+double slot_value(const dl_ctx *c, int slot)
+{
+    T v;
+    memcpy(&v, static_cast<const char *>(c->hpin) + sizeof(double) * slot, sizeof(T));
+    return (double)v;
 }
 
 template <typename T, typename C>
@@ -1297,7 +1341,8 @@ int gmres_fp64(dl_ctx *c, dl_gmres_report *rep)
     return g.converged ? 0 : DL_W_GMRES_NOT_CONVERGED;
 }
 
-// The coupled rows of the current neighbour lists; nc = their count.
+// The coupled rows of the current neighbour lists; their count is read with the next
+// read_slots (word 8 of the pinned buffer).
 int reduce_rows(dl_ctx *c, int &nc)
 {
     const int nps = c->nps;
@@ -1311,9 +1356,10 @@ int reduce_rows(dl_ctx *c, int &nc)
         k_red_partner<<<dl_blocks(c->nnz, 256), 256, 0, c->stream>>>(c->nnz, c->nei_idx, c->red_pos, c->red_partner);
         DL_CHECK_LAUNCH(c);
     }
-    nc = 0;
-    DL_CUDA(c, cudaMemcpyAsync(&nc, c->red_pos + nps, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    // the count arrives in word 8 of the pinned buffer with the next read_slots
+    DL_CUDA(c, cudaMemcpyAsync(static_cast<char *>(c->hpin) + 64, c->red_pos + nps, sizeof(int),
+                               cudaMemcpyDeviceToHost, c->stream));
+    nc = -1;
     return 0;
 }
 
@@ -1371,10 +1417,12 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
                                                  tp<float>(dl_vp_ptr(c, 1)), tp<float>(dl_vp_ptr(c, 2)), ld, b);
     DL_CHECK_LAUNCH(c);
     int r, nc = 0;
+    if ((r = pinned(c))) return r;
     if ((r = reduce_rows(c, nc))) return r;
-    double nb2 = 0.0;
-    if ((r = sumsq<double>(c, b, n3, &nb2))) return r;
-    const double norm_b = std::sqrt(nb2);
+    if ((r = sumsq_to_slot<double>(c, b, n3, 0))) return r;
+    if ((r = read_slots(c, 1))) return r;
+    const double norm_b = std::sqrt(slot_value<double>(c, 0));
+    memcpy(&nc, static_cast<const char *>(c->hpin) + 64, sizeof(int));
     const ArnArgs A = arn_args(c, nc);
     rep->iterations = 0;
     rep->refinements = 0;
@@ -1386,9 +1434,17 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
         k_residual64<<<bs, 256, 0, c->stream>>>(nps, c->nei_start, c->nei_idx, c->nei_coef64, x, ld, b, r64, c->rf32);
         DL_CHECK_LAUNCH(c);
         rep->refinements = sweep + 1;
-        double rr = 0.0;
-        if ((r = sumsq<double>(c, r64, n3, &rr))) return r;
-        const double nr = std::sqrt(rr);
+        if ((r = sumsq_to_slot<double>(c, r64, n3, 1))) return r;
+        // the reduced right-hand side of the correction and its norm, read with ||r||
+        if (nc > 0) {
+            k_red_rhs<<<dl_blocks(nc, 256), 256, 0, c->stream>>>(nc, ld, c->red_list, c->red_start, c->nei_idx,
+                                                                 c->red_partner, tp<float>(c->nei_coef), c->rf32,
+                                                                 c->red_rhs);
+            DL_CHECK_LAUNCH(c);
+            if ((r = sumsq_to_slot<float>(c, c->red_rhs, 3 * (int64_t)nc, 2))) return r;
+        }
+        if ((r = read_slots(c, 3))) return r;
+        const double nr = std::sqrt(slot_value<double>(c, 1));
         if (sweep == 0) {
             rep->norm_rhs = nr;
             if (nr < kSmallRhs) {   // nothing to solve: pertvel unchanged (partlib.f90:2853-2856)
@@ -1400,16 +1456,7 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
         if (sweep > 0 && rep->residual < kMaxErr) { converged = true; break; }
         if (sweep == kMaxRefine) break;
         // correction (I + N) d = r: d_U = r_U, FP32 GMRES for d_C from d0 = 0
-        double nf = 0.0;
-        if (nc > 0) {
-            k_red_rhs<<<dl_blocks(nc, 256), 256, 0, c->stream>>>(nc, ld, c->red_list, c->red_start, c->nei_idx,
-                                                                 c->red_partner, tp<float>(c->nei_coef), c->rf32,
-                                                                 c->red_rhs);
-            DL_CHECK_LAUNCH(c);
-            double nf2 = 0.0;
-            if ((r = sumsq<float>(c, c->red_rhs, 3 * (int64_t)nc, &nf2))) return r;
-            nf = std::sqrt(nf2);
-        }
+        const double nf = nc > 0 ? std::sqrt(slot_value<float>(c, 2)) : 0.0;
         const bool solve = nf > 0.0;
         if (solve) {
             // stop the FP32 solve at a tenth of the FP64 target, or at FP32 resolution of r
@@ -1418,8 +1465,8 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
             if ((r = arnoldi_f32(c, sweep, nc, norm_b, nf, stop_abs, iters))) return r;
             rep->iterations += iters;
         }
-        k_red_xupdate<<<dim3(dl_blocks(nps, 256), 3), 256, 0, c->stream>>>(nps, c->red_pos, A.st, solve ? 1 : 0, A.Q,
-                                                                             A.qld, r64, x);
+        k_red_xupdate<<<dim3(dl_blocks(nps, 256) + dl_blocks(nc, 256), 3), 256, 0, c->stream>>>(
+            nps, nc, c->red_pos, c->red_list, A.st, solve ? 1 : 0, A.Q, A.qld, r64, x);
         DL_CHECK_LAUNCH(c);
     }
     k_uncopy3<double, float><<<bs, 256, 0, c->stream>>>(nps, x, ld, tp<float>(c->pert[0]), tp<float>(c->pert[1]),
@@ -1475,6 +1522,8 @@ int launch_nei_list(dl_ctx *c)
     A.app_cap = c->nei_app_cap;
     A.flag = c->overlap_flag;
     unsigned long long napp = 0;
+    int pr = pinned(c);
+    if (pr) return pr;
     for (int attempt = 0; attempt < 2; attempt++) {
         // one walk finds every entry: counts per owner and the entries themselves
         DL_CUDA(c, cudaMemsetAsync(d_napp, 0, 2 * sizeof(unsigned long long), c->stream));
@@ -1484,9 +1533,17 @@ int launch_nei_list(dl_ctx *c)
         if (attempt) DL_CUDA(c, cudaMemsetAsync(c->nei_cnt, 0, sizeof(int) * (m + 1), c->stream));
         k_nei_walk<<<dl_blocks(A.ne, 128), 128, 0, c->stream>>>(A);
         DL_CHECK_LAUNCH(c);
-        DL_CUDA(c, cudaMemcpyAsync(&napp, d_napp, sizeof(napp), cudaMemcpyDeviceToHost, c->stream));
+        // CSR offsets and the largest count (the counts are complete even when the entry
+        // buffer overflowed); one read for the entry count and the flags
+        DL_CUDA(c, dl_scan_counts(c->stream, c->nei_cnt, c->nei_start, nps, c->nei_blk, c->overlap_flag + 2));
+        c->launches += 3;
+        DL_CUDA(c, cudaMemcpyAsync(c->hpin, d_napp, sizeof(napp), cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaMemcpyAsync(static_cast<char *>(c->hpin) + 16, c->overlap_flag, sizeof(int) * 4,
+                                   cudaMemcpyDeviceToHost, c->stream));
         DL_CUDA(c, cudaStreamSynchronize(c->stream));
+        memcpy(&napp, c->hpin, sizeof(napp));
         if (napp <= c->nei_app_cap) break;
+        DL_CUDA(c, cudaMemsetAsync(c->overlap_flag, 0, sizeof(int) * 4, c->stream));
         // more entries than the buffer holds: grow it and walk again
         cudaFree(c->nei_app);
         c->nei_app = nullptr;
@@ -1500,12 +1557,9 @@ int launch_nei_list(dl_ctx *c)
         A.app_cap = c->nei_app_cap;
     }
     if (napp > c->nei_app_cap) return dl_fail(c, DL_E_STATE, "NEI_LIST_PRECOMP: entry buffer still too small");
-    // CSR offsets and the capacity check (the reference allows nei_max = 100 per droplet)
-    DL_CUDA(c, dl_scan_counts(c->stream, c->nei_cnt, c->nei_start, nps, c->nei_blk, c->overlap_flag + 2));
-    c->launches += 3;
-    int hf[4] = {0, 0, 0, 0};
-    DL_CUDA(c, cudaMemcpyAsync(hf, c->overlap_flag, sizeof(int) * 4, cudaMemcpyDeviceToHost, c->stream));
-    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    // the capacity check (the reference allows nei_max = 100 per droplet)
+    int hf[4];
+    memcpy(hf, static_cast<const char *>(c->hpin) + 16, sizeof(hf));
     const int nnz = (int)napp;
     if (hf[0]) {
         int ref = -1;

@@ -216,6 +216,9 @@ struct dl_ctx {
     double *dots;                // reduction scratch
     void *arn;                   // fused FP32 Arnoldi: least-squares state, partial dots, scalars
     int arn_guess[8];            // iterations of the previous FP32 solve of each refinement sweep
+    void *hpin;                  // 256 bytes of pinned host memory for small device->host reads
+    void *hstage;                // pinned staging of a step's variable-size reads (grown on demand)
+    size_t hstage_cap;
     void *co_buf;                // COALESCE scratch (index lists, pertvel values), grown on demand
     size_t co_cap;
     int *scan_buf;               // multi-block scan scratch
@@ -305,7 +308,10 @@ int run_gmres(dl_ctx *c, dl_gmres_report *rep);
 // dl_abi.cu helpers
 int dl_scan(dl_ctx *c, const int *cnt, int *start, int m);
 void *dl_vp_ptr(dl_ctx *c, int k);
-int dl_pairs_to_host(dl_ctx *c, std::vector<PairRec> &pr);
+int dl_pairs_gather(dl_ctx *c, int np);
+int dl_pairs_to_host(dl_ctx *c, const PairRec *pr, int np, const int *oref, const int *oypn, const int *ojid,
+                     const double *rows);
+void *dl_host_stage(dl_ctx *c, size_t bytes);
 int dl_hist_boundary(dl_ctx *c);
 int dl_apply_remap(dl_ctx *c, const std::vector<int> &old_ref, const std::vector<int> &new_ref);
 void dl_brick_dims(int mixed, int *bx, int *by, int *bz);
