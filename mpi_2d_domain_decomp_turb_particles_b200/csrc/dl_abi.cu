@@ -486,6 +486,7 @@ static int allocate_state(dl_ctx *c)
     c->fp_comp = c->fp_plane * e;
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
     if (c->num_sms <= 0) c->num_sms = 148;
+    c->arn_coop_ctas = -1;
     return 0;
 }
 

@@ -27,7 +27,10 @@
 //   mixed context: FP32 Krylov vectors, FP32 tensors and FP32 accumulation for the
 //     iterations, wrapped in FP64 residual refinement: r = b - (I + N) x with FP64
 //     tensors and FP64 x, an FP32 GMRES solve for the correction, x += d, until the FP64
-//     relative residual ||b - (I + N) x|| / ||b|| is below 1e-6.
+//     relative residual ||b - (I + N) x|| / ||b|| is below 1e-6.  The FP32 solve runs
+//     on the coupled rows only (droplets with neighbour entries) as one cooperative
+//     launch (k_arn_solve), or as three launches per iteration where the grid cannot be
+//     resident at once.
 #include "dl_internal.cuh"
 #include "dl_scan.cuh"
 
@@ -566,6 +569,8 @@ struct ArnArgs {
     float *h1, *h2;       // [kMaxIter] projections of the two passes
     float *s;             // [0] norm of the vector the next k_arn_spmv normalises
     unsigned *ticket;
+    float *part2;         // second bank of partial sums (cooperative solve)
+    unsigned *sync;       // grid barrier of the cooperative solve: count, generation, error
 };
 
 __device__ __forceinline__ float warp_sum_f(float v)
@@ -697,8 +702,9 @@ __device__ __forceinline__ void arn_finish_dots(const ArnArgs &A, int k, const f
     if (threadIdx.x == 0) *A.ticket = 0u;
 }
 
-__global__ void k_arn_init(ArnState *st, double norm_b, double norm_rhs, double stop_abs, float *s)
+__global__ void k_arn_init(ArnState *st, double norm_b, double norm_rhs, double stop_abs, float *s, unsigned *sync)
 {
+    if (blockIdx.x == 0 && threadIdx.x < 4) sync[threadIdx.x] = 0u;
     double *p = reinterpret_cast<double *>(st);
     const int nd = (int)(sizeof(ArnState) / sizeof(double));
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nd; i += gridDim.x * blockDim.x) {
@@ -970,6 +976,276 @@ __global__ void k_red_rhs(int nc, int64_t ld, const int *list, const int *rstart
     rc[2 * nc + i] = r2;
 }
 
+// ---------------------------------------------------------------------------------------
+// The whole FP32 solve as one cooperative launch: the same three phases per iteration,
+// separated by grid barriers instead of kernel boundaries.  Every CTA reduces the
+// per-CTA partial sums itself (same data, same order: the same values in every CTA), so
+// a phase needs one barrier; the partial sums alternate between two banks so that a
+// bank is rewritten only after every CTA has read it.  The least-squares problem is
+// kept as the usual Givens rotations (cs, sn) and rotated right-hand side g, updated
+// redundantly by every CTA; the residual estimate is |g_{k+1}|.  CTA 0 keeps the
+// triangular factor and solves for y at the end.  Values other CTAs wrote are read
+// with ld.global.cg (L1 is not coherent across SMs).
+// ---------------------------------------------------------------------------------------
+constexpr unsigned kSpinLimit = 1u << 22;   // ~0.3 s of polling before a barrier gives up
+constexpr int kArnCoopCtasPerSm = kArnCtasPerSm;   // CTAs per SM of the cooperative solve
+
+// Grid barrier for co-resident CTAs (cooperative launch).  Bounded: a CTA that polls
+// kSpinLimit times without the generation moving sets the error word and returns false.
+__device__ __forceinline__ bool arn_grid_sync(unsigned *sy)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = sy + 1;
+        const unsigned g0 = *gen;
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(sy, 1u) == gridDim.x - 1) {
+            sy[0] = 0u;
+            __threadfence();
+            atomicAdd(sy + 1, 1u);
+        } else {
+            unsigned spins = 0;
+            while (*gen == g0) {
+                if (++spins > kSpinLimit) {
+                    ok = 0;
+                    atomicExch(sy + 2, 1u);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok && *(volatile unsigned *)(sy + 2) == 0u;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// this CTA's partial sums (dots of the warps' basis vectors, and/or the norm) -> bank P
+__device__ __forceinline__ void arn_put_partials(float *P, int k, const float *acc, bool dots, float nrm, bool norm)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, G = gridDim.x;
+    if (dots) {
+#pragma unroll
+        for (int m = 0; m < kArnSlots; m++) {
+            const int j = w + m * kArnWarps;
+            if (j < k) {
+                const float s = warp_sum_f(acc[m]);
+                if (lane == 0) P[(int64_t)j * G + blockIdx.x] = s;
+            }
+        }
+    }
+    if (norm) {
+        const float t = arn_cta_sum(nrm);
+        if (threadIdx.x == 0) P[(int64_t)kMaxIter * G + blockIdx.x] = t;
+    }
+}
+
+// after a barrier: every CTA sums bank P in CTA order (dots -> out[0..k), norm -> *nout)
+__device__ __forceinline__ void arn_get_partials(const float *P, int k, bool dots, float *out, bool norm, float *nout)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, G = gridDim.x;
+    if (dots) {
+        for (int j = w; j < k; j += kArnWarps) {
+            float s = 0.0f;
+            for (int b = lane; b < G; b += 32) s += __ldcg(P + (int64_t)j * G + b);
+            s = warp_sum_f(s);
+            if (lane == 0) out[j] = s;
+        }
+    }
+    if (norm && w == kArnWarps - 1) {
+        float s = 0.0f;
+        for (int b = lane; b < G; b += 32) s += __ldcg(P + (int64_t)kMaxIter * G + b);
+        s = warp_sum_f(s);
+        if (lane == 0) *nout = s;
+    }
+    __syncthreads();
+}
+
+// v -= Q h over this CTA's rows; also its share of ||v||^2 and, with dots, of Q^T v
+__device__ __forceinline__ void arn_project(const ArnArgs &A, int k, float *v, const float *h, bool dots,
+                                            float (*sv)[kArnThreads], float *acc, float &nrm)
+{
+    for (int base = blockIdx.x * kArnThreads; base < A.nps; base += gridDim.x * kArnThreads) {
+        const int a = base + threadIdx.x;
+        float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
+        if (a < A.nps) {
+            v0 = v[a];
+            v1 = v[A.ld + a];
+            v2 = v[2 * A.ld + a];
+            const float *q = A.Q + a;
+#pragma unroll 4
+            for (int j = 0; j < k; j++, q += A.qld) {
+                const float hj = h[j];
+                v0 = __fmaf_rn(-hj, q[0], v0);
+                v1 = __fmaf_rn(-hj, q[A.ld], v1);
+                v2 = __fmaf_rn(-hj, q[2 * A.ld], v2);
+            }
+            v[a] = v0;
+            v[A.ld + a] = v1;
+            v[2 * A.ld + a] = v2;
+            nrm = __fmaf_rn(v0, v0, __fmaf_rn(v1, v1, __fmaf_rn(v2, v2, nrm)));
+        }
+        if (dots) {   // CTA-uniform
+            sv[0][threadIdx.x] = v0;
+            sv[1][threadIdx.x] = v1;
+            sv[2][threadIdx.x] = v2;
+            __syncthreads();
+            arn_tile_dots(A, k, base, sv, acc);
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kArnThreads, kArnCtasPerSm) k_arn_solve(ArnArgs A, const float *w1, float *b0,
+                                                                          float *b1)
+{
+    __shared__ float sv[3][kArnThreads];
+    __shared__ float sh1[kMaxIter], sh2[kMaxIter];
+    __shared__ float s_nv2, s_nn2;
+    __shared__ double cs[kMaxIter], sn[kMaxIter], g[kM1];
+    __shared__ int s_done, s_reorth;
+    ArnState *S = A.st;
+    const double norm_b = S->norm_b, stop_abs = S->stop_abs;
+    if (threadIdx.x == 0) {
+        g[0] = S->norm_rhs;
+        s_done = 0;
+    }
+    float snorm = (float)S->norm_rhs;   // norm of the vector the next iteration normalises
+    double maxerr = kMaxErr, res = 0.0;
+    int phase = 0, k = 0, conv = 0;
+    __syncthreads();
+    for (k = 1; k <= kMaxIter; k++) {
+        const float *w = k == 1 ? w1 : (((k - 1) & 1) ? b1 : b0);
+        float *v = (k & 1) ? b1 : b0;
+        float acc[kArnSlots];
+#pragma unroll
+        for (int m = 0; m < kArnSlots; m++) acc[m] = 0.0f;
+        float nrm = 0.0f;
+        // ---- phase 1: q_k = w / s, v = N q_k, h1 = Q^T v, ||v||^2 ----
+        {
+            const float inv = 1.0f / snorm;
+            float *qk = A.Q + (int64_t)(k - 1) * A.qld;
+            for (int base = blockIdx.x * kArnThreads; base < A.nps; base += gridDim.x * kArnThreads) {
+                const int a = base + threadIdx.x;
+                float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
+                if (a < A.nps) {
+                    float r0 = 0.0f, r1 = 0.0f, r2 = 0.0f;
+                    const int e1 = A.start[a + 1];
+                    for (int e = A.start[a]; e < e1; e++) {
+                        const int p = A.partner[e];
+                        if (p < 0) continue;
+                        const float x1 = __ldcg(w + p), x2 = __ldcg(w + A.ld + p), x3 = __ldcg(w + 2 * A.ld + p);
+                        const float *n = A.coef + (int64_t)e * 6;
+                        r0 = __fmaf_rn(n[0], x1, __fmaf_rn(n[1], x2, __fmaf_rn(n[2], x3, r0)));
+                        r1 = __fmaf_rn(n[1], x1, __fmaf_rn(n[3], x2, __fmaf_rn(n[4], x3, r1)));
+                        r2 = __fmaf_rn(n[2], x1, __fmaf_rn(n[4], x2, __fmaf_rn(n[5], x3, r2)));
+                    }
+                    const float w0 = __ldcg(w + a), wy = __ldcg(w + A.ld + a), wz = __ldcg(w + 2 * A.ld + a);
+                    v0 = r0 * inv;
+                    v1 = r1 * inv;
+                    v2 = r2 * inv;
+                    qk[a] = w0 * inv;
+                    qk[A.ld + a] = wy * inv;
+                    qk[2 * A.ld + a] = wz * inv;
+                    v[a] = v0;
+                    v[A.ld + a] = v1;
+                    v[2 * A.ld + a] = v2;
+                    nrm = __fmaf_rn(v0, v0, __fmaf_rn(v1, v1, __fmaf_rn(v2, v2, nrm)));
+                }
+                sv[0][threadIdx.x] = v0;
+                sv[1][threadIdx.x] = v1;
+                sv[2][threadIdx.x] = v2;
+                __syncthreads();
+                arn_tile_dots(A, k, base, sv, acc);
+                __syncthreads();
+            }
+        }
+        float *P = (phase++ & 1) ? A.part2 : A.part;
+        arn_put_partials(P, k, acc, true, nrm, true);
+        if (!arn_grid_sync(A.sync)) return;
+        arn_get_partials(P, k, true, sh1, true, &s_nv2);
+        if (threadIdx.x == 0) {
+            double hh = 0.0;
+            for (int j = 0; j < k; j++) hh += (double)sh1[j] * (double)sh1[j];
+            s_reorth = ((double)s_nv2 - hh) < 0.5 * (double)s_nv2;
+        }
+        __syncthreads();
+        const bool again = s_reorth != 0;
+        // ---- phase 2: v -= Q h1, then h2 = Q^T v (second projection) or ||v||^2 ----
+#pragma unroll
+        for (int m = 0; m < kArnSlots; m++) acc[m] = 0.0f;
+        nrm = 0.0f;
+        arn_project(A, k, v, sh1, again, sv, acc, nrm);
+        P = (phase++ & 1) ? A.part2 : A.part;
+        arn_put_partials(P, k, acc, again, nrm, !again);
+        if (!arn_grid_sync(A.sync)) return;
+        arn_get_partials(P, k, again, sh2, !again, &s_nn2);
+        if (again) {
+            // ---- phase 3: v -= Q h2, ||v||^2 ----
+            nrm = 0.0f;
+            arn_project(A, k, v, sh2, false, sv, acc, nrm);
+            P = (phase++ & 1) ? A.part2 : A.part;
+            arn_put_partials(P, k, acc, false, nrm, true);
+            if (!arn_grid_sync(A.sync)) return;
+            arn_get_partials(P, k, false, nullptr, true, &s_nn2);
+        }
+        // ---- Hessenberg column, Givens update, residual estimate (every CTA) ----
+        if (threadIdx.x == 0) {
+            double hc[kM1];
+            for (int i = 0; i < k; i++)
+                hc[i] = (double)sh1[i] + (again ? (double)sh2[i] : 0.0) + (i == k - 1 ? 1.0 : 0.0);
+            const double hn = sqrt((double)s_nn2);
+            hc[k] = hn;
+            for (int i = 0; i < k - 1; i++) {
+                const double t = cs[i] * hc[i] + sn[i] * hc[i + 1];
+                hc[i + 1] = -sn[i] * hc[i] + cs[i] * hc[i + 1];
+                hc[i] = t;
+            }
+            const double d = sqrt(hc[k - 1] * hc[k - 1] + hc[k] * hc[k]);
+            cs[k - 1] = hc[k - 1] / d;
+            sn[k - 1] = hc[k] / d;
+            hc[k - 1] = d;
+            g[k] = -sn[k - 1] * g[k - 1];
+            g[k - 1] = cs[k - 1] * g[k - 1];
+            if (blockIdx.x == 0)
+                for (int i = 0; i < k; i++) S->RN[(k - 1) * kM1 + i] = hc[i];
+            const double rabs = fabs(g[k]);
+            res = rabs / norm_b;
+            if (res < maxerr || (stop_abs > 0.0 && rabs < stop_abs)) {
+                conv = 1;
+                s_done = 1;
+            } else {
+                if (k == kMaxIter / 2) maxerr = maxerr * 10;
+                if (k >= kMaxIter - 2) maxerr = maxerr * 10;
+                if (k >= kMaxIter) s_done = 1;
+            }
+            s_nv2 = (float)hn;   // the next normalisation
+        }
+        __syncthreads();
+        snorm = s_nv2;
+        if (s_done) break;
+    }
+    if (k > kMaxIter) k = kMaxIter;
+    // ---- CTA 0: y from the triangular factor, the state for the x update ----
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double y[kMaxIter];
+        for (int i = k - 1; i >= 0; i--) {
+            double t = g[i];
+            for (int j = i + 1; j < k; j++) t = t - S->RN[j * kM1 + i] * y[j];
+            y[i] = t / S->RN[i * kM1 + i];
+        }
+        for (int i = 0; i < k; i++) S->y[i] = y[i];
+        S->iters = k;
+        S->res = res;
+        S->maxerr = maxerr;
+        S->converged = conv;
+        S->done = 1;
+    }
+}
+
 // x += d: r on the uncoupled rows (the first blocks, one thread per droplet), Q y on the
 // coupled rows when solved (the remaining blocks, one thread per coupled row)
 __global__ void k_red_xupdate(int nps, int nc, const int *pos, const int *list, const ArnState *st, int solved,
@@ -1009,8 +1285,9 @@ int grow(dl_ctx *c, void **p, size_t bytes, size_t *have)
     return 0;
 }
 
-// Layout of c->arn: the least-squares state, then [kMaxIter + 1][grid] partial sums,
-// h1[kMaxIter], h2[kMaxIter], the norm slot and the ticket.
+// Layout of c->arn: the least-squares state, then two banks of [kMaxIter + 1][grid]
+// partial sums, h1[kMaxIter], h2[kMaxIter], the norm slot, the ticket and the grid
+// barrier words.
 int arn_grid(const dl_ctx *c, int nps)
 {
     return std::max(1, std::min((nps + kArnThreads - 1) / kArnThreads, c->num_sms * kArnCtasPerSm));
@@ -1019,7 +1296,7 @@ int arn_grid(const dl_ctx *c, int nps)
 size_t arn_bytes(const dl_ctx *c)
 {
     const size_t st = (sizeof(ArnState) + 255) / 256 * 256;
-    return st + sizeof(float) * ((size_t)(kMaxIter + 1) * c->num_sms * kArnCtasPerSm + 2 * kMaxIter + 4) + 16;
+    return st + sizeof(float) * (2 * (size_t)(kMaxIter + 1) * c->num_sms * kArnCtasPerSm + 2 * kMaxIter + 4) + 32;
 }
 
 ArnArgs arn_args(dl_ctx *c, int nc)
@@ -1037,10 +1314,12 @@ ArnArgs arn_args(dl_ctx *c, int nc)
     A.Q = tp<float>(c->kry);
     A.st = reinterpret_cast<ArnState *>(base);
     A.part = reinterpret_cast<float *>(base + st);
-    A.h1 = A.part + (size_t)(kMaxIter + 1) * gmax;
+    A.part2 = A.part + (size_t)(kMaxIter + 1) * gmax;
+    A.h1 = A.part2 + (size_t)(kMaxIter + 1) * gmax;
     A.h2 = A.h1 + kMaxIter;
     A.s = A.h2 + kMaxIter;
     A.ticket = reinterpret_cast<unsigned *>(A.s + 4);
+    A.sync = A.ticket + 4;
     return A;
 }
 
@@ -1371,12 +1650,38 @@ int arnoldi_f32(dl_ctx *c, int sweep, int nc, double norm_b, double nf, double s
 {
     const ArnArgs A = arn_args(c, nc);
     const int G = arn_grid(c, nc);
-    k_arn_init<<<8, 256, 0, c->stream>>>(A.st, norm_b, nf, stop_abs, A.s);
+    k_arn_init<<<8, 256, 0, c->stream>>>(A.st, norm_b, nf, stop_abs, A.s, A.sync);
     DL_CHECK_LAUNCH(c);
     float *buf[2] = {tp<float>(c->wv), tp<float>(c->xt)};
+    ArnStatus hs{};
+    // one cooperative launch when every CTA of the grid can be resident at once
+    if (c->arn_coop_ctas < 0) {
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_arn_solve, kArnThreads, 0) != cudaSuccess)
+            per_sm = 0;
+        int coop = 0;
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
+        c->arn_coop_ctas = coop ? per_sm * c->num_sms : 0;
+    }
+    const int Gc = std::min(G, kArnCoopCtasPerSm * c->num_sms);
+    if (Gc <= c->arn_coop_ctas) {
+        ArnArgs a = A;
+        const float *w1 = c->red_rhs;
+        float *b0 = buf[0], *b1 = buf[1];
+        void *args[] = {&a, &w1, &b0, &b1};
+        DL_CUDA(c, cudaLaunchCooperativeKernel((const void *)k_arn_solve, dim3(Gc), dim3(kArnThreads), args, 0,
+                                               c->stream));
+        DL_CHECK_LAUNCH(c);
+        unsigned sync_err = 0;
+        DL_CUDA(c, cudaMemcpyAsync(&hs, A.st, sizeof(hs), cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaMemcpyAsync(&sync_err, A.sync + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaStreamSynchronize(c->stream));
+        if (sync_err || !hs.done) return dl_fail(c, DL_E_CUDA, "HDI_GMRES: grid barrier of the FP32 solve timed out");
+        iters = hs.iters;
+        return 0;
+    }
     int &guess = c->arn_guess[std::min(sweep, 7)];
     int batch = guess > 0 ? guess : 4;
-    ArnStatus hs{};
     int k = 0;
     while (k < kMaxIter) {
         const int kend = std::min(kMaxIter, k + batch);
