@@ -1515,8 +1515,12 @@ extern "C" int dl_particle_step(dl_ctx *c, dl_coll_report *coll, dl_gmres_report
         if (r) return r;
     }
     cudaEventRecord(c->ev[1], c->stream);
-    r = launch_headlist(c, hdi ? c->sc.d_hdi : c->sc.d_coll);
-    if (r) return r;
+    {
+        // the previous step's OVERLAP_DET leaves this cell list when nothing moved since
+        const double dist = hdi ? c->sc.d_hdi : c->sc.d_coll;
+        if (!(c->hl_valid && c->hl_dist == dist)) r = launch_headlist(c, dist);
+        if (r) return r;
+    }
     cudaEventRecord(c->ev[2], c->stream);
     int warn = 0;
     if (hdi) {

@@ -1189,8 +1189,17 @@ int launch_overlap_sweep(dl_ctx *c, std::vector<int2> &hits)
 {
     const DevConst &D = c->dc;
     const double d_overl = 2.0 * D.radmax;
-    int r = launch_headlist(c, d_overl);
-    if (r) return r;
+    // The reference sweeps a cell list built for d_overl.  The cell list the next step's
+    // COLLISION_DET / NEI_LIST_PRECOMP needs (halo d_coll or d_hdi, both >= d_overl, same
+    // cells) gives the same overlaps: its extra halo droplets lie farther than d_overl
+    // from every owned droplet.  Built here, it stays valid for the next step unless a
+    // relocation moves droplets.
+    const double dist = D.hdi ? c->sc.d_hdi : c->sc.d_coll;
+    int r = 0;
+    if (!(c->hl_valid && c->hl_dist == dist && dist >= d_overl)) {
+        r = launch_headlist(c, dist >= d_overl ? dist : d_overl);
+        if (r) return r;
+    }
     const int jmax = 1 + (int)(d_overl * (double)D.ncd / D.hy);
     const int kmax = 1 + (int)(d_overl * (double)D.ncd / D.hz);
     DL_CUDA(c, cudaMemsetAsync(c->ovl_cnt, 0, sizeof(int), c->stream));
@@ -1206,8 +1215,6 @@ int launch_overlap_sweep(dl_ctx *c, std::vector<int2> &hits)
     if (n > c->ovl_cap) return dl_fail(c, DL_E_CAPACITY, "OVERLAP_DET: overlap list capacity exceeded");
     hits.resize(n);
     if (n) DL_CUDA(c, cudaMemcpy(hits.data(), c->ovl_list, sizeof(int2) * n, cudaMemcpyDeviceToHost));
-    // the sweep's cell list was built for d_overl; the collision cell list is stale now
-    c->hl_valid = 0;
     return 0;
 }
 
@@ -1241,6 +1248,7 @@ int launch_periodic_reorder(dl_ctx *c)
                                             c->lv_new, c->lv_dev, c->ref_of_dev, c->dev_of_ref, c->d_err,
                                             c->pert[0], c->pert[1], c->pert[2], pesz, c->pert_tmp, c->lv_src);
     DL_CHECK_LAUNCH(c);
+    c->hl_valid = 0;   // reference indices moved: the packed entries' keys are stale
     return 0;
 }
 
@@ -1254,6 +1262,7 @@ int dl_apply_remap(dl_ctx *c, const std::vector<int> &old_ref, const std::vector
     k_remap_read<<<dl_blocks(m, 256), 256, 0, c->stream>>>(m, c->lv_old, c->dev_of_ref, c->lv_dev);
     k_remap_write<<<dl_blocks(m, 256), 256, 0, c->stream>>>(m, c->lv_dev, c->lv_new, c->ref_of_dev, c->dev_of_ref);
     DL_CHECK_LAUNCH(c);
+    c->hl_valid = 0;
     return 0;
 }
 
@@ -1270,5 +1279,6 @@ int launch_set_positions(dl_ctx *c, const std::vector<int> &refs, const std::vec
                                                               c->pos[c->pcur][0], c->pos[c->pcur][1],
                                                               c->pos[c->pcur][2], clear_leave ? c->leave_nid : nullptr);
     DL_CHECK_LAUNCH(c);
+    c->hl_valid = 0;   // the cell list indexes the old positions
     return 0;
 }
