@@ -36,7 +36,7 @@ class Params(C.Structure):
         ("hdi_trunc", C.c_double),
         ("msize", C.c_int), ("ncollmax", C.c_int), ("nei_max", C.c_int), ("mevent", C.c_int),
         ("precision", C.c_int), ("init_velocity", C.c_int), ("resort_interval", C.c_int),
-        ("device", C.c_int),
+        ("device", C.c_int), ("gmres_launch", C.c_int),
     ]
 
 

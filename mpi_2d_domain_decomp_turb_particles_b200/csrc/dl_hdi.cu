@@ -1664,7 +1664,7 @@ int arnoldi_f32(dl_ctx *c, int sweep, int nc, double norm_b, double nf, double s
         c->arn_coop_ctas = coop ? per_sm * c->num_sms : 0;
     }
     const int Gc = std::min(G, kArnCoopCtasPerSm * c->num_sms);
-    if (Gc <= c->arn_coop_ctas) {
+    if (c->p.gmres_launch == 0 && Gc <= c->arn_coop_ctas) {
         ArnArgs a = A;
         const float *w1 = c->red_rhs;
         float *b0 = buf[0], *b1 = buf[1];

@@ -50,6 +50,7 @@ class ParticleParams:
     precision: str = "fp64"          # "fp64" or "mixed"
     init_velocity: int = 0           # 0 terminal (reference), 1 fluid velocity, 2 fluid + terminal
     resort_interval: int = 0
+    gmres_launch: int = 0
     device: int = 0
 
     def to_c(self) -> Params:
@@ -63,7 +64,7 @@ class ParticleParams:
                   "ediss_cloud", "viscosity_cloud", "gravity", "hdi_trunc"):
             setattr(p, k, float(getattr(self, k)))
         for k in ("new_particle", "nonoverlap", "hdi_included", "ndrag", "msize", "ncollmax",
-                  "nei_max", "mevent", "init_velocity", "resort_interval", "device"):
+                  "nei_max", "mevent", "init_velocity", "resort_interval", "device", "gmres_launch"):
             setattr(p, k, int(getattr(self, k)))
         p.precision = _lib.DL_MIXED if self.precision == "mixed" else _lib.DL_FP64
         return p

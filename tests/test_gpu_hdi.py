@@ -110,6 +110,26 @@ def test_gmres_mixed_refined_to_fp64_tolerance():
     assert np.linalg.norm(pg - po) <= 1e-5 * np.linalg.norm(po)
 
 
+def test_gmres_mixed_launch_modes_agree():
+    """The FP32 solve as one cooperative launch (default) and as launches per iteration
+    reach the same FP64-refined pertvel (both within the refinement tolerance of the
+    oracle's FP64 GMRES)."""
+    f = smooth_field(32)
+    out = []
+    for mode in (0, 1):
+        g, o = make_settled(hdi_params("mixed", gmres_launch=mode), f)
+        through_nei(g, o, f)
+        rep = g.hdi_gmres()
+        o.hdi_gmres()
+        assert rep.refinements >= 2 and rep.residual < 1e-6
+        po = o.arr("pertvel")[:3 * o.nps].reshape(-1, 3)
+        pg = g.get_pertvel()
+        assert np.linalg.norm(pg - po) <= 1e-5 * np.linalg.norm(po)
+        out.append(pg)
+        g.close()
+    assert np.linalg.norm(out[0] - out[1]) <= 1e-5 * np.linalg.norm(out[0])
+
+
 def test_hdi_particle_steps_fp64_track_oracle():
     f = smooth_field(32)
     g, o = make_settled(hdi_params("fp64"), f)
