@@ -137,7 +137,25 @@ struct UpdArgs {
     const double2 *nh;    // transform of u x omega [3][M], not normalised
     double nu, dt, inv_n3;
     const double *afor;   // stochastic forcing a1r..a3r (3 x 5 x 5 x 6) or null
+    double2 *work;        // with emit: the next step's transform inputs (curl u, u)
+    int emit;             // finish the modes kx > 2 here (k_finish_low does kx <= 2)
 };
+
+__device__ __forceinline__ void emit_mode(const Grid &G, int64_t m, double kx, double ky, double kz,
+                                          const double2 *v, double2 *u, double2 *work)
+{
+    for (int c = 0; c < 3; c++) {
+        u[c * G.M + m] = v[c];
+        work[(3 + c) * G.M + m] = v[c];
+    }
+    // curl: w = k x u, multiplied by i: (re, im) -> (-im, re)
+    const double2 w[3] = {make_double2(ky * v[2].x - kz * v[1].x, ky * v[2].y - kz * v[1].y),
+                          make_double2(kz * v[0].x - kx * v[2].x, kz * v[0].y - kx * v[2].y),
+                          make_double2(kx * v[1].x - ky * v[0].x, kx * v[1].y - ky * v[0].y)};
+    for (int c = 0; c < 3; c++) work[c * G.M + m] = make_double2(-w[c].y, w[c].x);
+}
+
+
 
 // dealias N, u <- u (1 - nu dt/2 k^2) + 1.5 dt N - dt/2 N_old (+ dt a), projection,
 // u <- u / (1 + nu dt/2 k^2), N_old <- N   (turb.f90:648-676)
@@ -188,12 +206,22 @@ __global__ void k_update(UpdArgs A)
     const double ti = (kx * v[0].y + ky * v[1].y + kz * v[2].y) * ik2;
     const double kk[3] = {kx, ky, kz};
     const double iden = 1.0 / (1.0 + A.nu * dth * k2);
+    double2 w[3];
     for (int c = 0; c < 3; c++) {
-        double2 w;
-        w.x = (v[c].x - kk[c] * tr) * iden;
-        w.y = (v[c].y - kk[c] * ti) * iden;
-        A.u[c * A.G.M + m] = w;
+        w[c].x = (v[c].x - kk[c] * tr) * iden;
+        w[c].y = (v[c].y - kk[c] * ti) * iden;
     }
+    if (A.emit && x > 2) {
+        // what k_finish does for this mode: Nyquist planes and aliased modes zeroed, then
+        // u and the next transforms' inputs written (kx > 2: no conjugate pair, and the
+        // deterministic forcing touches kx <= 2 only)
+        const int h = A.G.n / 2;
+        if (x == h || y == h || z == h || alias)
+            for (int c = 0; c < 3; c++) w[c] = make_double2(0.0, 0.0);
+        emit_mode(A.G, m, kx, ky, kz, w, A.u, A.work);
+        return;
+    }
+    for (int c = 0; c < 3; c++) A.u[c * A.G.M + m] = w[c];
 }
 
 // supforDET (flowlib.f90:195-229): shells 1 and 2 rescaled to the energies force(1:2);
@@ -237,24 +265,8 @@ __global__ void k_force_det(Grid G, double2 *u, double f1, double f2)
 
 // symmetrize (flowlib.f90:233-334) + dealiasing (180-191) of u^, then the inputs of the
 // next inverse transforms: work = [i k x u^ (3), u^ (3)]  (turb.f90:506-521)
-__device__ __forceinline__ void emit_mode(const Grid &G, int64_t m, double kx, double ky, double kz,
-                                          const double2 *v, double2 *u, double2 *work)
+__device__ __forceinline__ void finish_mode(const Grid &G, int64_t m, double2 *u, double2 *work)
 {
-    for (int c = 0; c < 3; c++) {
-        u[c * G.M + m] = v[c];
-        work[(3 + c) * G.M + m] = v[c];
-    }
-    // curl: w = k x u, multiplied by i: (re, im) -> (-im, re)
-    const double2 w[3] = {make_double2(ky * v[2].x - kz * v[1].x, ky * v[2].y - kz * v[1].y),
-                          make_double2(kz * v[0].x - kx * v[2].x, kz * v[0].y - kx * v[2].y),
-                          make_double2(kx * v[1].x - ky * v[0].x, kx * v[1].y - ky * v[0].y)};
-    for (int c = 0; c < 3; c++) work[c * G.M + m] = make_double2(-w[c].y, w[c].x);
-}
-
-__global__ void k_finish(Grid G, double2 *u, double2 *work)
-{
-    const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= G.M) return;
     int x, y, z;
     double kx, ky, kz;
     mode_of(G, m, x, y, z, kx, ky, kz);
@@ -284,6 +296,21 @@ __global__ void k_finish(Grid G, double2 *u, double2 *work)
     }
     emit_mode(G, m, kx, ky, kz, v, u, work);
     emit_mode(G, mp, kx, -ky, -kz, vp, u, work);
+}
+
+__global__ void k_finish(Grid G, double2 *u, double2 *work)
+{
+    const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < G.M) finish_mode(G, m, u, work);
+}
+
+// k_finish on the planes kx = 0, 1, 2 only (after k_update finished the others)
+__global__ void k_finish_low(Grid G, double2 *u, double2 *work)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * (int64_t)G.n * G.n) return;
+    const int64_t zy = t / 3;
+    finish_mode(G, zy * G.nh + (t - 3 * zy), u, work);
 }
 
 // energy per shell ik2 (kx = 0 modes count half): partial sums per CTA, in order
@@ -715,6 +742,8 @@ extern "C" int dl_flow_step(dl_flow *f, dl_ctx *droplets)
     A.dt = f->p.dt;
     A.inv_n3 = 1.0 / (double)n3;
     A.afor = nullptr;
+    A.work = f->work;
+    A.emit = 1;
     if (f->p.forcing == 2) {
         double a[450];
         stochastic_amplitudes(f, a);
@@ -727,9 +756,9 @@ extern "C" int dl_flow_step(dl_flow *f, dl_ctx *droplets)
         k_force_det<<<1, 96, 0, f->stream>>>(f->G, f->u, f->p.force[0], f->p.force[1]);
         FCUDA(f, cudaGetLastError());
     }
-    const int r = finish(f);
-    if (r) return r;
-    f->launches += 4;
+    k_finish_low<<<blocks(3 * (int64_t)n * n, 256), 256, 0, f->stream>>>(f->G, f->u, f->work);
+    FCUDA(f, cudaGetLastError());
+    f->launches += 5;
     f->steps++;
     return 0;
 }
