@@ -1072,6 +1072,9 @@ int dl_check_device_errors(dl_ctx *c)
     DL_CUDA(c, cudaMemcpyAsync(&e, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     DL_CUDA(c, cudaStreamSynchronize(c->stream));
     if (e & DL_DERR_REORDER) return dl_fail(c, DL_E_STATE, "PERIODIC: reorder bookkeeping mismatch");
+    if (e & DL_DERR_TMA_TIMEOUT) return dl_fail(c, DL_E_CUDA, "INTERPOLATE: a field tile wait timed out");
+    if (e & DL_DERR_LONG_ROW)
+        return dl_fail(c, DL_E_CAPACITY, "HEADLIST: more than 4096 droplets in one row of cells");
     return 0;
 }
 

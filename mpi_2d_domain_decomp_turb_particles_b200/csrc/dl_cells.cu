@@ -212,39 +212,42 @@ __global__ void k_row_sort(int nrows, const int *row_start, long long *row_ent, 
     if (lane + 32 < len) row_ent[s + r1] = v1;
 }
 
-// One CTA per long row: bitonic sort in shared memory (length padded to a power of two).
+// The long rows, one per CTA of a fixed grid (the count stays on the device): bitonic sort
+// in shared memory (length padded to a power of two).  A row longer than kLongRowMax
+// raises DL_DERR_LONG_ROW and stays unsorted.
+constexpr int kLongRowGrid = 64;
+
 __global__ void __launch_bounds__(1024) k_row_sort_long(const int *long_rows, const int *n_long,
-                                                        const int *row_start, long long *row_ent)
+                                                        const int *row_start, long long *row_ent, int *err)
 {
     __shared__ long long sk[kLongRowMax];
-    if ((int)blockIdx.x >= *n_long) return;
-    const int r = long_rows[blockIdx.x];
-    const int s = row_start[r], len = row_start[r + 1] - s;
-    if (len > kLongRowMax) return;   // rejected on the host before launch
-    int np2 = 1;
-    while (np2 < len) np2 <<= 1;
-    for (int i = threadIdx.x; i < np2; i += blockDim.x) sk[i] = i < len ? row_ent[s + i] : LLONG_MAX;
-    __syncthreads();
-    for (int k = 2; k <= np2; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < np2; i += blockDim.x) {
-                int ixj = i ^ j;
-                if (ixj > i) {
-                    bool up = (i & k) == 0;
-                    long long a = sk[i], b = sk[ixj];
-                    if ((a > b) == up) { sk[i] = b; sk[ixj] = a; }
-                }
-            }
-            __syncthreads();
+    for (int q = blockIdx.x; q < *n_long; q += gridDim.x) {
+        const int r = long_rows[q];
+        const int s = row_start[r], len = row_start[r + 1] - s;
+        if (len > kLongRowMax) {
+            if (threadIdx.x == 0) atomicOr(err, DL_DERR_LONG_ROW);
+            continue;
         }
+        int np2 = 1;
+        while (np2 < len) np2 <<= 1;
+        for (int i = threadIdx.x; i < np2; i += blockDim.x) sk[i] = i < len ? row_ent[s + i] : LLONG_MAX;
+        __syncthreads();
+        for (int k = 2; k <= np2; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+                    int ixj = i ^ j;
+                    if (ixj > i) {
+                        bool up = (i & k) == 0;
+                        long long a = sk[i], b = sk[ixj];
+                        if ((a > b) == up) { sk[i] = b; sk[ixj] = a; }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (int i = threadIdx.x; i < len; i += blockDim.x) row_ent[s + i] = sk[i];
+        __syncthreads();   // sk is reused by the next row
     }
-    for (int i = threadIdx.x; i < len; i += blockDim.x) row_ent[s + i] = sk[i];
-}
-
-__global__ void k_max_row(int nrows, const int *row_start, int *mx)
-{
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r < nrows) atomicMax(mx, row_start[r + 1] - row_start[r]);
 }
 
 // first index in [s, e) whose ix >= key
@@ -990,23 +993,11 @@ int launch_headlist(dl_ctx *c, double dist)
         k_row_sort<<<(int)(((int64_t)c->nrows * 32 + t - 1) / t), t, 0, c->stream>>>(
             c->nrows, c->row_start, (long long *)c->row_ent, c->long_rows, c->n_long);
         DL_CHECK_LAUNCH(c);
-        int nl = 0;
-        DL_CUDA(c, cudaMemcpyAsync(&nl, c->n_long, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-        DL_CUDA(c, cudaStreamSynchronize(c->stream));
-        if (nl > 0) {
-            // crowded rows: every one must fit a CTA's shared-memory sort
-            DL_CUDA(c, cudaMemsetAsync(c->d_nghost, 0, sizeof(int), c->stream));
-            k_max_row<<<dl_blocks(c->nrows, t), t, 0, c->stream>>>(c->nrows, c->row_start, c->d_nghost);
-            DL_CHECK_LAUNCH(c);
-            int mx = 0;
-            DL_CUDA(c, cudaMemcpyAsync(&mx, c->d_nghost, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-            DL_CUDA(c, cudaStreamSynchronize(c->stream));
-            if (mx > kLongRowMax)
-                return dl_fail(c, DL_E_CAPACITY, "HEADLIST: more than 4096 droplets in one row of cells");
-            k_row_sort_long<<<nl, 1024, 0, c->stream>>>(c->long_rows, c->n_long, c->row_start,
-                                                        (long long *)c->row_ent);
-            DL_CHECK_LAUNCH(c);
-        }
+        // crowded rows (none for uniformly spread droplets): a fixed grid reads their count
+        // on the device; an over-long row is reported through the device error flags
+        k_row_sort_long<<<kLongRowGrid, 1024, 0, c->stream>>>(c->long_rows, c->n_long, c->row_start,
+                                                              (long long *)c->row_ent, c->d_err);
+        DL_CHECK_LAUNCH(c);
     }
     // bucketed cell starts (the searches of COLLISION_DET, OVERLAP_DET and the HDI walk):
     // buckets of about half an entry on average, at most 32 cells
@@ -1106,10 +1097,15 @@ static int collision_t(dl_ctx *c, dl_coll_report *rep)
     char *hs = static_cast<char *>(dl_host_stage(c, sizeof(int) * ncount + 16));
     if (!hs) return dl_fail(c, DL_E_ALLOC, "cudaHostAlloc of the staging buffer failed");
     DL_CUDA(c, cudaMemcpyAsync(hs, c->cand, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    DL_CUDA(c, cudaMemcpyAsync(hs + 8, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     DL_CUDA(c, cudaMemcpyAsync(hs + 16, c->counts, sizeof(int) * ncount, cudaMemcpyDeviceToHost, c->stream));
     DL_CUDA(c, cudaStreamSynchronize(c->stream));
     unsigned long long cand;
     memcpy(&cand, hs, sizeof(cand));
+    int derr;
+    memcpy(&derr, hs + 8, sizeof(int));
+    if (derr & DL_DERR_LONG_ROW)   // the cell list this search read was not fully sorted
+        return dl_fail(c, DL_E_CAPACITY, "HEADLIST: more than 4096 droplets in one row of cells");
     std::vector<int> cnt(ncount);
     memcpy(cnt.data(), hs + 16, sizeof(int) * ncount);
     if (cnt[6]) return dl_fail(c, DL_E_CAPACITY, "COLLISION_DET: pair, contact or removal buffer full");

@@ -302,6 +302,8 @@ int launch_set_positions(dl_ctx *c, const std::vector<int> &refs, const std::vec
 int launch_periodic_reorder(dl_ctx *c);
 int dl_check_device_errors(dl_ctx *c);
 #define DL_DERR_REORDER 1        // PERIODIC bookkeeping mismatch
+#define DL_DERR_TMA_TIMEOUT 2    // an interpolation tile wait ran out (the tiles' droplets were skipped)
+#define DL_DERR_LONG_ROW 4       // a cell-list row longer than the shared-memory sort holds
 // dl_hdi.cu
 int launch_nei_list(dl_ctx *c);
 int run_gmres(dl_ctx *c, dl_gmres_report *rep);

@@ -359,7 +359,6 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
-#define DL_DERR_TMA_TIMEOUT 2
 
 // ---------------------------------------------------------------------------------------
 // The brick kernel: persistent, warp-specialised.  The last warp is the producer: it

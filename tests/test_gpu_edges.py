@@ -101,3 +101,51 @@ def test_hdi_neighbour_capacity_is_an_error():
     with pytest.raises(DropletError, match="NEI_CAPACITY"):
         g.particle_step()
     g.close()
+
+
+def _crowd_row(yp, idx, n, cell=0):
+    """Moves droplets idx into the cell row iy = iz = cell + 1 (y, z inside that cell), x spread."""
+    h = 2 * np.pi / n
+    rng = np.random.default_rng(5)
+    yp[idx, 1] = (cell + rng.uniform(0.1, 0.9, len(idx))) * h
+    yp[idx, 2] = (cell + rng.uniform(0.1, 0.9, len(idx))) * h
+    return yp
+
+
+def test_crowded_cell_row_matches_oracle():
+    """A row of cells holding a few hundred droplets goes through the shared-memory sort
+    of long rows; pairs and positions still follow the oracle."""
+    n = 32
+    f = smooth_field(n)
+    p = dense_params(n=n, npart=2000, ncollmax=100000)
+    g = Partlib(p)
+    g.part_init()
+    o = orc.Oracle(**p.oracle_kwargs())
+    o.part_init()
+    yp = _crowd_row(o.yp[:o.nps].copy(), np.arange(300), n)
+    o.yp[:o.nps] = yp
+    g.set_particles(yp)
+    g.set_fields(*f)
+    for _ in range(3):
+        g.particle_step()
+        o.particle_step(*f)
+        gp = sorted(map(tuple, g.pairs().tolist()))
+        op = sorted((int(r[0]), int(r[2]), int(r[3]), int(r[4])) for r in o.pairs())
+        assert gp == op
+    assert g.nps == o.nps
+    assert np.array_equal(g.get_particles()["yp"], o.yp[:o.nps])
+
+
+def test_overfull_cell_row_is_an_error():
+    """More than 4096 droplets in one row of cells (in the middle of the box, away from
+    the halo): HEADLIST's capacity error (the reference has no check)."""
+    n = 32
+    p = dense_params(n=n, npart=6000, ncollmax=100000)
+    g = Partlib(p)
+    g.part_init()
+    g.set_fields(*smooth_field(n))
+    yp = _crowd_row(g.get_particles()["yp"], np.arange(5000), n, cell=n // 2)   # no halo images
+    g.set_particles(yp)
+    with pytest.raises(DropletError, match="one row of cells"):
+        g.particle_step()
+    g.close()
