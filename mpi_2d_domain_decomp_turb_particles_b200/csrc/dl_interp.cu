@@ -698,6 +698,28 @@ __global__ void k_brick_scatter(int nps, const int *keys, const int *start, int 
     perm[start[k] + base + __popc(peers & ((1u << lane) - 1u))] = d;
 }
 
+// The scatter's order inside a brick follows the atomics' timing; this restores the
+// previous device order inside every brick (one warp per brick ranks its droplets by
+// their old index), so the device order, and every sum taken in it, is reproducible.
+// Bricks of more than kOrderMax droplets keep the scatter's order.
+constexpr int kOrderMax = 2048;
+
+__global__ void k_brick_order(int nseg, const int *start, const int *perm, int *out)
+{
+    const int w = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (w >= nseg) return;
+    const int s = start[w], len = start[w + 1] - s;
+    for (int i = lane; i < len; i += 32) {
+        const int v = perm[s + i];
+        int r = i;
+        if (len <= kOrderMax) {
+            r = 0;
+            for (int j = 0; j < len; j++) r += perm[s + j] < v;
+        }
+        out[s + r] = v;
+    }
+}
+
 template <typename E>
 __global__ void k_gather(int nps, const int *perm, const E *in, E *out)
 {
@@ -920,6 +942,11 @@ int launch_brick_sort(dl_ctx *c)
     DL_CUDA(c, cudaMemsetAsync(c->brick_cnt, 0, sizeof(int) * nkeys, c->stream));
     k_brick_scatter<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, c->keys, c->brick_start, c->brick_cnt, c->perm);
     DL_CHECK_LAUNCH(c);
+    // the keys are spent: the ordered permutation goes there
+    k_brick_order<<<(int)(((int64_t)nkeys * 32 + t - 1) / t), t, 0, c->stream>>>(nkeys, c->brick_start, c->perm,
+                                                                                 c->keys);
+    DL_CHECK_LAUNCH(c);
+    int *perm = c->keys;
     // permute every live array in two passes: gather all of them into the scratch region,
     // then copy back (coalesced); one index load per droplet for ~30 arrays
     PermTable tb;
@@ -941,7 +968,7 @@ int launch_brick_sort(dl_ctx *c)
     tb.s8 = (unsigned long long *)c->perm_scratch;
     tb.s4 = (unsigned int *)((unsigned long long *)c->perm_scratch + (size_t)tb.n8 * c->msize);
     tb.m = c->msize;
-    k_permute_gather<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, c->perm, tb);
+    k_permute_gather<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, perm, tb);
     DL_CHECK_LAUNCH(c);
     k_permute_copyback<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, tb);
     DL_CHECK_LAUNCH(c);
