@@ -167,8 +167,10 @@ __device__ __forceinline__ int cell_above(double v, double r, double h)
 // hdi_trunc * radmax of the owner are read: every entry (distance below hdi_trunc times
 // a radius) and every overlap (below the sum of two radii) lies there, and the entries
 // keep the keys of the full box.  The reach uses the largest radius of the current
-// droplets (coalescence can grow droplets past the largest initial radius).
-__global__ void __launch_bounds__(128) k_nei_walk(NeiArgs A)
+// droplets (coalescence can grow droplets past the largest initial radius).  The walk is
+// bound by memory latency: 64 registers and 8 CTAs per SM (a few bytes spilled) hide it
+// better than 80 registers and 6 CTAs.
+__global__ void __launch_bounds__(128, 8) k_nei_walk(NeiArgs A)
 {
     const int sa = blockIdx.x * blockDim.x + threadIdx.x;
     if (sa >= A.ne) return;
