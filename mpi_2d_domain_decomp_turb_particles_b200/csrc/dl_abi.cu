@@ -510,7 +510,7 @@ extern "C" int dl_destroy(dl_ctx *c)
     F(c->counts); F(c->cand); F(c->pairs); F(c->contacts); F(c->remove_dev); F(c->pair_buf); F(c->pair_ibuf); F(c->mv_acc);
     F(c->ovl_list); F(c->ovl_cnt); F(c->fpad_own);
     F(c->nei_cnt); F(c->nei_start); F(c->nei_idx); F(c->nei_coef); F(c->nei_coef64); F(c->overlap_flag);
-    F(c->kry); F(c->xg); F(c->rg); F(c->bg64); F(c->tmp64); F(c->wv); F(c->xt); F(c->dots); F(c->arn); F(c->co_buf); F(c->scan_buf);
+    F(c->kry); F(c->xg); F(c->rg); F(c->bg64); F(c->tmp64); F(c->wv); F(c->xt); F(c->dots); F(c->arn); F(c->co_buf); F(c->scan_buf); F(c->rmax_dev);
     if (c->hpin) cudaFreeHost(c->hpin);
     if (c->hstage) cudaFreeHost(c->hstage);
     F(c->red_pos); F(c->red_list); F(c->red_start); F(c->red_partner); F(c->red_rhs);

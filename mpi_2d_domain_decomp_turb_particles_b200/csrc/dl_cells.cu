@@ -571,9 +571,11 @@ __global__ void k_accumulate(int nbinsz, const int *hi, const double *hd, int *a
 
 // OVERLAP_DET sweep (partlib.f90:2069-2156): per owned droplet, number of partners
 // (ypn index > ih1, 27 neighbour cells, half shell) within rcoll.  One thread per sorted
-// entry that is an owned droplet, streaming the packed entries.
+// entry that is an owned droplet, streaming the packed entries.  Of the 27 cells only
+// those within twice the largest current radius of the droplet are read (an overlap is
+// a distance below the sum of two radii): mostly its own cell.
 __global__ void k_overlap(DevConst D, int nps, int ne, const double4 *pk_x, const int4 *pk_id, const int *cell_start,
-                          int jmax, int kmax, int2 *hits, int cap, int *cnt)
+                          int jmax, int kmax, const double *rmax, int2 *hits, int cap, int *cnt)
 {
     const int sa = blockIdx.x * blockDim.x + threadIdx.x;
     if (sa >= ne) return;
@@ -585,28 +587,35 @@ __global__ void k_overlap(DevConst D, int nps, int ne, const double4 *pk_x, cons
     const int refa = ida.y;
     int ix, iy, iz;
     own_cell(D, xa[0], xa[1], xa[2], ix, iy, iz);
+    const double reach = 2.0 * *rmax;
+    const double cx = D.hx / D.ncd, cy = D.hy / D.ncd, cz = D.hz / D.ncd;
+    // the x cells ix - 1 .. ix + 1 (unwrapped) within reach
+    const int wlo = max(ix - 1, cell_below(xa[0], reach, cx)), whi = min(ix + 1, cell_above(xa[0], reach, cx));
+    const int jlo = max(-1, cell_below(xa[1], reach, cy) - iy), jhi = min(1, cell_above(xa[1], reach, cy) - iy);
+    const int klo = max(-1, cell_below(xa[2], reach, cz) - iz), khi = min(1, cell_above(xa[2], reach, cz) - iz);
     int nov = 0;
-    for (int jj = -1; jj <= 1; jj++) {
+    for (int jj = jlo; jj <= jhi; jj++) {
         int iy2 = iy + jj;
         if (iy2 < 1 - jmax || iy2 > D.ncd + jmax) continue;
-        for (int kk = -1; kk <= 1; kk++) {
+        for (int kk = klo; kk <= khi; kk++) {
             int iz2 = iz + kk;
             if (iz2 < 1 - kmax || iz2 > D.ncd + kmax) continue;
             if (iz2 < 1) continue;
             if (iz2 <= D.ncd && iy2 < 1) continue;
             const int row = row_of(D, iy2, iz2);
-            // x cells ix - 1 .. ix + 1: the part inside the box, then the wrapped cell
+            // the part inside the box, then the wrapped cell
 #pragma unroll 1
             for (int q = 0; q < 3; q++) {
                 int lo, hi;
                 double sx;
                 if (q == 0) {
-                    lo = max(1, ix - 1); hi = min(D.ncd, ix + 1); sx = 0.0;
+                    lo = max(1, wlo); hi = min(D.ncd, whi); sx = 0.0;
+                    if (lo > hi) continue;
                 } else if (q == 1) {
-                    if (ix - 1 >= 1) continue;
+                    if (wlo >= 1) continue;
                     lo = D.ncd; hi = D.ncd; sx = -1.0;
                 } else {
-                    if (ix + 1 <= D.ncd) continue;
+                    if (whi <= D.ncd) continue;
                     lo = 1; hi = 1; sx = 1.0;
                 }
                 int s0, s1;
@@ -1201,8 +1210,14 @@ int launch_overlap_sweep(dl_ctx *c, std::vector<int2> &hits)
     DL_CUDA(c, cudaMemsetAsync(c->ovl_cnt, 0, sizeof(int), c->stream));
     if (c->nps > 0) {
         const int ne = c->nps + c->nghost;
+        if (!c->rmax_dev && cudaMalloc(&c->rmax_dev, sizeof(double)) != cudaSuccess)
+            return dl_fail(c, DL_E_ALLOC, "OVERLAP_DET: cudaMalloc failed");
+        DL_CUDA(c, cudaMemsetAsync(c->rmax_dev, 0, sizeof(double), c->stream));
+        k_rad_max<<<std::min(dl_blocks(c->nps, 256), 4 * c->num_sms), 256, 0, c->stream>>>(
+            c->nps, c->rad, reinterpret_cast<unsigned long long *>(c->rmax_dev));
+        DL_CHECK_LAUNCH(c);
         k_overlap<<<dl_blocks(ne, 128), 128, 0, c->stream>>>(D, c->nps, ne, c->pk_x, c->pk_id, c->cell_start, jmax, kmax,
-                                                             c->ovl_list, c->ovl_cap, c->ovl_cnt);
+                                                             c->rmax_dev, c->ovl_list, c->ovl_cap, c->ovl_cnt);
         DL_CHECK_LAUNCH(c);
     }
     int n = 0;

@@ -127,15 +127,6 @@ __device__ __forceinline__ void nei_emit(const NeiArgs &A, int owner, int partne
     stokes_tensor(arad, dnij, xd, e.coef);
 }
 
-// largest radius (positive doubles order like their bit patterns)
-__global__ void k_rad_max(int n, const double *rad, unsigned long long *out)
-{
-    double m = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = fmax(m, rad[i]);
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
-}
-
 // appended entries -> CSR slots of their owners (order fixed afterwards by k_nei_sort)
 __global__ void k_nei_scatter(int nnz, const NeiApp *app, const int *start, int *fill, int *partner,
                               unsigned long long *key, double *coef)
@@ -147,18 +138,6 @@ __global__ void k_nei_scatter(int nnz, const NeiApp *app, const int *start, int 
     partner[slot] = e.partner;
     key[slot] = e.key;
     for (int t = 0; t < 6; t++) coef[(int64_t)slot * 6 + t] = e.coef[t];
-}
-
-// Cells of the search box that can hold a droplet within distance r of coordinate v
-// (cell index 1 + floor(v / h) as HEADLIST assigns it, widened by a millionth of a cell
-// against rounding at the faces).
-__device__ __forceinline__ int cell_below(double v, double r, double h)
-{
-    return (int)floor((v - r) / h - 1.0e-6) + 1;
-}
-__device__ __forceinline__ int cell_above(double v, double r, double h)
-{
-    return (int)floor((v + r) / h + 1.0e-6) + 1;
 }
 
 // One thread per sorted entry that is an owned droplet: consecutive threads own

@@ -217,6 +217,7 @@ struct dl_ctx {
     void *arn;                   // fused FP32 Arnoldi: least-squares state, partial dots, scalars
     int arn_guess[8];            // iterations of the previous FP32 solve of each refinement sweep
     int arn_coop_ctas;           // CTAs of the cooperative FP32 solve that fit at once (-1: not yet asked)
+    double *rmax_dev;            // largest droplet radius (OVERLAP_DET reach)
     void *hpin;                  // 256 bytes of pinned host memory for small device->host reads
     void *hstage;                // pinned staging of a step's variable-size reads (grown on demand)
     size_t hstage_cap;
@@ -270,6 +271,29 @@ __device__ __forceinline__ void cell_range(const int *cs, const DevConst &D, int
     s0 = c[(lo - 1) >> D.cs_shift];
     s1 = c[min(D.cs_nb, ((hi - 1) >> D.cs_shift) + 1)];
 }
+// Cells of a search that can hold a point within distance r of coordinate v (cell index
+// 1 + floor(v / h) as HEADLIST assigns it, widened by a millionth of a cell against
+// rounding at the faces).
+__device__ __forceinline__ int cell_below(double v, double r, double h)
+{
+    return (int)floor((v - r) / h - 1.0e-6) + 1;
+}
+__device__ __forceinline__ int cell_above(double v, double r, double h)
+{
+    return (int)floor((v + r) / h + 1.0e-6) + 1;
+}
+
+namespace {
+// largest radius (positive doubles order like their bit patterns); *out zeroed before
+__global__ void k_rad_max(int n, const double *rad, unsigned long long *out)
+{
+    double m = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = fmax(m, rad[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+}  // namespace
+
 #define CHECK_INIT(c)                                                                   \
     do {                                                                                \
         if (!(c)) return DL_E_ARG;                                                      \
