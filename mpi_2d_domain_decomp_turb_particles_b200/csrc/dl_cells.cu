@@ -9,9 +9,11 @@
 // reference builds them, so every cell index and every shifted coordinate is the same
 // double.  Instead of a dense head/list array over (nx * (ny+2*ny_max) * (nz+2*nz_max))
 // cells, entries are counting-sorted by cell row (iy, iz) and sorted by ix inside each
-// row; a neighbour cell is then a binary search in a short row.  The set of visited
-// (ih1, ih2 > ih1) pairs is the reference's: owned partners are compared by reference
-// index (ypn order), ghosts always follow owned droplets in ypn order.
+// row; a start table per bucket of 2^s x cells locates a cell range, and a packed copy
+// of the sorted entries (positions, radius, ids) is what the searches stream, one
+// thread per sorted entry that is an owned droplet.  The set of visited (ih1, ih2 > ih1)
+// pairs is the reference's: owned partners are compared by reference index (ypn order),
+// ghosts always follow owned droplets in ypn order.
 #include "dl_internal.cuh"
 
 #include <algorithm>
