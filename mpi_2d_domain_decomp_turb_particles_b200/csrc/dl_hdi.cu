@@ -267,53 +267,6 @@ __global__ void k_coef_to_f32(int64_t n, const double *c, float *o)
 }
 
 // ---------------------------------------------------------------------------------------
-// AFUN_PRECOMP (partlib.f90:3466-3497): Ax = x + sum_j N_ij x_j, and b = sum_j N_ij (V_j - U_j)
-// ---------------------------------------------------------------------------------------
-template <typename T, typename C>
-__global__ void k_afun(int nps, const int *start, const int *partner, const C *coef, const T *x, int64_t ld, T *ax)
-{
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= nps) return;
-    T r0 = (T)0, r1 = (T)0, r2 = (T)0;
-    const int e1 = start[a + 1];
-    for (int e = start[a]; e < e1; e++) {
-        const int p = partner[e];
-        const T x1 = x[p], x2 = x[ld + p], x3 = x[2 * ld + p];
-        const C *n = coef + (int64_t)e * 6;
-        const T n2 = (T)n[0], n3 = (T)n[1], n4 = (T)n[2], n5 = (T)n[3], n6 = (T)n[4], n7 = (T)n[5];
-        r0 = r0 + n2 * x1 + n3 * x2 + n4 * x3;
-        r1 = r1 + n3 * x1 + n5 * x2 + n6 * x3;
-        r2 = r2 + n4 * x1 + n6 * x2 + n7 * x3;
-    }
-    ax[a] = r0 + x[a];
-    ax[ld + a] = r1 + x[ld + a];
-    ax[2 * ld + a] = r2 + x[2 * ld + a];
-}
-
-template <typename V>
-__global__ void k_afun_rhs(int nps, const int *start, const int *partner, const double *coef, const V *vx,
-                           const V *vy, const V *vz, const V *ux, const V *uy, const V *uz, int64_t ld, double *b)
-{
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= nps) return;
-    double b0 = 0.0, b1 = 0.0, b2 = 0.0;
-    const int e1 = start[a + 1];
-    for (int e = start[a]; e < e1; e++) {
-        const int p = partner[e];
-        const double w1 = (double)vx[p] - (double)ux[p];
-        const double w2 = (double)vy[p] - (double)uy[p];
-        const double w3 = (double)vz[p] - (double)uz[p];
-        const double *n = coef + (int64_t)e * 6;
-        b0 = b0 + n[0] * w1 + n[1] * w2 + n[2] * w3;
-        b1 = b1 + n[1] * w1 + n[3] * w2 + n[4] * w3;
-        b2 = b2 + n[2] * w1 + n[4] * w2 + n[5] * w3;
-    }
-    b[a] = b0;
-    b[ld + a] = b1;
-    b[2 * ld + a] = b2;
-}
-
-// ---------------------------------------------------------------------------------------
 // Vector kernels.  Reductions: fixed grid, per-thread strided partial sums in T, block
 // tree, then the last CTA to finish sums the CTA partials in order -> deterministic.
 // ---------------------------------------------------------------------------------------
@@ -349,6 +302,64 @@ __device__ __forceinline__ void finish_reduction(T part, T *partials, T *out, un
     if (threadIdx.x == 0) {
         *out = v;
         *ticket = 0u;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// AFUN_PRECOMP (partlib.f90:3466-3497): Ax = x + sum_j N_ij x_j, and b = sum_j N_ij (V_j - U_j)
+// ---------------------------------------------------------------------------------------
+template <typename T, typename C>
+__global__ void k_afun(int nps, const int *start, const int *partner, const C *coef, const T *x, int64_t ld, T *ax)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= nps) return;
+    T r0 = (T)0, r1 = (T)0, r2 = (T)0;
+    const int e1 = start[a + 1];
+    for (int e = start[a]; e < e1; e++) {
+        const int p = partner[e];
+        const T x1 = x[p], x2 = x[ld + p], x3 = x[2 * ld + p];
+        const C *n = coef + (int64_t)e * 6;
+        const T n2 = (T)n[0], n3 = (T)n[1], n4 = (T)n[2], n5 = (T)n[3], n6 = (T)n[4], n7 = (T)n[5];
+        r0 = r0 + n2 * x1 + n3 * x2 + n4 * x3;
+        r1 = r1 + n3 * x1 + n5 * x2 + n6 * x3;
+        r2 = r2 + n4 * x1 + n6 * x2 + n7 * x3;
+    }
+    ax[a] = r0 + x[a];
+    ax[ld + a] = r1 + x[ld + a];
+    ax[2 * ld + a] = r2 + x[2 * ld + a];
+}
+
+// Grid-stride over the droplets; with nrm, also ||b||^2 (fixed grid, CTA partials summed
+// in order by the last CTA: deterministic).
+template <typename V>
+__global__ void __launch_bounds__(kRedThreads) k_afun_rhs(int nps, const int *start, const int *partner,
+                                                          const double *coef, const V *vx, const V *vy, const V *vz,
+                                                          const V *ux, const V *uy, const V *uz, int64_t ld, double *b,
+                                                          double *nrm, double *partials, unsigned *ticket)
+{
+    __shared__ double sh[32];
+    double acc = 0.0;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nps; a += gridDim.x * blockDim.x) {
+        double b0 = 0.0, b1 = 0.0, b2 = 0.0;
+        const int e1 = start[a + 1];
+        for (int e = start[a]; e < e1; e++) {
+            const int p = partner[e];
+            const double w1 = (double)vx[p] - (double)ux[p];
+            const double w2 = (double)vy[p] - (double)uy[p];
+            const double w3 = (double)vz[p] - (double)uz[p];
+            const double *n = coef + (int64_t)e * 6;
+            b0 = b0 + n[0] * w1 + n[1] * w2 + n[2] * w3;
+            b1 = b1 + n[1] * w1 + n[3] * w2 + n[4] * w3;
+            b2 = b2 + n[2] * w1 + n[4] * w2 + n[5] * w3;
+        }
+        b[a] = b0;
+        b[ld + a] = b1;
+        b[2 * ld + a] = b2;
+        acc += b0 * b0 + b1 * b1 + b2 * b2;
+    }
+    if (nrm) {
+        acc = block_sum(acc, sh);
+        finish_reduction(acc, partials, nrm, ticket, sh);
     }
 }
 
@@ -451,26 +462,34 @@ __global__ void k_xupdate(int64_t n, int iters, const T *Q, int64_t qld, const d
 }
 
 // FP64 residual of the mixed solve: r = b - ((I + N) x) with FP64 tensors; also r in FP32
-__global__ void k_residual64(int nps, const int *start, const int *partner, const double *coef, const double *x,
-                             int64_t ld, const double *b, double *r, float *rf)
+// and ||r||^2 (grid-stride over a fixed grid, deterministic sum)
+__global__ void __launch_bounds__(kRedThreads) k_residual64(int nps, const int *start, const int *partner,
+                                                            const double *coef, const double *x, int64_t ld,
+                                                            const double *b, double *r, float *rf, double *nrm,
+                                                            double *partials, unsigned *ticket)
 {
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= nps) return;
-    double r0 = 0.0, r1 = 0.0, r2 = 0.0;
-    const int e1 = start[a + 1];
-    for (int e = start[a]; e < e1; e++) {
-        const int p = partner[e];
-        const double x1 = x[p], x2 = x[ld + p], x3 = x[2 * ld + p];
-        const double *n = coef + (int64_t)e * 6;
-        r0 = r0 + n[0] * x1 + n[1] * x2 + n[2] * x3;
-        r1 = r1 + n[1] * x1 + n[3] * x2 + n[4] * x3;
-        r2 = r2 + n[2] * x1 + n[4] * x2 + n[5] * x3;
+    __shared__ double sh[32];
+    double acc = 0.0;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nps; a += gridDim.x * blockDim.x) {
+        double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+        const int e1 = start[a + 1];
+        for (int e = start[a]; e < e1; e++) {
+            const int p = partner[e];
+            const double x1 = x[p], x2 = x[ld + p], x3 = x[2 * ld + p];
+            const double *n = coef + (int64_t)e * 6;
+            r0 = r0 + n[0] * x1 + n[1] * x2 + n[2] * x3;
+            r1 = r1 + n[1] * x1 + n[3] * x2 + n[4] * x3;
+            r2 = r2 + n[2] * x1 + n[4] * x2 + n[5] * x3;
+        }
+        const double q0 = b[a] - (r0 + x[a]);
+        const double q1 = b[ld + a] - (r1 + x[ld + a]);
+        const double q2 = b[2 * ld + a] - (r2 + x[2 * ld + a]);
+        r[a] = q0; r[ld + a] = q1; r[2 * ld + a] = q2;
+        rf[a] = (float)q0; rf[ld + a] = (float)q1; rf[2 * ld + a] = (float)q2;
+        acc += q0 * q0 + q1 * q1 + q2 * q2;
     }
-    const double q0 = b[a] - (r0 + x[a]);
-    const double q1 = b[ld + a] - (r1 + x[ld + a]);
-    const double q2 = b[2 * ld + a] - (r2 + x[2 * ld + a]);
-    r[a] = q0; r[ld + a] = q1; r[2 * ld + a] = q2;
-    rf[a] = (float)q0; rf[ld + a] = (float)q1; rf[2 * ld + a] = (float)q2;
+    acc = block_sum(acc, sh);
+    finish_reduction(acc, partials, nrm, ticket, sh);
 }
 
 template <typename S, typename D>
@@ -1572,10 +1591,10 @@ int gmres_fp64(dl_ctx *c, dl_gmres_report *rep)
                                                        tp<double>(c->pert[2]), ld, x0);
     DL_CHECK_LAUNCH(c);
     const int vs = c->vcur;
-    k_afun_rhs<double><<<bs, 256, 0, c->stream>>>(nps, c->nei_start, c->nei_idx, c->nei_coef64,
-                                                  tp<double>(c->vel[vs][0]), tp<double>(c->vel[vs][1]),
-                                                  tp<double>(c->vel[vs][2]), tp<double>(dl_vp_ptr(c, 0)),
-                                                  tp<double>(dl_vp_ptr(c, 1)), tp<double>(dl_vp_ptr(c, 2)), ld, b);
+    k_afun_rhs<double><<<kRedGrid, kRedThreads, 0, c->stream>>>(
+        nps, c->nei_start, c->nei_idx, c->nei_coef64, tp<double>(c->vel[vs][0]), tp<double>(c->vel[vs][1]),
+        tp<double>(c->vel[vs][2]), tp<double>(dl_vp_ptr(c, 0)), tp<double>(dl_vp_ptr(c, 1)),
+        tp<double>(dl_vp_ptr(c, 2)), ld, b, nullptr, nullptr, nullptr);
     DL_CHECK_LAUNCH(c);
     int r = afun<double, double>(c, c->nei_coef64, x0, ax);
     if (r) return r;
@@ -1697,15 +1716,16 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
                                                       tp<float>(c->pert[2]), ld, x);
     DL_CHECK_LAUNCH(c);
     const int vs = c->vcur;
-    k_afun_rhs<float><<<bs, 256, 0, c->stream>>>(nps, c->nei_start, c->nei_idx, c->nei_coef64,
-                                                 tp<float>(c->vel[vs][0]), tp<float>(c->vel[vs][1]),
-                                                 tp<float>(c->vel[vs][2]), tp<float>(dl_vp_ptr(c, 0)),
-                                                 tp<float>(dl_vp_ptr(c, 1)), tp<float>(dl_vp_ptr(c, 2)), ld, b);
+    // b and ||b||^2 (slot 0) in one pass
+    const Red<double> R = red_of<double>(c);
+    k_afun_rhs<float><<<kRedGrid, kRedThreads, 0, c->stream>>>(
+        nps, c->nei_start, c->nei_idx, c->nei_coef64, tp<float>(c->vel[vs][0]), tp<float>(c->vel[vs][1]),
+        tp<float>(c->vel[vs][2]), tp<float>(dl_vp_ptr(c, 0)), tp<float>(dl_vp_ptr(c, 1)),
+        tp<float>(dl_vp_ptr(c, 2)), ld, b, c->dots + kSlot0, R.partials, R.ticket);
     DL_CHECK_LAUNCH(c);
     int r, nc = 0;
     if ((r = pinned(c))) return r;
     if ((r = reduce_rows(c, nc))) return r;
-    if ((r = sumsq_to_slot<double>(c, b, n3, 0))) return r;
     if ((r = read_slots(c, 1))) return r;
     const double norm_b = std::sqrt(slot_value<double>(c, 0));
     memcpy(&nc, static_cast<const char *>(c->hpin) + 64, sizeof(int));
@@ -1716,11 +1736,12 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
     rep->norm_rhs = 0.0;
     bool converged = false;
     for (int sweep = 0; sweep <= kMaxRefine; sweep++) {
-        // FP64 residual of the current x
-        k_residual64<<<bs, 256, 0, c->stream>>>(nps, c->nei_start, c->nei_idx, c->nei_coef64, x, ld, b, r64, c->rf32);
+        // FP64 residual of the current x and ||r||^2 (slot 1)
+        k_residual64<<<kRedGrid, kRedThreads, 0, c->stream>>>(nps, c->nei_start, c->nei_idx, c->nei_coef64, x, ld, b,
+                                                              r64, c->rf32, c->dots + kSlot0 + 1, R.partials,
+                                                              R.ticket);
         DL_CHECK_LAUNCH(c);
         rep->refinements = sweep + 1;
-        if ((r = sumsq_to_slot<double>(c, r64, n3, 1))) return r;
         // the reduced right-hand side of the correction and its norm, read with ||r||
         if (nc > 0) {
             k_red_rhs<<<dl_blocks(nc, 256), 256, 0, c->stream>>>(nc, ld, c->red_list, c->red_start, c->nei_idx,
