@@ -229,16 +229,6 @@ __device__ __forceinline__ void interp_jac(const Field<double> &F, const double 
     }
 }
 
-__device__ __forceinline__ void load3(const float *p, float *v)
-{
-    const float4 q = *reinterpret_cast<const float4 *>(p);
-    v[0] = q.x; v[1] = q.y; v[2] = q.z;
-}
-__device__ __forceinline__ void load3(const double *p, double *v)
-{
-    const double2 q = *reinterpret_cast<const double2 *>(p);
-    v[0] = q.x; v[1] = q.y; v[2] = p[2];
-}
 // one vector atomic per point (FP32); three scalar atomics (FP64)
 __device__ __forceinline__ void add3(float *p, float a, float b, float c)
 {

@@ -1709,7 +1709,7 @@ int arnoldi_f32(dl_ctx *c, int sweep, int nc, double norm_b, double nf, double s
 int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
 {
     const int nps = c->nps;
-    const int64_t ld = nps, n3 = 3 * (int64_t)nps;
+    const int64_t ld = nps;
     const int bs = dl_blocks(nps, 256);
     double *x = c->xg, *b = c->bg64, *r64 = c->rg;
     k_copy3<float, double><<<bs, 256, 0, c->stream>>>(nps, tp<float>(c->pert[0]), tp<float>(c->pert[1]),
