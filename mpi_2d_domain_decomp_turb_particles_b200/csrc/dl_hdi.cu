@@ -1669,8 +1669,15 @@ int arnoldi_f32(dl_ctx *c, int sweep, int nc, double norm_b, double nf, double s
         const float *w1 = c->red_rhs;
         float *b0 = buf[0], *b1 = buf[1];
         void *args[] = {&a, &w1, &b0, &b1};
-        DL_CUDA(c, cudaLaunchCooperativeKernel((const void *)k_arn_solve, dim3(Gc), dim3(kArnThreads), args, 0,
-                                               c->stream));
+        const cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_arn_solve, dim3(Gc), dim3(kArnThreads),
+                                                          args, 0, c->stream);
+        if (e == cudaErrorCooperativeLaunchTooLarge) {
+            // the device is shared more than the occupancy query assumed: per-iteration launches
+            cudaGetLastError();
+            c->arn_coop_ctas = 0;
+            return arnoldi_f32(c, sweep, nc, norm_b, nf, stop_abs, iters);
+        }
+        DL_CUDA(c, e);
         DL_CHECK_LAUNCH(c);
         unsigned sync_err = 0;
         DL_CUDA(c, cudaMemcpyAsync(&hs, A.st, sizeof(hs), cudaMemcpyDeviceToHost, c->stream));
