@@ -953,27 +953,34 @@ __global__ void k_red_partner(int nnz, const int *partner, const int *pos, int *
     rpartner[e] = pos[p + 1] > pos[p] ? pos[p] : -1;
 }
 
-// r_C - N_CU r_U, packed
-__global__ void k_red_rhs(int nc, int64_t ld, const int *list, const int *rstart, const int *partner,
-                          const int *rpartner, const float *coef, const float *rf, float *rc)
+// r_C - N_CU r_U, packed, and its ||.||^2 (grid-stride over a fixed grid, deterministic)
+__global__ void __launch_bounds__(kRedThreads) k_red_rhs(int nc, int64_t ld, const int *list, const int *rstart,
+                                                         const int *partner, const int *rpartner, const float *coef,
+                                                         const float *rf, float *rc, float *nrm, float *partials,
+                                                         unsigned *ticket)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nc) return;
-    const int a = list[i];
-    float r0 = rf[a], r1 = rf[ld + a], r2 = rf[2 * ld + a];
-    const int e1 = rstart[i + 1];
-    for (int e = rstart[i]; e < e1; e++) {
-        if (rpartner[e] >= 0) continue;
-        const int p = partner[e];
-        const float x1 = rf[p], x2 = rf[ld + p], x3 = rf[2 * ld + p];
-        const float *n = coef + (int64_t)e * 6;
-        r0 = r0 - (n[0] * x1 + n[1] * x2 + n[2] * x3);
-        r1 = r1 - (n[1] * x1 + n[3] * x2 + n[4] * x3);
-        r2 = r2 - (n[2] * x1 + n[4] * x2 + n[5] * x3);
+    __shared__ float sh[32];
+    float acc = 0.0f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x) {
+        const int a = list[i];
+        float r0 = rf[a], r1 = rf[ld + a], r2 = rf[2 * ld + a];
+        const int e1 = rstart[i + 1];
+        for (int e = rstart[i]; e < e1; e++) {
+            if (rpartner[e] >= 0) continue;
+            const int p = partner[e];
+            const float x1 = rf[p], x2 = rf[ld + p], x3 = rf[2 * ld + p];
+            const float *n = coef + (int64_t)e * 6;
+            r0 = r0 - (n[0] * x1 + n[1] * x2 + n[2] * x3);
+            r1 = r1 - (n[1] * x1 + n[3] * x2 + n[4] * x3);
+            r2 = r2 - (n[2] * x1 + n[4] * x2 + n[5] * x3);
+        }
+        rc[i] = r0;
+        rc[nc + i] = r1;
+        rc[2 * nc + i] = r2;
+        acc += r0 * r0 + r1 * r1 + r2 * r2;
     }
-    rc[i] = r0;
-    rc[nc + i] = r1;
-    rc[2 * nc + i] = r2;
+    acc = block_sum(acc, sh);
+    finish_reduction(acc, partials, nrm, ticket, sh);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1407,16 +1414,6 @@ int pinned(dl_ctx *c)
     return 0;
 }
 
-template <typename T>
-int sumsq_to_slot(dl_ctx *c, const T *x, int64_t n, int slot)
-{
-    Red<T> R = red_of<T>(c);
-    k_sumsq<T><<<kRedGrid, kRedThreads, 0, c->stream>>>(n, x, reinterpret_cast<T *>(c->dots + kSlot0 + slot),
-                                                        R.partials, R.ticket);
-    DL_CHECK_LAUNCH(c);
-    return 0;
-}
-
 // slots [0, n) -> c->hpin (as 8-byte words), after whatever else was queued to c->hpin
 int read_slots(dl_ctx *c, int n)
 {
@@ -1751,11 +1748,11 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
         rep->refinements = sweep + 1;
         // the reduced right-hand side of the correction and its norm, read with ||r||
         if (nc > 0) {
-            k_red_rhs<<<dl_blocks(nc, 256), 256, 0, c->stream>>>(nc, ld, c->red_list, c->red_start, c->nei_idx,
-                                                                 c->red_partner, tp<float>(c->nei_coef), c->rf32,
-                                                                 c->red_rhs);
+            const Red<float> Rf = red_of<float>(c);
+            k_red_rhs<<<std::min(dl_blocks(nc, kRedThreads), kRedGrid), kRedThreads, 0, c->stream>>>(
+                nc, ld, c->red_list, c->red_start, c->nei_idx, c->red_partner, tp<float>(c->nei_coef), c->rf32,
+                c->red_rhs, reinterpret_cast<float *>(c->dots + kSlot0 + 2), Rf.partials, Rf.ticket);
             DL_CHECK_LAUNCH(c);
-            if ((r = sumsq_to_slot<float>(c, c->red_rhs, 3 * (int64_t)nc, 2))) return r;
         }
         if ((r = read_slots(c, 3))) return r;
         const double nr = std::sqrt(slot_value<double>(c, 1));

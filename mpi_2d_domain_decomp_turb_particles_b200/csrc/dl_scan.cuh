@@ -8,7 +8,7 @@ namespace {
 
 __global__ void __launch_bounds__(1024) k_cnt_blocksum(int n, const int *cnt, int *bsum, int *maxcnt)
 {
-    __shared__ int ws[32];
+    __shared__ int ws[32], wm[32];
     const int i = blockIdx.x * 1024 + threadIdx.x;
     const int v = i < n ? cnt[i] : 0;
     int s = v, m = v;
@@ -18,13 +18,19 @@ __global__ void __launch_bounds__(1024) k_cnt_blocksum(int n, const int *cnt, in
     }
     if ((threadIdx.x & 31) == 0) {
         ws[threadIdx.x >> 5] = s;
-        if (maxcnt) atomicMax(maxcnt, m);
+        wm[threadIdx.x >> 5] = m;
     }
     __syncthreads();
     if (threadIdx.x < 32) {
-        int t = ws[threadIdx.x];
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-        if (threadIdx.x == 0) bsum[blockIdx.x] = t;
+        int t = ws[threadIdx.x], u = wm[threadIdx.x];
+        for (int o = 16; o > 0; o >>= 1) {
+            t += __shfl_down_sync(0xffffffffu, t, o);
+            u = max(u, __shfl_down_sync(0xffffffffu, u, o));
+        }
+        if (threadIdx.x == 0) {
+            bsum[blockIdx.x] = t;
+            if (maxcnt) atomicMax(maxcnt, u);   // one atomic per CTA
+        }
     }
 }
 
