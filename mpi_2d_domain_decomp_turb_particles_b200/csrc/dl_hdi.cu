@@ -954,12 +954,13 @@ __global__ void k_red_partner(int nnz, const int *partner, const int *pos, int *
 }
 
 // r_C - N_CU r_U, packed, and its ||.||^2 (grid-stride over a fixed grid, deterministic)
-__global__ void __launch_bounds__(kRedThreads) k_red_rhs(int nc, int64_t ld, const int *list, const int *rstart,
-                                                         const int *partner, const int *rpartner, const float *coef,
-                                                         const float *rf, float *rc, float *nrm, float *partials,
-                                                         unsigned *ticket)
+__global__ void __launch_bounds__(kRedThreads) k_red_rhs(const int *ncp, int64_t ld, const int *list,
+                                                         const int *rstart, const int *partner, const int *rpartner,
+                                                         const float *coef, const float *rf, float *rc, float *nrm,
+                                                         float *partials, unsigned *ticket)
 {
     __shared__ float sh[32];
+    const int nc = *ncp;   // the coupled-row count stays on the device
     float acc = 0.0f;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x) {
         const int a = list[i];
@@ -1404,6 +1405,7 @@ int sumsq(dl_ctx *c, const T *x, int64_t n, double *out)
 // Result slots for reductions whose values the host reads together (8 bytes each, after
 // the reduction scratch in c->dots), and the pinned host buffer they are read into.
 constexpr int kSlot0 = kRedGrid + kMaxIter + 4;
+constexpr int kArnStatusAt = 96;   // byte offset of a deferred Arnoldi state in c->hpin
 
 int pinned(dl_ctx *c)
 {
@@ -1641,6 +1643,8 @@ int reduce_rows(dl_ctx *c, int &nc)
 
 // The FP32 solve of the coupled rows: (I + N_CC) d_C = c->red_rhs (norm nf) from d0 = 0
 // by the fused Arnoldi kernels; the coefficients stay in the state for the x update.
+// The cooperative launch returns iters = -1: its state arrives in the pinned buffer
+// (at kArnStatusAt) with the caller's next read_slots.
 // The iterations are queued in batches (the first as long as this sweep's previous
 // solve, then two at a time) and the host reads the state once per batch.
 int arnoldi_f32(dl_ctx *c, int sweep, int nc, double norm_b, double nf, double stop_abs, int &iters)
@@ -1676,12 +1680,12 @@ int arnoldi_f32(dl_ctx *c, int sweep, int nc, double norm_b, double nf, double s
         }
         DL_CUDA(c, e);
         DL_CHECK_LAUNCH(c);
-        unsigned sync_err = 0;
-        DL_CUDA(c, cudaMemcpyAsync(&hs, A.st, sizeof(hs), cudaMemcpyDeviceToHost, c->stream));
-        DL_CUDA(c, cudaMemcpyAsync(&sync_err, A.sync + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
-        DL_CUDA(c, cudaStreamSynchronize(c->stream));
-        if (sync_err || !hs.done) return dl_fail(c, DL_E_CUDA, "HDI_GMRES: grid barrier of the FP32 solve timed out");
-        iters = hs.iters;
+        // the state and the barrier's error word come back with the caller's next read
+        DL_CUDA(c, cudaMemcpyAsync(static_cast<char *>(c->hpin) + kArnStatusAt, A.st, sizeof(ArnStatus),
+                                   cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaMemcpyAsync(static_cast<char *>(c->hpin) + kArnStatusAt + sizeof(ArnStatus), A.sync + 2,
+                                   sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+        iters = -1;
         return 0;
     }
     int &guess = c->arn_guess[std::min(sweep, 7)];
@@ -1729,11 +1733,10 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
     DL_CHECK_LAUNCH(c);
     int r, nc = 0;
     if ((r = pinned(c))) return r;
-    if ((r = reduce_rows(c, nc))) return r;
-    if ((r = read_slots(c, 1))) return r;
-    const double norm_b = std::sqrt(slot_value<double>(c, 0));
-    memcpy(&nc, static_cast<const char *>(c->hpin) + 64, sizeof(int));
-    const ArnArgs A = arn_args(c, nc);
+    if ((r = reduce_rows(c, nc))) return r;   // the count arrives with the first read
+    double norm_b = 0.0;
+    ArnArgs A = arn_args(c, 0);
+    bool pending = false;                      // a solve whose state comes with the next read
     rep->iterations = 0;
     rep->refinements = 0;
     rep->residual = 0.0;
@@ -1746,15 +1749,31 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
                                                               R.ticket);
         DL_CHECK_LAUNCH(c);
         rep->refinements = sweep + 1;
-        // the reduced right-hand side of the correction and its norm, read with ||r||
-        if (nc > 0) {
+        // the reduced right-hand side of the correction and its norm, read with ||r|| (and,
+        // the first time, with ||b|| and the coupled-row count)
+        {
             const Red<float> Rf = red_of<float>(c);
-            k_red_rhs<<<std::min(dl_blocks(nc, kRedThreads), kRedGrid), kRedThreads, 0, c->stream>>>(
-                nc, ld, c->red_list, c->red_start, c->nei_idx, c->red_partner, tp<float>(c->nei_coef), c->rf32,
-                c->red_rhs, reinterpret_cast<float *>(c->dots + kSlot0 + 2), Rf.partials, Rf.ticket);
+            k_red_rhs<<<kRedGrid, kRedThreads, 0, c->stream>>>(
+                c->red_pos + nps, ld, c->red_list, c->red_start, c->nei_idx, c->red_partner, tp<float>(c->nei_coef),
+                c->rf32, c->red_rhs, reinterpret_cast<float *>(c->dots + kSlot0 + 2), Rf.partials, Rf.ticket);
             DL_CHECK_LAUNCH(c);
         }
         if ((r = read_slots(c, 3))) return r;
+        if (sweep == 0) {
+            norm_b = std::sqrt(slot_value<double>(c, 0));
+            memcpy(&nc, static_cast<const char *>(c->hpin) + 64, sizeof(int));
+            A = arn_args(c, nc);
+        }
+        if (pending) {
+            ArnStatus hs;
+            unsigned sync_err = 0;
+            memcpy(&hs, static_cast<const char *>(c->hpin) + kArnStatusAt, sizeof(hs));
+            memcpy(&sync_err, static_cast<const char *>(c->hpin) + kArnStatusAt + sizeof(hs), sizeof(sync_err));
+            if (sync_err || !hs.done)
+                return dl_fail(c, DL_E_CUDA, "HDI_GMRES: grid barrier of the FP32 solve timed out");
+            rep->iterations += hs.iters;
+            pending = false;
+        }
         const double nr = std::sqrt(slot_value<double>(c, 1));
         if (sweep == 0) {
             rep->norm_rhs = nr;
@@ -1774,7 +1793,8 @@ int gmres_mixed(dl_ctx *c, dl_gmres_report *rep)
             const double stop_abs = std::max(0.1 * kMaxErr * norm_b, 1.0e-5 * nf);
             int iters = 0;
             if ((r = arnoldi_f32(c, sweep, nc, norm_b, nf, stop_abs, iters))) return r;
-            rep->iterations += iters;
+            if (iters < 0) pending = true;
+            else rep->iterations += iters;
         }
         k_red_xupdate<<<dim3(dl_blocks(nps, 256) + dl_blocks(nc, 256), 3), 256, 0, c->stream>>>(
             nps, nc, c->red_pos, c->red_list, A.st, solve ? 1 : 0, A.Q, A.qld, r64, x);
