@@ -167,7 +167,10 @@ int dl_interpolate(dl_ctx *ctx, int icpt);
 int dl_part_history_fvp(dl_ctx *ctx);                       /* PART_HISTORY_FVP(id), partlib.f90:553-595 */
 int dl_headlist(dl_ctx *ctx, double dist);                  /* HEADLIST(id, dist), partlib.f90:2171-2444 */
 int dl_nei_list_precomp(dl_ctx *ctx);                       /* NEI_LIST_PRECOMP(id), partlib.f90:3218-3371 */
-int dl_hdi_gmres(dl_ctx *ctx, dl_gmres_report *rep);        /* HDI_GMRES(id), partlib.f90:2795-3005 */
+/* HDI_GMRES(id), partlib.f90:2795-3005.  The mixed path's FP32 solve runs as one cooperative
+ * launch whose grid barriers give up after a polling limit (DL_E_CUDA, pertvel unchanged);
+ * the environment variable DL_ARN_SPIN_LIMIT, read by dl_create, lowers that limit (tests). */
+int dl_hdi_gmres(dl_ctx *ctx, dl_gmres_report *rep);
 int dl_part_history_fdp(dl_ctx *ctx);                       /* PART_HISTORY_FDP(id), partlib.f90:599-625 */
 int dl_part_advance(dl_ctx *ctx);                           /* PART_ADVANCE(id), partlib.f90:629-726 */
 int dl_complete_ypn(dl_ctx *ctx);                           /* COMPLETE_YPN(id), partlib.f90:761-838 */
@@ -368,7 +371,8 @@ int dl_adj_timing(dl_adj *a, double *forward_ms, double *backward_ms);
  * most 2^26 droplets and 2^17 departing droplets per call (DL_E_ARG / DL_E_CAPACITY beyond,
  * with new_of_old left as the identity in the latter case).  Calls that overlap on the GPU
  * race on the shared scratch.  The first call on a device looks up the scratch address
- * (cudaGetSymbolAddress) and should come before any stream capture on that device.
+ * (cudaGetSymbolAddress), keeps it for the life of the process and should come before any
+ * stream capture on that device; a device reset (cudaDeviceReset) after it is not supported.
  * Runs on `stream` (a cudaStream_t, NULL = default stream) and synchronises it. */
 int dl_periodic_order_noalloc(const double *y, const double *z, int n, int *new_of_old, void *stream);
 

@@ -9,6 +9,7 @@
 #include "dl_scan.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <unordered_map>
 #include <cmath>
 #include <cstdio>
@@ -487,6 +488,9 @@ static int allocate_state(dl_ctx *c)
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
     if (c->num_sms <= 0) c->num_sms = 148;
     c->arn_coop_ctas = -1;
+    // test hook: DL_ARN_SPIN_LIMIT (read here, once per context) lowers the polling limit of
+    // the cooperative FP32 solve's grid barrier so that a test can make the barrier give up
+    if (const char *lim = getenv("DL_ARN_SPIN_LIMIT")) c->arn_spin_limit = atoll(lim);
     return 0;
 }
 

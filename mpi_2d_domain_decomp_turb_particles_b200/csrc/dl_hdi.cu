@@ -571,6 +571,7 @@ struct ArnArgs {
     unsigned *ticket;
     float *part2;         // second bank of partial sums (cooperative solve)
     unsigned *sync;       // grid barrier of the cooperative solve: count, generation, error
+    unsigned spin_limit;  // polls before a grid barrier of the cooperative solve gives up
 };
 
 __device__ __forceinline__ float warp_sum_f(float v)
@@ -999,8 +1000,9 @@ constexpr unsigned kSpinLimit = 1u << 22;   // ~0.3 s of polling before a barrie
 constexpr int kArnCoopCtasPerSm = kArnCtasPerSm;   // CTAs per SM of the cooperative solve
 
 // Grid barrier for co-resident CTAs (cooperative launch).  Bounded: a CTA that polls
-// kSpinLimit times without the generation moving sets the error word and returns false.
-__device__ __forceinline__ bool arn_grid_sync(unsigned *sy)
+// `limit` times (kSpinLimit unless lowered for a test) without the generation moving sets
+// the error word and returns false; every later barrier of the launch then fails as well.
+__device__ __forceinline__ bool arn_grid_sync(unsigned *sy, unsigned limit)
 {
     __shared__ int s_ok;
     __syncthreads();
@@ -1016,7 +1018,7 @@ __device__ __forceinline__ bool arn_grid_sync(unsigned *sy)
         } else {
             unsigned spins = 0;
             while (*gen == g0) {
-                if (++spins > kSpinLimit) {
+                if (++spins > limit) {
                     ok = 0;
                     atomicExch(sy + 2, 1u);
                     break;
@@ -1173,7 +1175,7 @@ __global__ void __launch_bounds__(kArnThreads, kArnCtasPerSm) k_arn_solve(ArnArg
         }
         float *P = (phase++ & 1) ? A.part2 : A.part;
         arn_put_partials(P, k, acc, true, nrm, true);
-        if (!arn_grid_sync(A.sync)) return;
+        if (!arn_grid_sync(A.sync, A.spin_limit)) return;
         arn_get_partials(P, k, true, sh1, true, &s_nv2);
         if (threadIdx.x == 0) {
             double hh = 0.0;
@@ -1189,7 +1191,7 @@ __global__ void __launch_bounds__(kArnThreads, kArnCtasPerSm) k_arn_solve(ArnArg
         arn_project(A, k, v, sh1, again, sv, acc, nrm);
         P = (phase++ & 1) ? A.part2 : A.part;
         arn_put_partials(P, k, acc, again, nrm, !again);
-        if (!arn_grid_sync(A.sync)) return;
+        if (!arn_grid_sync(A.sync, A.spin_limit)) return;
         arn_get_partials(P, k, again, sh2, !again, &s_nn2);
         if (again) {
             // ---- phase 3: v -= Q h2, ||v||^2 ----
@@ -1197,7 +1199,7 @@ __global__ void __launch_bounds__(kArnThreads, kArnCtasPerSm) k_arn_solve(ArnArg
             arn_project(A, k, v, sh2, false, sv, acc, nrm);
             P = (phase++ & 1) ? A.part2 : A.part;
             arn_put_partials(P, k, acc, false, nrm, true);
-            if (!arn_grid_sync(A.sync)) return;
+            if (!arn_grid_sync(A.sync, A.spin_limit)) return;
             arn_get_partials(P, k, false, nullptr, true, &s_nn2);
         }
         // ---- Hessenberg column, Givens update, residual estimate (every CTA) ----
@@ -1328,6 +1330,7 @@ ArnArgs arn_args(dl_ctx *c, int nc)
     A.s = A.h2 + kMaxIter;
     A.ticket = reinterpret_cast<unsigned *>(A.s + 4);
     A.sync = A.ticket + 4;
+    A.spin_limit = c->arn_spin_limit > 0 ? (unsigned)c->arn_spin_limit : kSpinLimit;
     return A;
 }
 

@@ -217,6 +217,7 @@ struct dl_ctx {
     void *arn;                   // fused FP32 Arnoldi: least-squares state, partial dots, scalars
     int arn_guess[8];            // iterations of the previous FP32 solve of each refinement sweep
     int arn_coop_ctas;           // CTAs of the cooperative FP32 solve that fit at once (-1: not yet asked)
+    long long arn_spin_limit;    // grid-barrier polling limit of that solve (0: the default; tests lower it)
     double *rmax_dev;            // largest droplet radius (OVERLAP_DET reach)
     void *hpin;                  // 256 bytes of pinned host memory for small device->host reads
     void *hstage;                // pinned staging of a step's variable-size reads (grown on demand)

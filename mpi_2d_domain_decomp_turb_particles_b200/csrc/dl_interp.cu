@@ -203,15 +203,18 @@ __device__ __forceinline__ double wrap_coord(double x, double h)
     return x;
 }
 
-// Advance of one droplet (partlib.f90:640-684) with the history already loaded.
+// Advance of one droplet (partlib.f90:640-684) with the history already loaded.  u is the
+// interpolated fluid velocity and pu the HDI disturbance velocity (nullptr without HDI):
+// the nonlinear drag's slip is (yp(4:6) - vp) - pertvel, in the reference's order.
 template <typename T>
-__device__ __forceinline__ void advance_math(T a, const T *u, const T *f0, const T *f1, const T *f2,
+__device__ __forceinline__ void advance_math(T a, const T *u, const T *pu, const T *f0, const T *f1, const T *f2,
                                              const T *d0, const T *d1, const T *d2, const T *d3,
                                              T dt, T tau2, T sv, T rnu, int ndrag, T *vnew, T *dm)
 {
     T fsn = (T)1.0;
     if (ndrag == 1) {
         T e0 = f0[0] - u[0], e1 = f0[1] - u[1], e2 = f0[2] - u[2];
+        if (pu) { e0 = e0 - pu[0]; e1 = e1 - pu[1]; e2 = e2 - pu[2]; }
         T vrel = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
         fsn = (T)1.0 + (T)0.15 * pow(vrel * (T)2.0 * a / rnu, (T)0.687);
     }
@@ -278,7 +281,8 @@ __device__ __forceinline__ void epilogue_one(const InterpArgs<T> &A, int d, cons
             d0[c] = u[c]; d1[c] = A.f1[c][d]; d2[c] = A.f2[c][d]; d3[c] = A.f3[c][d];
         }
     }
-    advance_math<T>(a, u, f0, f1, f2, d0, d1, d2, d3, A.dt, A.tau2, A.sv, A.rnu, A.ndrag, vn, dm);
+    advance_math<T>(a, u, (const T *)nullptr, f0, f1, f2, d0, d1, d2, d3, A.dt, A.tau2, A.sv, A.rnu, A.ndrag, vn,
+                    dm);
     double xo[3] = {A.px[d], A.py[d], A.pz[d]};
     double xn[3];
 #pragma unroll
@@ -833,14 +837,15 @@ __global__ void k_advance(AdvArgs<T> A)
 {
     int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= A.nps) return;
-    T f0[3], f1[3], f2[3], e0[3], e1[3], e2[3], e3[3], u[3], vn[3], dm[3];
+    T f0[3], f1[3], f2[3], e0[3], e1[3], e2[3], e3[3], u[3], pu[3], vn[3], dm[3];
     for (int c = 0; c < 3; c++) {
         f0[c] = A.v0[c][d]; f1[c] = A.v1[c][d]; f2[c] = A.v2[c][d];
         e0[c] = A.d0[c][d]; e1[c] = A.d1[c][d]; e2[c] = A.d2[c][d]; e3[c] = A.d3[c][d];
         u[c] = A.u[c][d];
-        if (A.hdi) u[c] = u[c] + A.pert[c][d];
+        pu[c] = A.hdi ? A.pert[c][d] : (T)0;
     }
-    advance_math<T>((T)A.rad[d], u, f0, f1, f2, e0, e1, e2, e3, A.dt, A.tau2, A.sv, A.rnu, A.ndrag, vn, dm);
+    advance_math<T>((T)A.rad[d], u, A.hdi ? pu : nullptr, f0, f1, f2, e0, e1, e2, e3, A.dt, A.tau2, A.sv, A.rnu,
+                    A.ndrag, vn, dm);
     for (int c = 0; c < 3; c++) { A.vn[c][d] = vn[c]; A.dm[c][d] = dm[c]; }
 }
 

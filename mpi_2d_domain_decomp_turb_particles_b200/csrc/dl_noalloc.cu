@@ -10,7 +10,10 @@
 // Limits: n <= DL_NOALLOC_MAX_N droplets and at most DL_NOALLOC_MAX_DEPART departing
 // droplets per call.  Every call shares the scratch array, which keeps the last call's
 // contents; calls that overlap on the GPU (different streams, different host threads)
-// race on it and must be serialised by the caller.
+// race on it and must be serialised by the caller.  The device address of the array is
+// looked up once per device, by the first call on that device, and kept for the life of
+// the process: that first call should come before any stream capture on the device, and a
+// device reset (cudaDeviceReset) after it is not supported.
 #include "dl_internal.cuh"
 
 #include <mutex>
@@ -21,8 +24,13 @@
 namespace {
 
 constexpr int kBlk = DL_NOALLOC_MAX_N / 1024;
-// layout: [0] status, [1] departures, [2..15] unused, [16 .. 16+kBlk] block counts/offsets,
-// then departing indices (ascending), then the departure examination order
+// A departing droplet is carried as (neighbour code << 26) | index (index < 2^26, code 1..8).
+constexpr int kIdxBits = 26;
+constexpr int kIdxMask = (1 << kIdxBits) - 1;
+// layout: [0] status, [1] departures, [2..10] departures per neighbour code 0..8, [11..15]
+// unused, [16 .. 16+kBlk] block counts/offsets, then the departing droplets (ascending
+// index), then the departures in the replay's examination order
+constexpr int kOffCode = 2;
 constexpr int kOffBlk = 16;
 constexpr int kOffP = kOffBlk + kBlk + 16;
 constexpr int kOffDep = kOffP + DL_NOALLOC_MAX_DEPART;
@@ -97,12 +105,14 @@ __global__ void __launch_bounds__(1024) k_na_scan(int nblk, int *s)
     }
 }
 
+// departing droplets in ascending index order, each with its neighbour code
 __global__ void __launch_bounds__(1024) k_na_compact(int n, const double *y, const double *z, double pi2, int *s)
 {
     __shared__ int wsum[32];
     if (s[0]) return;
     const int i = blockIdx.x * 1024 + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const bool f = i < n && depart_code(y[i], z[i], pi2) != 0;
+    const int code = i < n ? depart_code(y[i], z[i], pi2) : 0;
+    const bool f = code != 0;
     const unsigned m = __ballot_sync(0xffffffffu, f);
     if (lane == 0) wsum[w] = __popc(m);
     __syncthreads();
@@ -115,38 +125,75 @@ __global__ void __launch_bounds__(1024) k_na_compact(int n, const double *y, con
         wsum[lane] = incl - v;
     }
     __syncthreads();
-    if (f) s[kOffP + s[kOffBlk + blockIdx.x] + wsum[w] + __popc(m & ((1u << lane) - 1))] = i;
+    if (f) s[kOffP + s[kOffBlk + blockIdx.x] + wsum[w] + __popc(m & ((1u << lane) - 1))] = (code << kIdxBits) | i;
 }
 
-// The swap-with-last loop replayed over the departing droplets only (one thread), then the
-// departures appended in neighbour order 1..8 (partlib.f90:1099-1133).
-__global__ void k_na_replay(int n, const double *y, const double *z, double pi2, int *s, int *new_of_old)
+// The swap-with-last loop of partlib.f90:866-1097 replayed over the departing droplets only
+// (one thread: each step depends on the previous one): records the order in which the
+// departures are examined and counts them per neighbour code.
+__global__ void k_na_replay(int n, int *s, int *new_of_old)
 {
     if (threadIdx.x != 0 || s[0]) return;
     const int k = s[1];
     const int *P = s + kOffP;
     int *dep = s + kOffDep;
+    int cnt[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     int lo = 0, hi = k - 1, sum = 0, nd = 0;
     while (lo <= hi) {
-        const int h = P[lo] + 1;
+        const int h = (P[lo] & kIdxMask) + 1;
         if (h + sum > n) break;
+        int pe = P[lo];
         lo++;
-        int e = h;
         for (int guard = 0; guard <= k; guard++) {
-            dep[nd++] = e - 1;
+            dep[nd++] = pe;
+            cnt[pe >> kIdxBits]++;
             sum++;
             const int t = n - sum + 1;
             if (t == h) break;
-            if (hi >= lo && P[hi] + 1 == t) { hi--; e = t; continue; }
+            if (hi >= lo && (P[hi] & kIdxMask) + 1 == t) { pe = P[hi]; hi--; continue; }
             new_of_old[t - 1] = h - 1;
             break;
         }
     }
     if (nd != k) { s[0] = 2; return; }
-    int slot = n - k;
-    for (int q = 1; q <= 8; q++)
-        for (int j = 0; j < nd; j++)
-            if (depart_code(y[dep[j]], z[dep[j]], pi2) == q) new_of_old[dep[j]] = slot++;
+    for (int q = 0; q <= 8; q++) s[kOffCode + q] = cnt[q];
+}
+
+// The departures appended in neighbour order 1..8, each code's droplets in examination
+// order (partlib.f90:1099-1133): a stable counting placement by one CTA.
+__global__ void __launch_bounds__(1024) k_na_place(int n, const int *s, int *new_of_old)
+{
+    __shared__ int wcnt[32][9];   // per warp and code: count, then the warp's first slot
+    __shared__ int base[9];       // next free slot of each code
+    if (s[0]) return;
+    const int k = s[1];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        int b = n - k;
+        base[0] = 0;
+        for (int q = 1; q <= 8; q++) { base[q] = b; b += s[kOffCode + q]; }
+    }
+    const int *dep = s + kOffDep;
+    for (int c0 = 0; c0 < k; c0 += 1024) {
+        const int j = c0 + threadIdx.x;
+        const int pe = j < k ? dep[j] : 0;
+        const int q = pe >> kIdxBits;   // 0 past the end
+        const unsigned peers = __match_any_sync(0xffffffffu, q);
+        const int rank = __popc(peers & ((1u << lane) - 1u));
+        if (lane < 9) wcnt[w][lane] = 0;
+        __syncwarp();
+        if (rank == 0) wcnt[w][q] = __popc(peers);
+        __syncthreads();
+        if (threadIdx.x < 9) {
+            const int c = threadIdx.x;
+            int a = base[c];
+            for (int v = 0; v < 32; v++) { const int t = wcnt[v][c]; wcnt[v][c] = a; a += t; }
+            base[c] = a;
+        }
+        __syncthreads();
+        if (q > 0) new_of_old[pe & kIdxMask] = wcnt[w][q] + rank;
+        __syncthreads();
+    }
 }
 
 std::mutex g_setup_mutex;
@@ -181,7 +228,8 @@ extern "C" int dl_periodic_order_noalloc(const double *y, const double *z, int n
     k_na_count<<<nblk, 1024, 0, st>>>(n, y, z, pi2, s, new_of_old);
     k_na_scan<<<1, 1024, 0, st>>>(nblk, s);
     k_na_compact<<<nblk, 1024, 0, st>>>(n, y, z, pi2, s);
-    k_na_replay<<<1, 32, 0, st>>>(n, y, z, pi2, s, new_of_old);
+    k_na_replay<<<1, 32, 0, st>>>(n, s, new_of_old);
+    k_na_place<<<1, 1024, 0, st>>>(n, s, new_of_old);
     if (cudaGetLastError() != cudaSuccess) return DL_E_CUDA;
     int status = 0;
     if (cudaMemcpyAsync(&status, s, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return DL_E_CUDA;

@@ -14,6 +14,7 @@ import pytest
 import oracle as orc
 from cases import dense_params, smooth_field
 from mpi_2d_domain_decomp_turb_particles_b200 import Partlib
+from mpi_2d_domain_decomp_turb_particles_b200._lib import DropletError
 
 pytestmark = pytest.mark.gpu
 
@@ -210,3 +211,65 @@ def test_hdi_coalescence_keeps_pertvel_by_reference():
         po = o.arr("pertvel")[:3 * o.nps].reshape(-1, 3)
         assert np.linalg.norm(pg - po) <= 1e-9 * np.linalg.norm(po)
     assert merged > 0
+
+
+def test_fp32_solve_grid_barrier_gives_up_with_an_error(monkeypatch):
+    """The cooperative FP32 solve's grid barriers are bounded: with the polling limit
+    lowered to one poll (DL_ARN_SPIN_LIMIT, read when the context is created) the barrier
+    gives up, HDI_GMRES returns DL_E_CUDA naming the barrier, and pertvel keeps its value.
+    A context created without the knob then solves the same system normally."""
+    f = smooth_field(32)
+    p = hdi_params("mixed")
+    monkeypatch.setenv("DL_ARN_SPIN_LIMIT", "1")
+    g, o = make_settled(p, f)
+    monkeypatch.delenv("DL_ARN_SPIN_LIMIT")
+    through_nei(g, o, f)
+    before = g.get_pertvel()
+    with pytest.raises(DropletError) as e:
+        g.hdi_gmres()
+    assert e.value.code == -2 and "grid barrier" in str(e.value)
+    assert np.array_equal(g.get_pertvel(), before)
+    g.close()
+    g, o = make_settled(p, f)
+    through_nei(g, o, f)
+    rep = g.hdi_gmres()
+    o.hdi_gmres()
+    assert rep.iterations > 0 and rep.residual < 1e-6
+    po = o.arr("pertvel")[:3 * o.nps].reshape(-1, 3)
+    assert np.linalg.norm(g.get_pertvel() - po) <= 1e-5 * np.linalg.norm(po)
+    g.close()
+
+
+@pytest.mark.parametrize("hdi", [False, True])
+def test_nonlinear_drag_tracks_oracle(hdi):
+    """ndrag = 1 (partlib.f90:645-653): the drag factor 1 + 0.15 Re_p^0.687 in the advance.
+    FP64 steps against the FP64 oracle (the device pow and the host libm pow may differ in
+    the last bit, so the state is compared to 1e-12 instead of bit for bit) with identical
+    pair lists; the mixed path's velocities within 1e-5."""
+    f = smooth_field(32)
+    for prec in ("fp64", "mixed"):
+        p = hdi_params(prec, ndrag=1) if hdi else dense_params(n=32, npart=6000, precision=prec, ndrag=1)
+        if hdi:
+            g, o = make_settled(p, f)
+        else:
+            g = Partlib(p)
+            g.part_init()
+            o = orc.Oracle(**p.oracle_kwargs())
+            o.part_init()
+            g.set_fields(*f)
+        for step in range(1, 6):
+            g.particle_step()
+            o.particle_step(*f)
+            assert g.nps == o.nps
+            s = g.get_particles()
+            ref = o.yp[:o.nps]
+            vrel = np.linalg.norm(s["yp"][:, 3:6] - ref[:, 3:6]) / np.linalg.norm(ref[:, 3:6])
+            if prec == "fp64":
+                gp = sorted(map(tuple, g.pairs().tolist()))
+                op = sorted((int(r[0]), int(r[2]), int(r[3]), int(r[4])) for r in o.pairs())
+                assert gp == op
+                assert np.abs(s["yp"][:, :3] - ref[:, :3]).max() < 1e-12
+                assert vrel < (1e-9 if hdi else 1e-12), (step, vrel)
+            else:
+                assert vrel < 1e-5, (step, vrel)
+        g.close()
