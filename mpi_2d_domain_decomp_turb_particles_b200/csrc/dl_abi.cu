@@ -456,6 +456,7 @@ static int allocate_state(dl_ctx *c)
     ALLOC(c->lv_dev, sizeof(int) * m);
     ALLOC(c->lv_dep, sizeof(int) * m);
     ALLOC(c->d_err, sizeof(int));
+    ALLOC(c->col_work, 2 * sizeof(int));
     ALLOC(c->xfer64, sizeof(double) * (3 * m + 16));
     ALLOC(c->xfer_i, sizeof(int) * (4 * m + 16));
     // statistics
@@ -509,7 +510,7 @@ extern "C" int dl_destroy(dl_ctx *c)
     F(c->long_rows); F(c->n_long);
     F(c->brick_start); F(c->brick_cnt); F(c->lhnode); F(c->bg); F(c->ghosts); F(c->d_nghost); F(c->gh_blk); F(c->gh_start); F(c->pert_tmp); F(c->lv_src); F(c->lv_list); F(c->lv_n);
     F(c->ent_row); F(c->ent_ix); F(c->row_start); F(c->row_fill); F(c->row_ent); F(c->leave_nid);
-    F(c->lv_refs); F(c->lv_old); F(c->lv_new); F(c->lv_dev); F(c->lv_dep); F(c->d_err);
+    F(c->lv_refs); F(c->lv_old); F(c->lv_new); F(c->lv_dev); F(c->lv_dep); F(c->d_err); F(c->col_work);
     F(c->xfer64); F(c->xfer_i); F(c->hist_i); F(c->hist_d); F(c->acc_i); F(c->acc_d); F(c->out_i); F(c->out_d);
     F(c->counts); F(c->cand); F(c->pairs); F(c->contacts); F(c->remove_dev); F(c->pair_buf); F(c->pair_ibuf); F(c->mv_acc);
     F(c->ovl_list); F(c->ovl_cnt); F(c->fpad_own);

@@ -121,6 +121,8 @@ struct dl_ctx {
     int field_set[3];
     int fpad_valid;              // bit k: component k present in fpad
     CUtensorMap tmap;            // TMA descriptor of fpad
+    CUtensorMap tmap1;           // the same field with a one-component box (column sweep)
+    int *col_work;               // column sweep's work counter (2 ints, zero between launches)
     const void *tmap_base;       // fpad the descriptor was built for
     int num_sms;
 

@@ -5,17 +5,22 @@
 // PART_HISTORY_FVP (553-595), PART_HISTORY_FDP (599-625), PART_ADVANCE (629-726),
 // UPDATE_PART_POSITION (730-757), the wrap of PERIODIC (1142-1151) and MEAN_VEL (1889-1980).
 //
-// Design (B200): droplets are kept sorted by "brick" (a BX x BY x BZ block of grid cells).
-// One CTA handles one brick: it stages the brick's field region plus the 6-point stencil
-// halo (2 cells below, 3 above) in shared memory with coalesced loads, then evaluates the
-// 216-point stencil of every (droplet, component) task out of shared memory.  Tasks are
-// grouped so that the 32 (FP32) or 16 (FP64 half-warp) lanes of a group start their
-// stencils in distinct shared-memory banks, which makes every stencil load
-// conflict-free.  The FP64 path sums in the reference's order (x outer, y, z inner,
-// vp = vp + v*bx*by*bz, no FMA contraction) and is bit-identical to the CPU restatement;
-// the mixed path evaluates the same tensor-product sum separably in FP32 with FMA.
-// A droplet that has drifted out of its brick since the last re-sort is evaluated from
-// global memory with the same arithmetic.
+// Design (B200):
+// * Mixed precision (k_interp_col): droplets are kept sorted by (column of 16 x 16 cells,
+//   z plane); each CTA sweeps work items (a column over a range of planes) in z, the field
+//   streaming through a ring of shared-memory slabs (four planes, three components, one
+//   TMA box each), with warp-specialised producer, prep, stencil and release warps.  The
+//   stencil warps evaluate the 216-point stencil of every (droplet, component) task out of
+//   shared memory in rounds of 32 tasks that start in 32 distinct banks, so every load is
+//   conflict-free; the FP32 tensor-product sum is taken separably with FMA.
+// * FP64 (k_interp): droplets are kept sorted by brick (a BX x BY x BZ block of cells).  One
+//   CTA handles one brick at a time: it stages the brick's field region plus the 6-point
+//   stencil halo in shared memory with TMA and evaluates the tasks in half-warp groups that
+//   start in distinct banks.  The sum is taken in the reference's order (x outer, y, z
+//   inner, vp = vp + v*bx*by*bz, no FMA contraction), bit-identical to the CPU restatement.
+// A droplet whose stencil is not inside the staged field (it drifted beyond the margins
+// since the last re-sort) is evaluated from the padded field in global memory with the same
+// arithmetic.
 #include "dl_internal.cuh"
 
 #include <algorithm>
@@ -128,6 +133,9 @@ struct InterpArgs {
     const T *fpad;
     int64_t fpy, fpz, fpc;
     int comp_lo, ncomp;             // components evaluated by this launch
+    int zseg, zbatch;               // column sweep: z planes per work item and per batch
+    int nband, band[17];            // column sweep: z bands of the work items (band[nband] = n)
+    int *work;                      // column sweep: [0] next work item, [1] CTAs done fetching
     // outputs (non-fused): vp
     T *vp[3];
     // fused advance
@@ -154,11 +162,6 @@ template <>
 struct Elems<double> {
     static constexpr int R = 16;
     static constexpr int LANES = 16;
-};
-template <>
-struct Elems<float> {
-    static constexpr int R = 32;
-    static constexpr int LANES = 32;
 };
 
 // Field tile of one component of one brick, as one TMA box.  Component c's box starts
@@ -614,6 +617,435 @@ __global__ void __launch_bounds__((NG * GW + 1) * 32, 1) k_interp(const __grid_c
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Column sweep (mixed precision).  The device order is sorted by (column, z plane), a
+// column being CX x CY cells in x-y.  The work items are (column, segment of zseg planes);
+// each CTA sweeps its items in z:
+//  * the producer warp streams the field through a ring of NSL slabs, a slab being four
+//    consecutive planes of the item's column plus the stencil halo, all three components,
+//    in one TMA box (a TMA copy costs about the same issue time whatever its size, so the
+//    boxes are made large);
+//  * prep warps (batches go round them) take the droplets of PZ consecutive planes at a
+//    time (a batch, at most MAXD droplets), compute their nodes, fractions and stencil
+//    corners, and sort the (droplet, component) tasks into 32 buckets by the shared-memory
+//    bank their stencil starts in;
+//  * NSW stencil warps wait for the slabs of a batch's window, then take rounds of its
+//    buckets (lane r evaluates the round's task of bucket r, so each of the round's 216
+//    shared-memory loads is conflict-free, and stores the result) until the batch has none
+//    left, and move on to the next batch without a block barrier;
+//  * a release warp hands the slabs no finished batch needs any more back to the producer
+//    and the batch slot back to the prep warps.
+// Each plane of an item enters shared memory once; only the 3 + 3 halo planes at the ends
+// of an item (and up to three padding planes that round it to whole slabs) are extra.
+// Droplets whose stencil is not inside the staged planes (drifted further than the
+// margins since the last sort) are evaluated by the prep warp from the padded field in
+// global memory with the same arithmetic.
+//
+// Slab layout in shared memory: [plane 0..3][component][y][x] (the tensor map orders the
+// field's dimensions x, y, component, z).  With BOX = EX * EY floats per component plane
+// and PS = ncomp * BOX per plane, BOX = 8 (mod 32) and PS = 24 (mod 32) for three
+// components, 8 for one, and 4 * PS = 0 (mod 32): plane u of the sweep starts at bank
+// PS * u (mod 32) whatever slab slot holds it, so the bank of a stencil's start plus
+// PS * k is the bank of its plane k, the same shift for every lane of a round.
+// ---------------------------------------------------------------------------------------
+namespace colk {
+constexpr int CX = 16, CY = 16;                  // column cross-section (cells)
+constexpr int M = 1;                             // y drift tolerated since the last sort (cells)
+constexpr int EX = CX + 8;                       // tile row: x from cx*CX - 4 (16-byte aligned x)
+constexpr int EY = CY + 5 + 2 * M;               // rows: y from cy*CY - 3
+constexpr int BOX = EX * EY;                     // floats of one component plane
+constexpr int SPL = 4;                           // planes per slab (one TMA box)
+constexpr int SLAB = SPL * 3 * BOX;              // floats of a slab (three components)
+constexpr int CAP = 32;                          // tasks per bank bucket (more go to the overflow list)
+constexpr int NPROD = 1;                         // producer warps (slab j goes to producer j % NPROD)
+constexpr int NPREP = 3;                         // prep warps (batches go round them)
+static_assert(BOX % 32 == 8 && (3 * BOX) % 32 == 24 && (SPL * 3 * BOX) % 32 == 0 && (SPL * BOX) % 32 == 0,
+              "slab bank pattern");
+static_assert((SLAB * 4) % 128 == 0 && (SPL * BOX * 4) % 128 == 0, "slab slots keep 128-byte alignment");
+}  // namespace colk
+
+template <int MAXD>
+struct ColBatch {   // per-batch shared-memory area
+    float4 fr[MAXD];                          // x, y, z fractions; w: corner | first plane << 12 (or -1)
+    int meta[16];   // d0, nd, full rounds, overflow tasks, release lo, hi, end, next round, window end
+    int cnt[32];                              // tasks per bucket
+    unsigned short task[32 * colk::CAP];      // bucketed tasks: droplet << 2 | component slot
+    unsigned short ovf[MAXD * 3];             // overflow tasks
+};
+
+template <int NSL, int MAXD, int NP>
+constexpr size_t col_smem()
+{
+    return (size_t)NSL * colk::SLAB * 4 + ((size_t)(2 * NSL + 3 * NP) * 8 + 127) / 128 * 128 +
+           (size_t)NP * ((sizeof(ColBatch<MAXD>) + 127) / 128 * 128);
+}
+
+// 6x6x6 FP32 stencil, planes outermost: acc = sum_k bz[k] sum_b by[b] sum_a bx[a] v(a, b, k)
+template <class L>
+__device__ __forceinline__ float stencil_planes(const L &ld, const float *bx, const float *by, const float *bz)
+{
+    float acc = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+        float t = 0.0f;
+#pragma unroll
+        for (int b = 0; b < 6; b++) {
+            float s = 0.0f;
+#pragma unroll
+            for (int a = 0; a < 6; a++) s = fmaf(ld(a, b, k), bx[a], s);
+            t = fmaf(s, by[b], t);
+        }
+        acc = fmaf(t, bz[k], acc);
+    }
+    return acc;
+}
+
+struct RingLoader {
+    const float *pl[6];   // stencil corner in each of the six planes
+    __device__ __forceinline__ float operator()(int a, int b, int k) const { return pl[k][b * colk::EX + a]; }
+};
+
+template <int NSL, int MAXD, int NP, int NSW>
+__global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
+    k_interp_col(const __grid_constant__ CUtensorMap tmap, InterpArgs<float> A)
+{
+    using namespace colk;
+    using B = ColBatch<MAXD>;
+    static_assert(NSL % NPROD == 0, "a slab slot always belongs to the same producer");
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    float *ring = reinterpret_cast<float *>(smem_raw);
+    unsigned long long *full = reinterpret_cast<unsigned long long *>(smem_raw + (size_t)NSL * SLAB * 4);
+    unsigned long long *empty = full + NSL;
+    unsigned long long *ready = empty + NSL;
+    unsigned long long *done = ready + NP;
+    unsigned long long *freep = done + NP;
+    unsigned char *bbase = smem_raw + (size_t)NSL * SLAB * 4 + ((size_t)(2 * NSL + 3 * NP) * 8 + 127) / 128 * 128;
+    constexpr size_t BSZ = (sizeof(B) + 127) / 128 * 128;
+    auto batch = [&](int p) { return reinterpret_cast<B *>(bbase + (size_t)p * BSZ); };
+    __shared__ int sabort;
+    constexpr int QI = 4;             // work-item queue between the producer and the prep warps
+    __shared__ int s_item[QI];
+    __shared__ int s_qn, s_qend;      // items published; items of this CTA (-1 until known)
+    __shared__ int s_qpos[NPREP];     // items each prep warp has taken from the queue
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n = A.n, ncx = A.nbx, ncol = A.nbx * A.nby;
+    const int ncomp = A.ncomp, clo = A.comp_lo;
+    const int PS = ncomp * BOX;                       // floats per plane in a slab
+    const int SLABF = SPL * PS;                       // floats of a slab actually used
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NSL; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        for (int p = 0; p < NP; p++) {
+            mbar_init(&ready[p], 1);
+            mbar_init(&done[p], NSW);
+            mbar_init(&freep[p], 1);
+        }
+        sabort = 0;
+        s_qn = 0;
+        s_qend = -1;
+        for (int w = 0; w < NPREP; w++) s_qpos[w] = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+
+    // Work items: (column, segment of zseg planes), numbered column fastest and handed out
+    // in that order by a global counter (the producer of each CTA takes the next item when
+    // it needs one), so the CTAs sweep neighbouring columns over the same z range at about
+    // the same time (the halo rows two columns share are read from DRAM once, through L2)
+    // and an SM that runs slower takes fewer items.  An item's planes za - 3 .. zb + 3 are
+    // padded to whole slabs.
+    const int nitems = ncol * A.nband;
+    const int PZ = A.zbatch;   // planes per batch
+    auto item_z = [&](int it, int &za, int &zb) { const int bd = it / ncol; za = A.band[bd]; zb = A.band[bd + 1]; };
+    auto seg_planes = [](int za, int zb) { return (zb - za + 7 + SPL - 1) / SPL * SPL; };
+    auto aborted = [&]() { return *(volatile int *)&sabort != 0; };
+    auto fail = [&]() {
+        atomicOr(A.err, DL_DERR_TMA_TIMEOUT);
+        *(volatile int *)&sabort = 1;
+    };
+
+    if (warp >= NSW && warp < NSW + NPROD) {
+        // ================= producers: slab j of the sweep goes to producer j % NPROD =================
+        const int pw = warp - NSW;
+        static_assert(NPROD == 1, "one producer takes the work items");
+        if (lane == 0) {
+            unsigned j = 0;   // slab index in the sweep
+            bool ok = true;
+            const int c0 = ncomp == 3 ? 0 : clo;   // first component of the box
+            int qn = 0;
+            bool more = true;
+            // takes the next work item and hands it to the prep warps (false at the end)
+            auto publish = [&]() -> bool {
+                if (!more) return false;
+                if (qn >= QI) {   // the queue slot is free once every prep warp has read it
+                    bool freed = false;
+                    for (int i = 0; i < (1 << 22) && !aborted(); i++) {
+                        int mn = 1 << 30;
+                        for (int w = 0; w < NPREP; w++) mn = min(mn, *(volatile int *)&s_qpos[w]);
+                        if (mn > qn - QI) { freed = true; break; }
+                        __nanosleep(64);
+                    }
+                    if (!freed) { fail(); more = false; return false; }
+                }
+                const int it = atomicAdd(&A.work[0], 1);
+                if (it >= nitems) {
+                    more = false;
+                    *(volatile int *)&s_qend = qn;
+                    return false;
+                }
+                *(volatile int *)&s_item[qn % QI] = it;
+                __threadfence_block();
+                *(volatile int *)&s_qn = qn + 1;
+                qn++;
+                return true;
+            };
+            publish();
+            for (int q = 0; q < qn && ok; q++) {
+                const int it = *(volatile int *)&s_item[q % QI];
+                int za, zb;
+                item_z(it, za, zb);
+                const int col = it % ncol;
+                const int cx = col % ncx, cy = col / ncx;
+                const int nsl = seg_planes(za, zb) / SPL;
+                for (int k = 0; k < nsl && ok; k++, j++) {
+                    // the next item is taken when this one's last slab is issued: late enough
+                    // that a CTA holds at most one item it has not started when the items run
+                    // out, early enough for the prep warps, which work behind the producer
+                    if (k == nsl - 1) publish();
+                    if ((int)(j % NPROD) != pw) continue;
+                    const int s = j % NSL;
+                    if (j >= (unsigned)NSL && !mbar_wait(&empty[s], ((j / NSL) - 1) & 1)) { fail(); ok = false; break; }
+                    if (aborted()) { ok = false; break; }
+                    mbar_arrive_expect_tx(&full[s], (unsigned)(SLABF * 4));
+                    // padded coordinates (grid + DL_PAD_LO) of the box origin: x, y, component, z
+                    tma_load_4d(ring + (size_t)s * SLAB, &tmap, &full[s], cx * CX, cy * CY + DL_PAD_LO - 3, c0,
+                                za - 3 + SPL * k + DL_PAD_LO);
+                }
+            }
+            if (more) {   // stopped early: the prep warps see the end of the queue
+                more = false;
+                *(volatile int *)&s_qend = qn;
+            }
+            // this producer's copies still in flight land before the CTA may leave (bounded waits)
+            for (unsigned q = (j > (unsigned)NSL ? j - NSL : 0u); q < j; q++)
+                if ((int)(q % NPROD) == pw) mbar_wait(&full[q % NSL], (q / NSL) & 1);
+            // the last CTA done taking items resets the counter for the next launch
+            __threadfence();
+            if (atomicAdd(&A.work[1], 1) == (int)gridDim.x - 1) {
+                atomicExch(&A.work[0], 0);
+                atomicExch(&A.work[1], 0);
+            }
+        }
+        return;
+    }
+
+    if (warp == NSW + NPROD) {
+        // ================= release =================
+        if (lane == 0) {
+            unsigned jr = 0;   // next slab to release
+            for (int b = 0;; b++) {
+                const int p = b % NP;
+                B *S = batch(p);
+                if (!mbar_wait(&done[p], (b / NP) & 1)) { fail(); return; }
+                if (S->meta[6]) return;
+                // slabs every plane of which lies below the release bound
+                const unsigned rel_hi = (unsigned)S->meta[5];
+                for (; (jr + 1) * SPL <= rel_hi; jr++) mbar_arrive(&empty[jr % NSL]);
+                mbar_arrive(&freep[p]);
+                if (aborted()) return;
+            }
+        }
+        return;
+    }
+
+    if (warp > NSW + NPROD) {
+        // ================= prep (batches go round the prep warps) =================
+        const int pw = warp - NSW - NPROD - 1;
+        int b = 0;
+        unsigned useg = 0;
+        auto take = [&](int bb) -> bool {   // wait until batch slot bb % NP is free again
+            if (bb < NP) return true;
+            return mbar_wait(&freep[bb % NP], ((bb / NP) - 1) & 1);
+        };
+        for (int q = 0;; q++) {
+            // the next work item from the producer's queue
+            bool have = false;
+            for (int i = 0; i < (1 << 22) && !aborted(); i++) {
+                if (*(volatile int *)&s_qn > q) { have = true; break; }
+                const int qe = *(volatile int *)&s_qend;
+                if (qe >= 0 && q >= qe) break;
+                __nanosleep(64);
+            }
+            if (!have) {
+                if (*(volatile int *)&s_qend < 0 && !aborted()) { fail(); return; }
+                break;
+            }
+            const int it = *(volatile int *)&s_item[q % QI];
+            __syncwarp();
+            if (lane == 0) *(volatile int *)&s_qpos[pw] = q + 1;
+            int za, zb;
+            item_z(it, za, zb);
+            const int col = it % ncol;
+            const int cx = col % ncx, cy = col / ncx;
+            const unsigned npl = (unsigned)seg_planes(za, zb);
+            for (int zp = za; zp < zb; zp += PZ) {
+                const int zq = min(zp + PZ, zb);
+                const int kd0 = A.brick_start[col * n + zp], kd1 = A.brick_start[col * n + zq];
+                const unsigned uhi = useg + (unsigned)(zq - za) + 6u;   // last plane of the window
+                // planes no later batch needs: up to the next batch's window, or the item's end
+                const int rel_hi = (int)(zq < zb ? useg + (unsigned)(zq - za) : useg + npl);
+                for (int d0 = kd0, first = 1; first || d0 < kd1; d0 += MAXD, first = 0, b++) {
+                    if (b % NPREP != pw) continue;
+                    const int nd = max(0, min(MAXD, kd1 - d0));
+                    const bool last = d0 + MAXD >= kd1;
+                    const int p = b % NP;
+                    B *S = batch(p);
+                    // the batch's positions are requested before the slot is taken
+                    constexpr int QN = (MAXD + 31) / 32;
+                    double P[QN][3];
+#pragma unroll
+                    for (int q = 0; q < QN; q++) {
+                        const int i = q * 32 + lane;
+                        if (i < nd) { P[q][0] = A.px[d0 + i]; P[q][1] = A.py[d0 + i]; P[q][2] = A.pz[d0 + i]; }
+                    }
+                    if (!take(b)) { fail(); return; }
+                    if (aborted()) return;
+                    S->cnt[lane] = 0;
+                    if (lane == 0) S->meta[3] = 0;
+                    __syncwarp();
+                    // nodes, fractions and corners; each task goes into the bucket of the bank
+                    // its stencil starts in (a task's value does not depend on its slot)
+#pragma unroll
+                    for (int q = 0; q < QN; q++) {
+                        const int i = q * 32 + lane;
+                        if (i >= nd) continue;
+                        int node[3];
+                        float fr[3];
+#pragma unroll
+                        for (int a = 0; a < 3; a++) {
+                            const double t = P[q][a] * A.inv_dx;
+                            node[a] = (int)floor(t);
+                            fr[a] = (float)(t - (double)node[a]);
+                        }
+                        // a droplet that crossed a face of the periodic box since the last sort
+                        // keeps its place in the order: its periodic image (node +- n) lies in
+                        // the staged halo of the padded field
+                        int lx = node[0] - cx * CX + 2, ly = node[1] - cy * CY + 1, nz = node[2];
+                        if (lx < 0) lx += n; else if (lx + 5 >= EX) lx -= n;
+                        if (ly < 0) ly += n; else if (ly + 5 >= EY) ly -= n;
+                        if (nz < zp - 1) nz += n; else if (nz > zq) nz -= n;
+                        const bool in = lx >= 0 && lx + 5 < EX && ly >= 0 && ly + 5 < EY && nz >= zp - 1 && nz <= zq;
+                        int co = -1;
+                        if (in) {
+                            const unsigned u0 = useg + (unsigned)(nz - 2 - (za - 3));   // plane of the corner
+                            const int corner = ly * EX + lx;
+                            co = corner | (int)(u0 << 12);
+                            for (int cc = 0; cc < ncomp; cc++) {
+                                const int key = (corner + cc * BOX + PS * (int)(u0 & 3u)) & 31;
+                                const unsigned short tk = (unsigned short)((i << 2) | cc);
+                                const int slot = atomicAdd(&S->cnt[key], 1);
+                                if (slot < CAP) S->task[key * CAP + slot] = tk;
+                                else S->ovf[atomicAdd(&S->meta[3], 1)] = tk;
+                            }
+                        } else {
+                            // outside the staged planes: the padded field in global memory
+                            float bx[6], by[6], bz[6];
+                            lagrange6(fr[0], bx);
+                            lagrange6(fr[1], by);
+                            lagrange6(fr[2], bz);
+                            const int x0 = wrapi(node[0], n) - 2 + DL_PAD_LO;
+                            const int y0 = wrapi(node[1], n) - 2 + DL_PAD_LO;
+                            const int z0 = wrapi(node[2], n) - 2 + DL_PAD_LO;
+                            for (int cc = 0; cc < ncomp; cc++) {
+                                GlobalLoaderPad<float> ld;
+                                ld.f = A.fpad + (clo + cc) * A.fpc + x0 + A.fpy * y0 + A.fpz * z0;
+                                ld.py = A.fpy;
+                                ld.pz = A.fpz;
+                                A.vp[clo + cc][d0 + i] = stencil_planes(ld, bx, by, bz);
+                            }
+                        }
+                        S->fr[i] = make_float4(fr[0], fr[1], fr[2], __int_as_float(co));
+                    }
+                    __syncwarp();
+                    int nrf = min(S->cnt[lane], CAP);
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) nrf = max(nrf, __shfl_xor_sync(0xffffffffu, nrf, o));
+                    if (lane == 0) {
+                        S->meta[0] = d0; S->meta[1] = nd; S->meta[2] = nrf;
+                        S->meta[5] = last ? rel_hi : 0;
+                        S->meta[6] = 0;
+                        S->meta[7] = 0;
+                        S->meta[8] = (int)uhi;   // last plane of the batch's window
+                    }
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&ready[p]);
+                }
+            }
+            useg += npl;
+        }
+        // end marker in the slot after the last batch (the prep warp that owns it)
+        if (b % NPREP == pw) {
+            const int p = b % NP;
+            B *S = batch(p);
+            if (!take(b)) { fail(); return; }
+            if (lane == 0) { S->meta[6] = 1; S->meta[1] = 0; S->meta[5] = 0; mbar_arrive(&ready[p]); }
+        }
+        return;
+    }
+
+    // ================= stencil warps =================
+    unsigned jw = 0;   // next slab this warp waits for (slabs are waited in order)
+    for (int b = 0;; b++) {
+        const int p = b % NP;
+        B *S = batch(p);
+        if (!mbar_wait(&ready[p], (b / NP) & 1)) { fail(); return; }
+        if (S->meta[6]) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&done[p]);
+            return;
+        }
+        // the slabs of the batch's window have landed.  Every earlier slab of the sweep was
+        // waited for by this warp, so the slot's barrier is in this slab's phase.
+        for (const unsigned jhi = (unsigned)S->meta[8] / SPL; jw <= jhi; jw++)
+            if (!mbar_wait(&full[jw % NSL], (jw / NSL) & 1)) { fail(); return; }
+        const int nrf = S->meta[2], novf = S->meta[3], d0 = S->meta[0];
+        const int total = nrf + (novf + 31) / 32;
+        const int mycnt = min(S->cnt[lane], CAP);
+        for (;;) {
+            int g = 0;
+            if (lane == 0) g = atomicAdd(&S->meta[7], 1);
+            g = __shfl_sync(0xffffffffu, g, 0);
+            if (g >= total) break;
+            int t = -1;
+            if (g < nrf) {
+                if (g < mycnt) t = S->task[lane * CAP + g];
+            } else {
+                const int q = (g - nrf) * 32 + lane;
+                if (q < novf) t = S->ovf[q];
+            }
+            if (t >= 0) {
+                const int i = t >> 2, cc = t & 3;
+                const float4 f = S->fr[i];
+                const int co = __float_as_int(f.w);
+                float bx[6], by[6], bz[6];
+                lagrange6(f.x, bx);
+                lagrange6(f.y, by);
+                lagrange6(f.z, bz);
+                RingLoader ld;
+                const int off = cc * BOX + (co & 0xfff);
+                unsigned u = (unsigned)co >> 12;
+#pragma unroll
+                for (int k = 0; k < 6; k++, u++)
+                    ld.pl[k] = ring + (size_t)((u / SPL) % NSL) * SLAB + (u % SPL) * PS + off;
+                A.vp[clo + cc][d0 + i] = stencil_planes(ld, bx, by, bz);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&done[p]);
+        if (aborted()) return;
+    }
+}
+
 template <typename T, int BX, int BY, int BZ, int XS, int YS, int M, int S, int MAXD, int NG>
 constexpr size_t interp_smem()
 {
@@ -624,9 +1056,11 @@ constexpr size_t interp_smem()
 // ---------------------------------------------------------------------------------------
 // Brick sort of the device order
 // ---------------------------------------------------------------------------------------
+// Sort key of a droplet: its brick, bricks numbered x fastest then y then z; with
+// colmajor (bz = 1: columns of bx x by cells) the key is (column, z plane), planes fastest.
 __global__ void k_brick_keys(int nps, const double *px, const double *py, const double *pz, double dx, int n,
-                             int bx, int by, int bz, int nbx, int nby, int *keys, int *cnt, const double *rad,
-                             int dead_key)
+                             int bx, int by, int bz, int nbx, int nby, int nbz, int colmajor, int *keys, int *cnt,
+                             const double *rad, int dead_key)
 {
     int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= nps) return;
@@ -639,7 +1073,8 @@ __global__ void k_brick_keys(int nps, const double *px, const double *py, const 
     ix = min(max(ix, 0), n - 1);
     iy = min(max(iy, 0), n - 1);
     iz = min(max(iz, 0), n - 1);
-    int key = ((iz / bz) * nby + (iy / by)) * nbx + (ix / bx);
+    const int key = colmajor ? ((iy / by) * nbx + (ix / bx)) * nbz + (iz / bz)
+                             : ((iz / bz) * nby + (iy / by)) * nbx + (ix / bx);
     keys[d] = key;
     atomicAdd(&cnt[key], 1);
 }
@@ -912,8 +1347,11 @@ __global__ void k_mean_vel(int nps, const T *ux, const T *uy, const T *uz, const
 
 // brick / pipeline configuration per precision: brick cells, component shifts (bank
 // spreading), TMA stages, droplets per chunk, consumer groups x warps per group
-constexpr int F32_BX = 16, F32_BY = 16, F32_BZ = 6, F32_XS = 0, F32_YS = 1, F32_M = 1, F32_S = 6, F32_MAXD = 256;
-constexpr int F32_NG = 2, F32_GW = 6;
+// mixed precision: column sweep (columns of colk::CX x colk::CY cells), ring of COL_NSL
+// slabs of colk::SPL planes, batches of COL_PZ planes (three consecutive batch windows of
+// COL_PZ + 7 planes fit the ring) and at most COL_MAXD droplets, COL_NP batch slots,
+// COL_NSW stencil warps
+constexpr int COL_NSL = 7, COL_PZ = 8, COL_MAXD = 160, COL_NP = 3, COL_NSW = 11;
 constexpr int F64_BX = 8, F64_BY = 8, F64_BZ = 8, F64_XS = 2, F64_YS = 0, F64_M = 1, F64_S = 5, F64_MAXD = 64;
 constexpr int F64_NG = 2, F64_GW = 6;
 
@@ -939,8 +1377,8 @@ int launch_brick_sort(dl_ctx *c)
     DL_CUDA(c, cudaMemsetAsync(c->brick_cnt, 0, sizeof(int) * nkeys, c->stream));
     const double *P[3] = {c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2]};
     k_brick_keys<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, P[0], P[1], P[2], c->dc.dx, c->dc.n, c->bx, c->by,
-                                                         c->bz, c->nbx, c->nby, c->keys, c->brick_cnt, c->rad,
-                                                         c->has_dead ? c->nbricks : -1);
+                                                         c->bz, c->nbx, c->nby, c->nbz, c->mixed, c->keys,
+                                                         c->brick_cnt, c->rad, c->has_dead ? c->nbricks : -1);
     DL_CHECK_LAUNCH(c);
     k_scan_single<<<1, 1024, 0, c->stream>>>(c->brick_cnt, c->brick_start, nkeys);
     DL_CHECK_LAUNCH(c);
@@ -991,8 +1429,8 @@ int launch_brick_sort(dl_ctx *c)
     return 0;
 }
 
-// TMA descriptor of the halo-padded field: 4D (x, y, z, component), box = one component tile
-static int make_tmap(dl_ctx *c, int box_x, int box_y, int box_z)
+// TMA descriptor of the halo-padded field: 4D (x, y, z, component), box = box_c component tiles
+static int make_tmap(dl_ctx *c, CUtensorMap *map, int box_x, int box_y, int box_z, int box_c = 1)
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
@@ -1007,14 +1445,40 @@ static int make_tmap(dl_ctx *c, int box_x, int box_y, int box_z)
     const cuuint64_t es = c->esz;
     cuuint64_t dims[4] = {(cuuint64_t)c->fp_pitch, e, e, 3};
     cuuint64_t strides[3] = {(cuuint64_t)c->fp_pitch * es, (cuuint64_t)c->fp_plane * es, (cuuint64_t)c->fp_comp * es};
-    cuuint32_t box[4] = {(cuuint32_t)box_x, (cuuint32_t)box_y, (cuuint32_t)box_z, 1};
+    cuuint32_t box[4] = {(cuuint32_t)box_x, (cuuint32_t)box_y, (cuuint32_t)box_z, (cuuint32_t)box_c};
     cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = encode(&c->tmap, c->mixed ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
+    CUresult r = encode(map, c->mixed ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
                         c->fpad, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return dl_fail(c, DL_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
-    c->tmap_base = c->fpad;
+    return 0;
+}
+
+// TMA descriptor of the FP32 halo-padded field with the dimensions ordered x, y, component,
+// z (strides need not grow with the dimension), so that a box of several planes lands in
+// shared memory as [plane][component][y][x]
+static int make_tmap_zc(dl_ctx *c, CUtensorMap *map, int box_x, int box_y, int box_c, int box_z)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        DL_CUDA(c, cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        if (!fn || q != cudaDriverEntryPointSuccess)
+            return dl_fail(c, DL_E_CUDA, "cuTensorMapEncodeTiled not available");
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    const cuuint64_t e = (cuuint64_t)c->dc.n + DL_PAD_LO + DL_PAD_HI;
+    const cuuint64_t es = c->esz;
+    cuuint64_t dims[4] = {(cuuint64_t)c->fp_pitch, e, 3, e};
+    cuuint64_t strides[3] = {(cuuint64_t)c->fp_pitch * es, (cuuint64_t)c->fp_comp * es, (cuuint64_t)c->fp_plane * es};
+    cuuint32_t box[4] = {(cuuint32_t)box_x, (cuuint32_t)box_y, (cuuint32_t)box_c, (cuuint32_t)box_z};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, c->fpad, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return dl_fail(c, DL_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
     return 0;
 }
 
@@ -1023,8 +1487,9 @@ static int launch_interp_t(dl_ctx *c, int comp_lo, int ncomp, int fused)
 {
     using G = Geo<T, BX, BY, BZ, XS, YS, M>;
     if (c->tmap_base != c->fpad) {
-        int r = make_tmap(c, G::EX, G::EY, G::EZ);
+        int r = make_tmap(c, &c->tmap, G::EX, G::EY, G::EZ);
         if (r) return r;
+        c->tmap_base = c->fpad;
     }
     InterpArgs<T> A;
     memset(&A, 0, sizeof(A));
@@ -1096,20 +1561,116 @@ static int launch_interp_t(dl_ctx *c, int comp_lo, int ncomp, int fused)
     return 0;
 }
 
+static int launch_interp_col(dl_ctx *c, int comp_lo, int ncomp, int fused)
+{
+    if (c->tmap_base != c->fpad) {
+        // one box per slab: colk::SPL planes of all three components, or of the single
+        // component of a one-component INTERPOLATE call; dimensions ordered x, y, component, z
+        int r = make_tmap_zc(c, &c->tmap, colk::EX, colk::EY, 3, colk::SPL);
+        if (!r) r = make_tmap_zc(c, &c->tmap1, colk::EX, colk::EY, 1, colk::SPL);
+        if (r) return r;
+        c->tmap_base = c->fpad;
+    }
+    InterpArgs<float> A;
+    memset(&A, 0, sizeof(A));
+    A.n = c->dc.n;
+    A.nps = c->nps;
+    A.dx = c->dc.dx;
+    A.inv_dx = 1.0 / c->dc.dx;
+    A.pi2 = c->dc.pi2;
+    A.px = c->pos[c->pcur][0]; A.py = c->pos[c->pcur][1]; A.pz = c->pos[c->pcur][2];
+    A.brick_start = c->brick_start;
+    A.nbx = c->nbx; A.nby = c->nby; A.nbricks = c->nbricks;
+    A.fpad = tp<float>(c->fpad);
+    A.fpy = c->fp_pitch;
+    A.fpz = c->fp_plane;
+    A.fpc = c->fp_comp;
+    for (int k = 0; k < 3; k++) A.vp[k] = tp<float>(c->vpv[k]);
+    if (fused)   // the interpolated velocity goes straight into fdp(:,0) = F[fnew]
+        for (int k = 0; k < 3; k++) A.vp[k] = tp<float>(c->flu[(c->fcur + 3) % 4][k]);
+    A.comp_lo = comp_lo;
+    A.ncomp = ncomp;
+    A.err = c->d_err;
+    A.work = c->col_work;
+    // z bands of the work items: nzs equal bands (the number that minimises the planes per
+    // CTA, halo included, plus one item of tail), the last of them cut into four thinner
+    // bands, so the items handed out last, when the CTAs finish at different times, are small
+    {
+        const int n = c->dc.n, ncol = c->nbx * c->nby, grid = c->num_sms;
+        int64_t best = -1;
+        int nzs = 1;
+        for (int k = 1; k <= std::min(n, 12); k++) {
+            const int zs = (n + k - 1) / k;
+            const int64_t cost = ((int64_t)ncol * k * (zs + 8) + grid - 1) / grid + (zs + 8);
+            if (best < 0 || cost < best) { best = cost; nzs = k; A.zseg = zs; }
+        }
+        int nb = 0;
+        for (int k = 0; k < nzs - 1; k++) A.band[nb++] = std::min(n, k * A.zseg);
+        const int z0 = (nzs - 1) * A.zseg, rest = n - z0;
+        const int nthin = rest >= 4 * COL_PZ ? 4 : 1;
+        for (int k = 0; k < nthin; k++) A.band[nb++] = z0 + (int)((int64_t)rest * k / nthin);
+        A.band[nb] = n;
+        A.nband = nb;
+        A.zbatch = COL_PZ;
+    }
+    constexpr size_t sm = col_smem<COL_NSL, COL_MAXD, COL_NP>();
+    static_assert(sm + 64 <= 227 * 1024, "shared memory budget");
+    auto kern = k_interp_col<COL_NSL, COL_MAXD, COL_NP, COL_NSW>;
+    DL_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const int grid = c->num_sms;
+    kern<<<grid, (COL_NSW + colk::NPROD + 1 + colk::NPREP) * 32, sm, c->stream>>>(ncomp == 3 ? c->tmap : c->tmap1, A);
+    DL_CHECK_LAUNCH(c);
+    if (fused) {
+        // the advance epilogue: history, drag, position update, wrap, departure flags
+        InterpArgs<float> E = A;
+        E.fused = 1;
+        E.first = c->new_particle;
+        E.init_mode = c->p.init_velocity;
+        E.ndrag = c->dc.ndrag;
+        E.dt = (float)c->dc.dt; E.tau2 = (float)c->dc.tau2; E.sv = (float)c->dc.sv; E.rnu = (float)c->dc.rnu;
+        E.rad = c->rad;
+        c->vnew = (c->vcur + 3) % 4;
+        c->fnew = (c->fcur + 3) % 4;
+        for (int k = 0; k < 3; k++) {
+            E.v0[k] = tp<float>(c->vel[c->vcur][k]);
+            E.v1[k] = tp<float>(c->vel[(c->vcur + 1) % 4][k]);
+            E.v2[k] = tp<float>(c->vel[(c->vcur + 2) % 4][k]);
+            E.vnew[k] = tp<float>(c->vel[c->vnew][k]);
+            E.f1[k] = tp<float>(c->flu[c->fcur][k]);
+            E.f2[k] = tp<float>(c->flu[(c->fcur + 1) % 4][k]);
+            E.f3[k] = tp<float>(c->flu[(c->fcur + 2) % 4][k]);
+            E.fnew[k] = tp<float>(c->flu[c->fnew][k]);
+            E.dmv[k] = tp<float>(c->dmv[k]);
+        }
+        E.qx = c->pos[1 - c->pcur][0]; E.qy = c->pos[1 - c->pcur][1]; E.qz = c->pos[1 - c->pcur][2];
+        E.ref_of_dev = c->ref_of_dev;
+        E.leave_nid = c->leave_nid;
+        E.lv_list = c->lv_list;
+        E.lv_n = c->lv_n;
+        static bool carve = false;
+        if (!carve) {
+            cudaFuncSetAttribute(k_advance_fused<float>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+            carve = true;
+        }
+        k_advance_fused<float><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(E);
+        DL_CHECK_LAUNCH(c);
+    }
+    return 0;
+}
+
 int launch_interp(dl_ctx *c, int icpt, int fused)
 {
     if (c->nps == 0) return 0;
     int lo = icpt > 0 ? icpt - 1 : 0, nc = icpt > 0 ? 1 : 3;
-    if (c->mixed)
-        return launch_interp_t<float, F32_BX, F32_BY, F32_BZ, F32_XS, F32_YS, F32_M, F32_S, F32_MAXD, F32_NG, F32_GW>(
-            c, lo, nc, fused);
+    if (c->mixed) return launch_interp_col(c, lo, nc, fused);
     return launch_interp_t<double, F64_BX, F64_BY, F64_BZ, F64_XS, F64_YS, F64_M, F64_S, F64_MAXD, F64_NG, F64_GW>(
         c, lo, nc, fused);
 }
 
 void dl_brick_dims(int mixed, int *bx, int *by, int *bz)
 {
-    if (mixed) { *bx = F32_BX; *by = F32_BY; *bz = F32_BZ; }
+    if (mixed) { *bx = colk::CX; *by = colk::CY; *bz = 1; }   // columns, sorted by z plane
     else { *bx = F64_BX; *by = F64_BY; *bz = F64_BZ; }
 }
 
