@@ -263,6 +263,10 @@ int dl_set_stream(dl_ctx *ctx, void *stream);
  * averaged over the steps since the last reset (CUDA events on the context's stream),
  * and the number of kernels the library launched in that span.  Synchronises. */
 int dl_timing(dl_ctx *ctx, int reset, double *avg_update_ms, int *nsteps, int64_t *kernel_launches);
+/* The same steps' time split into the interpolation kernel and the advance kernel (ms per
+ * step, averaged; the reference times INTERPOLATE and PART_ADVANCE separately, turb.f90:
+ * 734-755).  Synchronises; call before dl_timing resets the steps. */
+int dl_timing_split(dl_ctx *ctx, double *interp_ms, double *advance_ms);
 
 /* ---------------------------------------------------------------------------------------
  * Carrier flow: spectral Navier-Stokes step on the device (turb.f90:506-691)
@@ -288,6 +292,11 @@ int dl_flow_destroy(dl_flow *f);
 const char *dl_flow_last_error(const dl_flow *f);
 int dl_flow_set_stream(dl_flow *f, void *stream);
 int dl_flow_sync(dl_flow *f);
+/* Device time of the flow steps taken since the last call, averaged per step (ms): the
+ * cuFFT transforms and the update / cross-product kernels, timed with CUDA events when
+ * enabled (the reference times the flow step as a whole, turb.f90:734-755).  Returns
+ * the averages, then enables (1) or disables (0) the timing and resets it.  Synchronises. */
+int dl_flow_timing(dl_flow *f, int enable, double *fft_ms, double *kernel_ms, int *steps);
 /* new flow from a physical velocity (3 components in the INTERPOLATE layout v(llx, ly, lz),
  * component c at u + c * pitch_z * n), host or device: transform, projection, symmetrize,
  * dealiasing; N_old = u as the reference's new-flow start (turb.f90:452-454). */

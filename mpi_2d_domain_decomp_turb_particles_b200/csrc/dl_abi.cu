@@ -377,6 +377,7 @@ extern "C" int dl_create(const dl_params *p, dl_ctx **out)
     c->own_stream = c->stream;
     for (int i = 0; i < 8; i++) DL_CUDA(c, cudaEventCreate(&c->ev[i]));
     for (int i = 0; i < 2 * dl_ctx::NTEV; i++) DL_CUDA(c, cudaEventCreate(&c->tev[i]));
+    for (int i = 0; i < dl_ctx::NTEV; i++) DL_CUDA(c, cudaEventCreate(&c->tmid[i]));
     // defaults for capacities (single GPU: no MPI load imbalance to absorb)
     if (c->p.msize <= 0) c->p.msize = std::max(16, p->npart);
     if (c->p.ncollmax <= 0) c->p.ncollmax = std::max(100, p->npart / 100);
@@ -525,6 +526,8 @@ extern "C" int dl_destroy(dl_ctx *c)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     for (int i = 0; i < 2 * dl_ctx::NTEV; i++)
         if (c->tev[i]) cudaEventDestroy(c->tev[i]);
+    for (int i = 0; i < dl_ctx::NTEV; i++)
+        if (c->tmid[i]) cudaEventDestroy(c->tmid[i]);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return 0;
@@ -1311,15 +1314,43 @@ extern "C" int dl_timing(dl_ctx *c, int reset, double *avg_ms, int *nsteps, int6
     return 0;
 }
 
-// brackets the update kernels of one step with a pair of timing events
+extern "C" int dl_timing_split(dl_ctx *c, double *interp_ms, double *advance_ms)
+{
+    if (!c) return DL_E_ARG;
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));
+    const int m = std::min(c->ntev, (int)dl_ctx::NTEV);
+    double ti = 0.0, ta = 0.0;
+    for (int i = 0; i < m; i++) {
+        float a = 0.f, b = 0.f;
+        DL_CUDA(c, cudaEventElapsedTime(&a, c->tev[2 * i], c->tmid[i]));
+        DL_CUDA(c, cudaEventElapsedTime(&b, c->tmid[i], c->tev[2 * i + 1]));
+        ti += a;
+        ta += b;
+    }
+    if (interp_ms) *interp_ms = m ? ti / m : 0.0;
+    if (advance_ms) *advance_ms = m ? ta / m : 0.0;
+    return 0;
+}
+
+// brackets the update kernels of one step with a pair of timing events; the interpolation
+// launcher records the event between the interpolation and the advance (dl_mark_interp_end)
 static void timing_begin(dl_ctx *c)
 {
-    cudaEventRecord(c->tev[2 * (c->ntev % dl_ctx::NTEV)], c->stream);
+    const int k = c->ntev % dl_ctx::NTEV;
+    cudaEventRecord(c->tev[2 * k], c->stream);
+    cudaEventRecord(c->tmid[k], c->stream);   // replaced by the interpolation launcher
+    c->tev_open = 1;
 }
 static void timing_end(dl_ctx *c)
 {
     cudaEventRecord(c->tev[2 * (c->ntev % dl_ctx::NTEV) + 1], c->stream);
+    c->tev_open = 0;
     c->ntev++;
+}
+
+void dl_mark_interp_end(dl_ctx *c)
+{
+    if (c->tev_open) cudaEventRecord(c->tmid[c->ntev % dl_ctx::NTEV], c->stream);
 }
 
 extern "C" int dl_get_phase_times(dl_ctx *c, double *ms6)

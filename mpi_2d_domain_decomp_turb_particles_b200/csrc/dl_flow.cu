@@ -389,6 +389,11 @@ struct dl_flow {
     int iseedf = 0, iyf = 0, ivf[32];
     int64_t launches = 0;
     cudaEvent_t ev_ready = nullptr, ev_used = nullptr;   // ordering with a droplet context's stream
+    // optional step timing: five events per step (before the inverse transform, after it,
+    // after the cross product, after the forward transform, after the update kernels)
+    static const int NTS = 64;
+    cudaEvent_t tse[5 * NTS] = {};
+    int timing = 0, nts = 0;
     // DISSIP (allocated on first use): one-component inverse plan and buffers
     cufftHandle c2r1 = 0;
     bool have_c2r1 = false;
@@ -594,6 +599,8 @@ extern "C" int dl_flow_destroy(dl_flow *f)
     void *ptrs[] = {f->u, f->nold, f->work, f->phys, f->afor, f->spec_part, f->diss_spec, f->diss_phys, f->diss};
     for (void *q : ptrs)
         if (q) cudaFree(q);
+    for (int i = 0; i < 5 * dl_flow::NTS; i++)
+        if (f->tse[i]) cudaEventDestroy(f->tse[i]);
     if (f->ev_ready) cudaEventDestroy(f->ev_ready);
     if (f->ev_used) cudaEventDestroy(f->ev_used);
     if (f->own_stream) cudaStreamDestroy(f->own_stream);
@@ -713,8 +720,11 @@ extern "C" int dl_flow_step(dl_flow *f, dl_ctx *droplets)
         FCUDA(f, cudaEventRecord(f->ev_used, droplets->stream));
         FCUDA(f, cudaStreamWaitEvent(f->stream, f->ev_used, 0));
     }
+    cudaEvent_t *te = f->timing ? f->tse + 5 * (f->nts % dl_flow::NTS) : nullptr;
+    if (te) FCUDA(f, cudaEventRecord(te[0], f->stream));
     // omega and u in physical space
     FFT(f, cufftExecZ2D(f->c2r, reinterpret_cast<cufftDoubleComplex *>(f->work), f->phys));
+    if (te) FCUDA(f, cudaEventRecord(te[1], f->stream));
     f->phys_valid = 1;
     if (droplets) {
         // u x omega, and the droplet context's padded copy of u from the same pass
@@ -732,7 +742,9 @@ extern "C" int dl_flow_step(dl_flow *f, dl_ctx *droplets)
         k_cross<<<blocks(n3, 256), 256, 0, f->stream>>>(n3, f->phys);
         FCUDA(f, cudaGetLastError());
     }
+    if (te) FCUDA(f, cudaEventRecord(te[2], f->stream));
     FFT(f, cufftExecD2Z(f->r2c, f->phys, reinterpret_cast<cufftDoubleComplex *>(f->work)));
+    if (te) FCUDA(f, cudaEventRecord(te[3], f->stream));
     UpdArgs A;
     A.G = f->G;
     A.u = f->u;
@@ -758,8 +770,38 @@ extern "C" int dl_flow_step(dl_flow *f, dl_ctx *droplets)
     }
     k_finish_low<<<blocks(3 * (int64_t)n * n, 256), 256, 0, f->stream>>>(f->G, f->u, f->work);
     FCUDA(f, cudaGetLastError());
+    if (te) {
+        FCUDA(f, cudaEventRecord(te[4], f->stream));
+        f->nts++;
+    }
     f->launches += 5;
     f->steps++;
+    return 0;
+}
+
+extern "C" int dl_flow_timing(dl_flow *f, int enable, double *fft_ms, double *kernel_ms, int *steps)
+{
+    if (!f) return DL_E_ARG;
+    FCUDA(f, cudaStreamSynchronize(f->stream));
+    const int m = std::min(f->nts, (int)dl_flow::NTS);
+    double tf = 0.0, tk = 0.0;
+    for (int i = 0; i < m; i++) {
+        const cudaEvent_t *e = f->tse + 5 * i;
+        float a = 0.f, b = 0.f, c = 0.f, d = 0.f;
+        FCUDA(f, cudaEventElapsedTime(&a, e[0], e[1]));
+        FCUDA(f, cudaEventElapsedTime(&b, e[1], e[2]));
+        FCUDA(f, cudaEventElapsedTime(&c, e[2], e[3]));
+        FCUDA(f, cudaEventElapsedTime(&d, e[3], e[4]));
+        tf += a + c;
+        tk += b + d;
+    }
+    if (fft_ms) *fft_ms = m ? tf / m : 0.0;
+    if (kernel_ms) *kernel_ms = m ? tk / m : 0.0;
+    if (steps) *steps = m;
+    if (enable && !f->tse[0])
+        for (int i = 0; i < 5 * dl_flow::NTS; i++) FCUDA(f, cudaEventCreate(&f->tse[i]));
+    f->timing = enable;
+    f->nts = 0;
     return 0;
 }
 

@@ -245,7 +245,9 @@ struct dl_ctx {
     cudaStream_t own_stream;
     static const int NTEV = 256;
     cudaEvent_t tev[2 * NTEV];   // start/stop of the update kernels of the last NTEV steps
+    cudaEvent_t tmid[NTEV];      // end of the interpolation kernel within those steps
     int ntev;                    // pairs recorded since the last reset
+    int tev_open;                // a pair is open: the interpolation launcher records tmid
     int64_t launches;            // kernels launched since the last reset
 };
 
@@ -345,6 +347,7 @@ void *dl_host_stage(dl_ctx *c, size_t bytes);
 int dl_hist_boundary(dl_ctx *c);
 int dl_apply_remap(dl_ctx *c, const std::vector<int> &old_ref, const std::vector<int> &new_ref);
 void dl_brick_dims(int mixed, int *bx, int *by, int *bz);
+void dl_mark_interp_end(dl_ctx *c);   // timing: the interpolation kernel of this step ends here
 
 // Host RNGs (accesories.f90)
 double dl_ranpp(int *idum, int *iy, int *iv);

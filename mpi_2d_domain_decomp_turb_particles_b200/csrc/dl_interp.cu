@@ -657,7 +657,7 @@ constexpr int BOX = EX * EY;                     // floats of one component plan
 constexpr int SPL = 4;                           // planes per slab (one TMA box)
 constexpr int SLAB = SPL * 3 * BOX;              // floats of a slab (three components)
 constexpr int CAP = 32;                          // tasks per bank bucket (more go to the overflow list)
-constexpr int NPROD = 1;                         // producer warps (slab j goes to producer j % NPROD)
+constexpr int NPROD = 1;                         // producer warps (slab j goes to the producer of slot j % NSL)
 constexpr int NPREP = 3;                         // prep warps (batches go round them)
 static_assert(BOX % 32 == 8 && (3 * BOX) % 32 == 24 && (SPL * 3 * BOX) % 32 == 0 && (SPL * BOX) % 32 == 0,
               "slab bank pattern");
@@ -669,7 +669,7 @@ struct ColBatch {   // per-batch shared-memory area
     float4 fr[MAXD];                          // x, y, z fractions; w: corner | first plane << 12 (or -1)
     int meta[16];   // d0, nd, full rounds, overflow tasks, release lo, hi, end, next round, window end
     int cnt[32];                              // tasks per bucket
-    unsigned short task[32 * colk::CAP];      // bucketed tasks: droplet << 2 | component slot
+    unsigned short task[colk::CAP * 32];      // bucketed tasks, entry g of bucket r at g * 32 + r: droplet << 2 | component slot
     unsigned short ovf[MAXD * 3];             // overflow tasks
 };
 
@@ -711,7 +711,6 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
 {
     using namespace colk;
     using B = ColBatch<MAXD>;
-    static_assert(NSL % NPROD == 0, "a slab slot always belongs to the same producer");
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     float *ring = reinterpret_cast<float *>(smem_raw);
     unsigned long long *full = reinterpret_cast<unsigned long long *>(smem_raw + (size_t)NSL * SLAB * 4);
@@ -726,7 +725,8 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
     constexpr int QI = 4;             // work-item queue between the producer and the prep warps
     __shared__ int s_item[QI];
     __shared__ int s_qn, s_qend;      // items published; items of this CTA (-1 until known)
-    __shared__ int s_qpos[NPREP];     // items each prep warp has taken from the queue
+    constexpr int NREAD = NPREP + NPROD - 1;    // warps that read the queue
+    __shared__ int s_qpos[NREAD];     // items each reader has taken from the queue
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int n = A.n, ncx = A.nbx, ncol = A.nbx * A.nby;
@@ -743,7 +743,7 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
         sabort = 0;
         s_qn = 0;
         s_qend = -1;
-        for (int w = 0; w < NPREP; w++) s_qpos[w] = 0;
+        for (int w = 0; w < NREAD; w++) s_qpos[w] = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     __syncthreads();
@@ -759,29 +759,47 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
     auto item_z = [&](int it, int &za, int &zb) { const int bd = it / ncol; za = A.band[bd]; zb = A.band[bd + 1]; };
     auto seg_planes = [](int za, int zb) { return (zb - za + 7 + SPL - 1) / SPL * SPL; };
     auto aborted = [&]() { return *(volatile int *)&sabort != 0; };
+    // item q of the queue (bounded wait); false at the end of the queue or on an abort
+    auto queue_item = [&](int q, int &it) -> bool {
+        for (int i = 0; i < (1 << 22) && !aborted(); i++) {
+            if (*(volatile int *)&s_qn > q) {
+                it = *(volatile int *)&s_item[q % QI];
+                return true;
+            }
+            const int qe = *(volatile int *)&s_qend;
+            if (qe >= 0 && q >= qe) return false;
+            __nanosleep(64);
+        }
+        if (!aborted()) {
+            atomicOr(A.err, DL_DERR_TMA_TIMEOUT);
+            *(volatile int *)&sabort = 1;
+        }
+        return false;
+    };
     auto fail = [&]() {
         atomicOr(A.err, DL_DERR_TMA_TIMEOUT);
         *(volatile int *)&sabort = 1;
     };
 
     if (warp >= NSW && warp < NSW + NPROD) {
-        // ================= producers: slab j of the sweep goes to producer j % NPROD =================
+        // ================= producers: slab j goes to the producer of its slot, slot % NPROD ==========
+        // (a slot always has the same producer, which fills it in order).  Producer 0 takes the
+        // work items from the global counter and puts them in the queue the other warps read.
         const int pw = warp - NSW;
-        static_assert(NPROD == 1, "one producer takes the work items");
         if (lane == 0) {
             unsigned j = 0;   // slab index in the sweep
             bool ok = true;
             const int c0 = ncomp == 3 ? 0 : clo;   // first component of the box
             int qn = 0;
-            bool more = true;
-            // takes the next work item and hands it to the prep warps (false at the end)
+            bool more = pw == 0;
+            // takes the next work item and puts it in the queue (false at the end)
             auto publish = [&]() -> bool {
                 if (!more) return false;
-                if (qn >= QI) {   // the queue slot is free once every prep warp has read it
+                if (qn >= QI) {   // the queue slot is free once every reader has read it
                     bool freed = false;
                     for (int i = 0; i < (1 << 22) && !aborted(); i++) {
                         int mn = 1 << 30;
-                        for (int w = 0; w < NPREP; w++) mn = min(mn, *(volatile int *)&s_qpos[w]);
+                        for (int w = 0; w < NREAD; w++) mn = min(mn, *(volatile int *)&s_qpos[w]);
                         if (mn > qn - QI) { freed = true; break; }
                         __nanosleep(64);
                     }
@@ -799,21 +817,28 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
                 qn++;
                 return true;
             };
-            publish();
-            for (int q = 0; q < qn && ok; q++) {
-                const int it = *(volatile int *)&s_item[q % QI];
+            if (pw == 0) publish();
+            for (int q = 0; ok; q++) {
+                int it = 0;
+                if (pw == 0) {
+                    if (q >= qn) break;
+                    it = *(volatile int *)&s_item[q % QI];
+                } else {
+                    if (!queue_item(q, it)) break;
+                    *(volatile int *)&s_qpos[NPREP + pw - 1] = q + 1;
+                }
                 int za, zb;
                 item_z(it, za, zb);
                 const int col = it % ncol;
                 const int cx = col % ncx, cy = col / ncx;
                 const int nsl = seg_planes(za, zb) / SPL;
                 for (int k = 0; k < nsl && ok; k++, j++) {
-                    // the next item is taken when this one's last slab is issued: late enough
+                    // the next item is taken when this item's last slab comes up: late enough
                     // that a CTA holds at most one item it has not started when the items run
-                    // out, early enough for the prep warps, which work behind the producer
-                    if (k == nsl - 1) publish();
-                    if ((int)(j % NPROD) != pw) continue;
+                    // out, early enough for the readers, which work behind the producers
+                    if (pw == 0 && k == nsl - 1) publish();
                     const int s = j % NSL;
+                    if (s % NPROD != pw) continue;
                     if (j >= (unsigned)NSL && !mbar_wait(&empty[s], ((j / NSL) - 1) & 1)) { fail(); ok = false; break; }
                     if (aborted()) { ok = false; break; }
                     mbar_arrive_expect_tx(&full[s], (unsigned)(SLABF * 4));
@@ -822,18 +847,20 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
                                 za - 3 + SPL * k + DL_PAD_LO);
                 }
             }
-            if (more) {   // stopped early: the prep warps see the end of the queue
+            if (more) {   // stopped early: the readers see the end of the queue
                 more = false;
                 *(volatile int *)&s_qend = qn;
             }
             // this producer's copies still in flight land before the CTA may leave (bounded waits)
             for (unsigned q = (j > (unsigned)NSL ? j - NSL : 0u); q < j; q++)
-                if ((int)(q % NPROD) == pw) mbar_wait(&full[q % NSL], (q / NSL) & 1);
-            // the last CTA done taking items resets the counter for the next launch
-            __threadfence();
-            if (atomicAdd(&A.work[1], 1) == (int)gridDim.x - 1) {
-                atomicExch(&A.work[0], 0);
-                atomicExch(&A.work[1], 0);
+                if ((int)(q % NSL) % NPROD == pw) mbar_wait(&full[q % NSL], (q / NSL) & 1);
+            if (pw == 0) {
+                // the last CTA done taking items resets the counter for the next launch
+                __threadfence();
+                if (atomicAdd(&A.work[1], 1) == (int)gridDim.x - 1) {
+                    atomicExch(&A.work[0], 0);
+                    atomicExch(&A.work[1], 0);
+                }
             }
         }
         return;
@@ -868,20 +895,11 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
             return mbar_wait(&freep[bb % NP], ((bb / NP) - 1) & 1);
         };
         for (int q = 0;; q++) {
-            // the next work item from the producer's queue
-            bool have = false;
-            for (int i = 0; i < (1 << 22) && !aborted(); i++) {
-                if (*(volatile int *)&s_qn > q) { have = true; break; }
-                const int qe = *(volatile int *)&s_qend;
-                if (qe >= 0 && q >= qe) break;
-                __nanosleep(64);
-            }
-            if (!have) {
-                if (*(volatile int *)&s_qend < 0 && !aborted()) { fail(); return; }
-                break;
-            }
-            const int it = *(volatile int *)&s_item[q % QI];
+            // the next work item from the queue
+            int it = 0;
+            const bool have = queue_item(q, it);
             __syncwarp();
+            if (!have) break;
             if (lane == 0) *(volatile int *)&s_qpos[pw] = q + 1;
             int za, zb;
             item_z(it, za, zb);
@@ -944,7 +962,7 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
                                 const int key = (corner + cc * BOX + PS * (int)(u0 & 3u)) & 31;
                                 const unsigned short tk = (unsigned short)((i << 2) | cc);
                                 const int slot = atomicAdd(&S->cnt[key], 1);
-                                if (slot < CAP) S->task[key * CAP + slot] = tk;
+                                if (slot < CAP) S->task[slot * 32 + key] = tk;
                                 else S->ovf[atomicAdd(&S->meta[3], 1)] = tk;
                             }
                         } else {
@@ -1018,7 +1036,7 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
             if (g >= total) break;
             int t = -1;
             if (g < nrf) {
-                if (g < mycnt) t = S->task[lane * CAP + g];
+                if (g < mycnt) t = S->task[g * 32 + lane];
             } else {
                 const int q = (g - nrf) * 32 + lane;
                 if (q < novf) t = S->ovf[q];
@@ -1554,6 +1572,7 @@ static int launch_interp_t(dl_ctx *c, int comp_lo, int ncomp, int fused)
     const int grid = std::min(c->nbricks, c->num_sms);
     kern<<<grid, (NG * GW + 1) * 32, sm, c->stream>>>(c->tmap, A);
     DL_CHECK_LAUNCH(c);
+    dl_mark_interp_end(c);
     if (fused) {
         k_advance_fused<T><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(A);
         DL_CHECK_LAUNCH(c);
@@ -1620,6 +1639,7 @@ static int launch_interp_col(dl_ctx *c, int comp_lo, int ncomp, int fused)
     const int grid = c->num_sms;
     kern<<<grid, (COL_NSW + colk::NPROD + 1 + colk::NPREP) * 32, sm, c->stream>>>(ncomp == 3 ? c->tmap : c->tmap1, A);
     DL_CHECK_LAUNCH(c);
+    dl_mark_interp_end(c);
     if (fused) {
         // the advance epilogue: history, drag, position update, wrap, departure flags
         InterpArgs<float> E = A;

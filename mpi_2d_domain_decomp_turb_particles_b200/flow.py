@@ -126,6 +126,13 @@ class Flow:
                                                      C.byref(seed), C.byref(iy), iv))
         return b.reshape(3, 5, 5, 6), seed.value, iy.value, np.array(iv[:], np.int32)
 
+    def timing(self, enable: bool = True):
+        """(cuFFT ms, update/cross kernel ms, steps) averaged over the steps since the last
+        call; then enables or disables the timing for the steps that follow."""
+        a, b, n = C.c_double(0), C.c_double(0), C.c_int(0)
+        self._chk(self.lib.dl_flow_timing(self.h, int(enable), C.byref(a), C.byref(b), C.byref(n)))
+        return a.value, b.value, n.value
+
     def set_stream(self, stream):
         h = None if stream is None else int(getattr(stream, "cuda_stream", stream))
         self._chk(self.lib.dl_flow_set_stream(self.h, C.c_void_p(h) if h else None))

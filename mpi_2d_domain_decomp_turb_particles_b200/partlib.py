@@ -412,6 +412,12 @@ class Partlib:
         self._chk(self.lib.dl_timing(self.h, int(reset), C.byref(ms), C.byref(n), C.byref(l)))
         return ms.value, n.value, l.value
 
+    def timing_split(self):
+        """(interpolation ms, advance ms) per step over the steps dl_timing would average."""
+        a, b = C.c_double(0), C.c_double(0)
+        self._chk(self.lib.dl_timing_split(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def phase_times(self) -> np.ndarray:
         out = np.zeros(6)
         self._chk(self.lib.dl_get_phase_times(self.h, _dptr(out)))
