@@ -252,9 +252,13 @@ int dl_get_collist(dl_ctx *ctx, double *collist20, int cap, int *ntotpair);
  * reference indices (partner = the ghost's source index for ghost partners). */
 int dl_get_nei(dl_ctx *ctx, int *nei_num, int *pairs2, double *coef6, int cap, int *nnz);
 
-/* Device timing of the phases of the last dl_particle_step (ms): interpolation+advance,
- * cell list, collision detection, HDI, periodic/relocate, overlap detection. */
-int dl_get_phase_times(dl_ctx *ctx, double *ms6);
+/* Device timing of the phases of the last dl_particle_step (ms), eight entries:
+ * [0] interpolation with PART_HISTORY_FVP (and, on the fused path without HDI, the advance
+ * and position update), [1] cell list (HEADLIST), [2] collision detection, [3] HDI
+ * (NEI_LIST_PRECOMP + HDI_GMRES), [4] periodic/relocate/coalesce, [5] overlap detection,
+ * [6] PART_HISTORY_FDP + PART_ADVANCE (+ MEAN_VEL) when not fused, [7] the interpolation
+ * kernel alone (the reference's INTERPOLATE timer, turb.f90:734-755). */
+int dl_get_phase_times(dl_ctx *ctx, double *ms8);
 
 /* Runs every later call of the context on the caller's CUDA stream (a cudaStream_t passed
  * as void*; NULL restores the context's own stream).  No reference counterpart. */
@@ -292,11 +296,13 @@ int dl_flow_destroy(dl_flow *f);
 const char *dl_flow_last_error(const dl_flow *f);
 int dl_flow_set_stream(dl_flow *f, void *stream);
 int dl_flow_sync(dl_flow *f);
-/* Device time of the flow steps taken since the last call, averaged per step (ms): the
- * cuFFT transforms and the update / cross-product kernels, timed with CUDA events when
- * enabled (the reference times the flow step as a whole, turb.f90:734-755).  Returns
- * the averages, then enables (1) or disables (0) the timing and resets it.  Synchronises. */
-int dl_flow_timing(dl_flow *f, int enable, double *fft_ms, double *kernel_ms, int *steps);
+/* Device time of the flow steps taken since the last call, averaged per step (ms), in
+ * four parts: the inverse cuFFT transform, the cross-product kernel (with the droplet
+ * field copy), the forward cuFFT transform, and the update kernels (update, forcing,
+ * finish); CUDA events when enabled (the reference times the flow step as a whole,
+ * turb.f90:734-755).  Returns the averages, then enables (1) or disables (0) the timing
+ * and resets it.  Synchronises. */
+int dl_flow_timing(dl_flow *f, int enable, double *ms4, int *steps);
 /* new flow from a physical velocity (3 components in the INTERPOLATE layout v(llx, ly, lz),
  * component c at u + c * pitch_z * n), host or device: transform, projection, symmetrize,
  * dealiasing; N_old = u as the reference's new-flow start (turb.f90:452-454). */

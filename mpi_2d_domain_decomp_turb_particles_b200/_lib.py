@@ -146,7 +146,7 @@ SIGNATURES = {
     "dl_flow_last_error": (C.c_char_p, [_vp]),
     "dl_flow_set_stream": (C.c_int, [_vp, C.c_void_p]),
     "dl_flow_sync": (C.c_int, [_vp]),
-    "dl_flow_timing": (C.c_int, [_vp, C.c_int, _dp, _dp, _ip]),
+    "dl_flow_timing": (C.c_int, [_vp, C.c_int, _dp, _ip]),
     "dl_flow_set_velocity": (C.c_int, [_vp, C.c_void_p, C.c_int64, C.c_int64, C.c_int]),
     "dl_flow_set_spectral": (C.c_int, [_vp, C.c_void_p, C.c_void_p, C.c_int]),
     "dl_flow_get_spectral": (C.c_int, [_vp, _dp, _dp]),

@@ -375,7 +375,7 @@ extern "C" int dl_create(const dl_params *p, dl_ctx **out)
     if (e != cudaSuccess) return dl_fail(c, DL_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
     DL_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     c->own_stream = c->stream;
-    for (int i = 0; i < 8; i++) DL_CUDA(c, cudaEventCreate(&c->ev[i]));
+    for (int i = 0; i < 10; i++) DL_CUDA(c, cudaEventCreate(&c->ev[i]));
     for (int i = 0; i < 2 * dl_ctx::NTEV; i++) DL_CUDA(c, cudaEventCreate(&c->tev[i]));
     for (int i = 0; i < dl_ctx::NTEV; i++) DL_CUDA(c, cudaEventCreate(&c->tmid[i]));
     // defaults for capacities (single GPU: no MPI load imbalance to absorb)
@@ -522,7 +522,7 @@ extern "C" int dl_destroy(dl_ctx *c)
     F(c->red_pos); F(c->red_list); F(c->red_start); F(c->red_partner); F(c->red_rhs);
     F(c->nei_fill); F(c->nei_blk); F(c->nei_key); F(c->rf32); F(c->nei_app); F(c->cell_start); F(c->pk_x); F(c->pk_id);
     F(c->scal[0]); F(c->scal[1]); F(c->gr_part); F(c->gr_bins); F(c->gr_mdens); F(c->scal_field);
-    for (int i = 0; i < 8; i++)
+    for (int i = 0; i < 10; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     for (int i = 0; i < 2 * dl_ctx::NTEV; i++)
         if (c->tev[i]) cudaEventDestroy(c->tev[i]);
@@ -1351,12 +1351,13 @@ static void timing_end(dl_ctx *c)
 void dl_mark_interp_end(dl_ctx *c)
 {
     if (c->tev_open) cudaEventRecord(c->tmid[c->ntev % dl_ctx::NTEV], c->stream);
+    if (c->phase_mark) cudaEventRecord(c->ev[8], c->stream);
 }
 
-extern "C" int dl_get_phase_times(dl_ctx *c, double *ms6)
+extern "C" int dl_get_phase_times(dl_ctx *c, double *ms8)
 {
-    if (!c || !ms6) return DL_E_ARG;
-    memcpy(ms6, c->phase_ms, sizeof(double) * 6);
+    if (!c || !ms8) return DL_E_ARG;
+    memcpy(ms8, c->phase_ms, sizeof(double) * 8);
     return 0;
 }
 
@@ -1496,7 +1497,10 @@ extern "C" int dl_coalesce(dl_ctx *c)
 static double elapsed(dl_ctx *c, int a, int b)
 {
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, c->ev[a], c->ev[b]);
+    if (cudaEventElapsedTime(&ms, c->ev[a], c->ev[b]) != cudaSuccess) {
+        (void)cudaGetLastError();   // a phase whose event was never recorded counts as 0
+        return 0.0;
+    }
     return ms;
 }
 
@@ -1534,13 +1538,16 @@ extern "C" int dl_particle_step(dl_ctx *c, dl_coll_report *coll, dl_gmres_report
     const bool hdi = c->dc.hdi;
     const bool nonoverlap = c->p.nonoverlap || c->p.hdi_included;
     cudaEventRecord(c->ev[0], c->stream);
+    cudaEventRecord(c->ev[8], c->stream);   // re-recorded after the interpolation kernel, when it runs
     // the fused kernel flags departures before COLLISION_DET; COALESCE (growth mode)
     // renumbers droplets in between, so those steps flag them afterwards (PERIODIC order)
     const bool growth = c->istep >= nstep_grow && nonoverlap;
     bool fused = !hdi && !growth;
+    c->phase_mark = 1;
     if (fused) {
         timing_begin(c);
         r = launch_interp(c, 0, 1);   // PREPARE_INTERP..PART_ADVANCE + position update + wrap
+        c->phase_mark = 0;
         if (r) return r;
         timing_end(c);
         c->vp_slot = c->fnew;   // vp = fdp(:,0): the fused kernel wrote it into the fluid ring
@@ -1549,6 +1556,7 @@ extern "C" int dl_particle_step(dl_ctx *c, dl_coll_report *coll, dl_gmres_report
     } else {
         c->vp_slot = -1;
         r = launch_interp(c, 0, 0);
+        c->phase_mark = 0;
         if (r) return r;
         r = launch_history_fvp(c);
         if (r) return r;
@@ -1569,6 +1577,7 @@ extern "C" int dl_particle_step(dl_ctx *c, dl_coll_report *coll, dl_gmres_report
         if (r < 0) return r;
         warn = r;   // GMRES not converged: the reference prints and carries on
     }
+    cudaEventRecord(c->ev[7], c->stream);
     if (!fused) {
         r = dl_part_history_fdp(c);
         if (r) return r;
@@ -1619,9 +1628,11 @@ extern "C" int dl_particle_step(dl_ctx *c, dl_coll_report *coll, dl_gmres_report
     c->phase_ms[0] = elapsed(c, 0, 1);
     c->phase_ms[1] = elapsed(c, 1, 2);
     c->phase_ms[2] = elapsed(c, 3, 4);
-    c->phase_ms[3] = elapsed(c, 2, 3);
+    c->phase_ms[3] = elapsed(c, 2, 7);
     c->phase_ms[4] = elapsed(c, 4, 5);
     c->phase_ms[5] = elapsed(c, 5, 6);
+    c->phase_ms[6] = elapsed(c, 7, 3);
+    c->phase_ms[7] = elapsed(c, 0, 8);
     c->time += c->dc.dt;
     c->steps_since_sort++;
     return warn;

@@ -779,24 +779,22 @@ extern "C" int dl_flow_step(dl_flow *f, dl_ctx *droplets)
     return 0;
 }
 
-extern "C" int dl_flow_timing(dl_flow *f, int enable, double *fft_ms, double *kernel_ms, int *steps)
+extern "C" int dl_flow_timing(dl_flow *f, int enable, double *ms4, int *steps)
 {
     if (!f) return DL_E_ARG;
     FCUDA(f, cudaStreamSynchronize(f->stream));
     const int m = std::min(f->nts, (int)dl_flow::NTS);
-    double tf = 0.0, tk = 0.0;
+    double t[4] = {0.0, 0.0, 0.0, 0.0};
     for (int i = 0; i < m; i++) {
         const cudaEvent_t *e = f->tse + 5 * i;
-        float a = 0.f, b = 0.f, c = 0.f, d = 0.f;
-        FCUDA(f, cudaEventElapsedTime(&a, e[0], e[1]));
-        FCUDA(f, cudaEventElapsedTime(&b, e[1], e[2]));
-        FCUDA(f, cudaEventElapsedTime(&c, e[2], e[3]));
-        FCUDA(f, cudaEventElapsedTime(&d, e[3], e[4]));
-        tf += a + c;
-        tk += b + d;
+        for (int k = 0; k < 4; k++) {
+            float a = 0.f;
+            FCUDA(f, cudaEventElapsedTime(&a, e[k], e[k + 1]));
+            t[k] += a;
+        }
     }
-    if (fft_ms) *fft_ms = m ? tf / m : 0.0;
-    if (kernel_ms) *kernel_ms = m ? tk / m : 0.0;
+    if (ms4)
+        for (int k = 0; k < 4; k++) ms4[k] = m ? t[k] / m : 0.0;
     if (steps) *steps = m;
     if (enable && !f->tse[0])
         for (int i = 0; i < 5 * dl_flow::NTS; i++) FCUDA(f, cudaEventCreate(&f->tse[i]));

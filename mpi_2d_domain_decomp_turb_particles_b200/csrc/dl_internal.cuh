@@ -240,8 +240,9 @@ struct dl_ctx {
     int ovl_cap;
 
     // ---- timing ----
-    cudaEvent_t ev[8];
-    double phase_ms[6];
+    cudaEvent_t ev[10];
+    double phase_ms[8];
+    int phase_mark;              // the interpolation launcher records ev[8] (particle step)
     cudaStream_t own_stream;
     static const int NTEV = 256;
     cudaEvent_t tev[2 * NTEV];   // start/stop of the update kernels of the last NTEV steps

@@ -127,11 +127,13 @@ class Flow:
         return b.reshape(3, 5, 5, 6), seed.value, iy.value, np.array(iv[:], np.int32)
 
     def timing(self, enable: bool = True):
-        """(cuFFT ms, update/cross kernel ms, steps) averaged over the steps since the last
-        call; then enables or disables the timing for the steps that follow."""
-        a, b, n = C.c_double(0), C.c_double(0), C.c_int(0)
-        self._chk(self.lib.dl_flow_timing(self.h, int(enable), C.byref(a), C.byref(b), C.byref(n)))
-        return a.value, b.value, n.value
+        """Device ms per step averaged over the steps since the last call: a dict with the
+        inverse transform, cross-product kernel, forward transform and update kernels, and
+        the step count; then enables or disables the timing for the steps that follow."""
+        ms = (C.c_double * 4)()
+        n = C.c_int(0)
+        self._chk(self.lib.dl_flow_timing(self.h, int(enable), ms, C.byref(n)))
+        return {"fft_inverse": ms[0], "cross": ms[1], "fft_forward": ms[2], "update": ms[3], "steps": n.value}
 
     def set_stream(self, stream):
         h = None if stream is None else int(getattr(stream, "cuda_stream", stream))

@@ -419,6 +419,9 @@ class Partlib:
         return a.value, b.value
 
     def phase_times(self) -> np.ndarray:
-        out = np.zeros(6)
+        """Device ms of the last particle step: interpolation(+fvp, +advance when fused),
+        cell list, collision, HDI, periodic, overlap, advance (not fused), interpolation
+        kernel alone."""
+        out = np.zeros(8)
         self._chk(self.lib.dl_get_phase_times(self.h, _dptr(out)))
         return out

@@ -17,7 +17,9 @@ import torch
 
 
 def spectral_field(n: int, seed: int = 1234, device="cuda", kpeak: float = 4.0, pad: int = 2):
-    gen = torch.Generator(device=device).manual_seed(seed)
+    """The random phases come from a CPU generator, so every device (and the host) gets the
+    same field up to the rounding of its FFT."""
+    gen = torch.Generator(device="cpu").manual_seed(seed)
     k1 = torch.fft.fftfreq(n, d=1.0 / n, device=device, dtype=torch.float64)
     kr = torch.fft.rfftfreq(n, d=1.0 / n, device=device, dtype=torch.float64)
     KZ, KY, KX = torch.meshgrid(k1, k1, kr, indexing="ij")
@@ -26,8 +28,8 @@ def spectral_field(n: int, seed: int = 1234, device="cuda", kpeak: float = 4.0, 
     spec = K ** 4 * torch.exp(-2.0 * (K / kpeak) ** 2)
     amp = torch.sqrt(spec / torch.clamp(4 * math.pi * K2, min=1.0))
     amp[0, 0, 0] = 0.0
-    a = [torch.complex(torch.randn(K.shape, generator=gen, device=device, dtype=torch.float64),
-                       torch.randn(K.shape, generator=gen, device=device, dtype=torch.float64)) * amp
+    a = [torch.complex(torch.randn(K.shape, generator=gen, dtype=torch.float64).to(device),
+                       torch.randn(K.shape, generator=gen, dtype=torch.float64).to(device)) * amp
          for _ in range(3)]
     # solenoidal projection a -= k (k.a)/k^2
     k2 = torch.where(K2 > 0, K2, torch.ones_like(K2))

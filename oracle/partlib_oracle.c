@@ -408,7 +408,12 @@ void orc_interpolate(orc_state *s, const double *v, int icpt, long pitch_y, long
 static inline void history_fvp_one(orc_state *s, long ih, int first)
 {
     int c, l;
-    if (first) {
+    if (first && s->init_velocity == 1) {
+        /* the CPU-runnable configuration starts droplets at the interpolated fluid velocity */
+        for (c = 0; c < 3; c++) YP(s, 3 + c, ih) = VP(s, c, ih);
+        for (l = 0; l < 3; l++)
+            for (c = 0; c < 3; c++) FVP(s, c, l, ih) = YP(s, 3 + c, ih);
+    } else if (first) {
         YP(s, 3, ih) = s->sv_const * (YP(s, 6, ih) * YP(s, 6, ih));
         YP(s, 4, ih) = 0.0;
         YP(s, 5, ih) = 0.0;
@@ -1681,6 +1686,7 @@ int orc_get_i(orc_state *s, const char *name)
     if (NAME_IS("istep")) return s->istep;
     if (NAME_IS("written")) return s->written;
     if (NAME_IS("new_particle")) return s->new_particle;
+    if (NAME_IS("init_velocity")) return s->init_velocity;
     if (NAME_IS("nx_max")) return s->nx_max;
     if (NAME_IS("ny_max")) return s->ny_max;
     if (NAME_IS("nz_max")) return s->nz_max;
@@ -1709,6 +1715,7 @@ void orc_set_i(orc_state *s, const char *name, int v)
     if (NAME_IS("nps")) s->nps = v;
     else if (NAME_IS("istep")) s->istep = v;
     else if (NAME_IS("new_particle")) s->new_particle = v;
+    else if (NAME_IS("init_velocity")) s->init_velocity = v;
 }
 
 void orc_set_d(orc_state *s, const char *name, double v)

@@ -73,6 +73,7 @@ typedef struct orc_state {
     int nx, ny, nz, lx, ly, lz;
     int npart, nps, nset, ndrag, msize, nbin, ncollmax, nuniform;
     int new_particle, nonoverlap, hdi_included;
+    int init_velocity;   /* not a reference option: 1 = first-step velocity is the fluid velocity */
     int ncdx, ncdy, ncdz;
     int nx_coll, ny_coll, nz_coll, nx_hdi, ny_hdi, nz_hdi, nx_max, ny_max, nz_max;
     int istep;
