@@ -648,36 +648,64 @@ __global__ void __launch_bounds__((NG * GW + 1) * 32, 1) k_interp(const __grid_c
 // PS * u (mod 32) whatever slab slot holds it, so the bank of a stencil's start plus
 // PS * k is the bank of its plane k, the same shift for every lane of a round.
 // ---------------------------------------------------------------------------------------
-namespace colk {
-constexpr int CX = 16, CY = 16;                  // column cross-section (cells)
-constexpr int M = 1;                             // y drift tolerated since the last sort (cells)
-constexpr int EX = CX + 8;                       // tile row: x from cx*CX - 4 (16-byte aligned x)
-constexpr int EY = CY + 5 + 2 * M;               // rows: y from cy*CY - 3
-constexpr int BOX = EX * EY;                     // floats of one component plane
-constexpr int SPL = 4;                           // planes per slab (one TMA box)
-constexpr int SLAB = SPL * 3 * BOX;              // floats of a slab (three components)
-constexpr int CAP = 32;                          // tasks per bank bucket (more go to the overflow list)
-constexpr int NPROD = 1;                         // producer warps (slab j goes to the producer of slot j % NSL)
-constexpr int NPREP = 3;                         // prep warps (batches go round them)
-static_assert(BOX % 32 == 8 && (3 * BOX) % 32 == 24 && (SPL * 3 * BOX) % 32 == 0 && (SPL * BOX) % 32 == 0,
-              "slab bank pattern");
-static_assert((SLAB * 4) % 128 == 0 && (SPL * BOX * 4) % 128 == 0, "slab slots keep 128-byte alignment");
-}  // namespace colk
-
-template <int MAXD>
-struct ColBatch {   // per-batch shared-memory area
-    float4 fr[MAXD];                          // x, y, z fractions; w: corner | first plane << 12 (or -1)
-    int meta[16];   // d0, nd, full rounds, overflow tasks, release lo, hi, end, next round, window end
-    int cnt[32];                              // tasks per bucket
-    unsigned short task[colk::CAP * 32];      // bucketed tasks, entry g of bucket r at g * 32 + r: droplet << 2 | component slot
-    unsigned short ovf[MAXD * 3];             // overflow tasks
+// Per-precision geometry of the column sweep.  FP32: columns of 16 x 16 cells, 32 bank
+// buckets of one word; FP64: columns of 16 x 8 cells (a slab of four planes of three
+// components is then 34.6 KB), 16 buckets of one double (two banks): a 64-bit shared load
+// is served per half-warp, so lanes L and L + 16 take consecutive entries of bucket L % 16.
+template <typename T>
+struct ColGeo;
+template <>
+struct ColGeo<float> {
+    static constexpr int CX = 16, CY = 16;
+    static constexpr int NBK = 32;                  // bank buckets
+    static constexpr int CAP = 32;                  // entries per bucket (more go to the overflow list)
+    static constexpr int NW = 3;                    // per-droplet words in the batch: x, y, z fractions
+};
+template <>
+struct ColGeo<double> {
+    static constexpr int CX = 16, CY = 8;
+    static constexpr int NBK = 16;
+    static constexpr int CAP = 64;
+    static constexpr int NW = 18;                   // the 18 FP64 Lagrange weights, computed once
 };
 
-template <int NSL, int MAXD, int NP>
+namespace colk {
+constexpr int M = 1;                             // y drift tolerated since the last sort (cells)
+constexpr int SPL = 4;                           // planes per slab (one TMA box)
+constexpr int NPROD = 1;                         // producer warps (slab j goes to the producer of slot j % NSL)
+constexpr int NPREP = 3;                         // prep warps (batches go round them)
+template <typename T>
+struct G {
+    static constexpr int CX = ColGeo<T>::CX, CY = ColGeo<T>::CY;
+    static constexpr int EX = CX + 8;            // tile row: x from cx*CX - 4 (16-byte aligned x)
+    static constexpr int EY = CY + 5 + 2 * M;    // rows: y from cy*CY - 3
+    static constexpr int BOX = EX * EY;          // elements of one component plane
+    static constexpr int SLAB = SPL * 3 * BOX;   // elements of a slab (three components)
+    static constexpr int NBK = ColGeo<T>::NBK, CAP = ColGeo<T>::CAP;
+    static_assert(BOX % NBK == 8 && (SPL * 3 * BOX) % NBK == 0 && (SPL * BOX) % NBK == 0, "slab bank pattern");
+    static_assert((SLAB * sizeof(T)) % 128 == 0 && (SPL * BOX * sizeof(T)) % 128 == 0,
+                  "slab slots keep 128-byte alignment");
+};
+}  // namespace colk
+
+template <typename T, int MAXD>
+struct ColBatch {   // per-batch shared-memory area
+    T w[MAXD][ColGeo<T>::NW];                 // FP32: x, y, z fractions; FP64: the weights
+    int co[MAXD];                             // corner | first plane << 12, or -1 (global-memory path)
+    int meta[16];   // d0, nd, tasks, overflow tasks, release lo, hi, end, next round, window end
+    int cnt[32];                              // tasks per bank bucket
+    unsigned lmask[ColGeo<T>::CAP];           // layer e: the buckets holding an entry e
+    int loff[ColGeo<T>::CAP];                 // layer e: its first position in the task list
+    // the tasks (droplet << 2 | component slot) in layer-major order: entry 0 of every
+    // bucket holding one, buckets ascending, then entry 1, ...; then the overflow tasks
+    unsigned short task[MAXD * 3];
+};
+
+template <typename T, int NSL, int MAXD, int NP>
 constexpr size_t col_smem()
 {
-    return (size_t)NSL * colk::SLAB * 4 + ((size_t)(2 * NSL + 3 * NP) * 8 + 127) / 128 * 128 +
-           (size_t)NP * ((sizeof(ColBatch<MAXD>) + 127) / 128 * 128);
+    return (size_t)NSL * colk::G<T>::SLAB * sizeof(T) + ((size_t)(2 * NSL + 3 * NP) * 8 + 127) / 128 * 128 +
+           (size_t)NP * ((sizeof(ColBatch<T, MAXD>) + 127) / 128 * 128);
 }
 
 // 6x6x6 FP32 stencil, planes outermost: acc = sum_k bz[k] sum_b by[b] sum_a bx[a] v(a, b, k)
@@ -700,25 +728,58 @@ __device__ __forceinline__ float stencil_planes(const L &ld, const float *bx, co
     return acc;
 }
 
+// The FP32 stencil: planes outermost, FMA
+template <class L>
+__device__ __forceinline__ float col_stencil(const L &ld, const float *bx, const float *by, const float *bz)
+{
+    return stencil_planes(ld, bx, by, bz);
+}
+// The FP64 stencil of a droplet whose weights lie in shared memory (x 0..5, y 6..11, z
+// 12..17), in the reference's order and rounding; the x loop stays rolled (a sixth of the
+// code, no register spills)
+template <class L>
+__device__ __forceinline__ double col_stencil_w(const L &ld, const double *w)
+{
+    double by[6], bz[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) { by[q] = w[6 + q]; bz[q] = w[12 + q]; }
+    double acc = 0.0;
+#pragma unroll 1
+    for (int a = 0; a < 6; a++) {
+        const double wa = w[a];
+#pragma unroll
+        for (int b = 0; b < 6; b++)
+#pragma unroll
+            for (int c = 0; c < 6; c++)
+                acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(__dmul_rn(ld(a, b, c), wa), by[b]), bz[c]));
+    }
+    return acc;
+}
+
+template <typename T>
 struct RingLoader {
-    const float *pl[6];   // stencil corner in each of the six planes
-    __device__ __forceinline__ float operator()(int a, int b, int k) const { return pl[k][b * colk::EX + a]; }
+    const T *pl[6];   // stencil corner in each of the six planes
+    __device__ __forceinline__ T operator()(int a, int b, int k) const { return pl[k][b * colk::G<T>::EX + a]; }
 };
 
-template <int NSL, int MAXD, int NP, int NSW>
+template <typename T, int NSL, int MAXD, int NP, int NSW>
 __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
-    k_interp_col(const __grid_constant__ CUtensorMap tmap, InterpArgs<float> A)
+    k_interp_col(const __grid_constant__ CUtensorMap tmap, InterpArgs<T> A)
 {
     using namespace colk;
-    using B = ColBatch<MAXD>;
+    using B = ColBatch<T, MAXD>;
+    constexpr int CX = G<T>::CX, CY = G<T>::CY, EX = G<T>::EX, EY = G<T>::EY, BOX = G<T>::BOX;
+    constexpr int SLAB = G<T>::SLAB, NBK = G<T>::NBK, CAP = G<T>::CAP;
+    constexpr bool F64 = sizeof(T) == 8;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    float *ring = reinterpret_cast<float *>(smem_raw);
-    unsigned long long *full = reinterpret_cast<unsigned long long *>(smem_raw + (size_t)NSL * SLAB * 4);
+    T *ring = reinterpret_cast<T *>(smem_raw);
+    unsigned long long *full = reinterpret_cast<unsigned long long *>(smem_raw + (size_t)NSL * SLAB * sizeof(T));
     unsigned long long *empty = full + NSL;
     unsigned long long *ready = empty + NSL;
     unsigned long long *done = ready + NP;
     unsigned long long *freep = done + NP;
-    unsigned char *bbase = smem_raw + (size_t)NSL * SLAB * 4 + ((size_t)(2 * NSL + 3 * NP) * 8 + 127) / 128 * 128;
+    unsigned char *bbase =
+        smem_raw + (size_t)NSL * SLAB * sizeof(T) + ((size_t)(2 * NSL + 3 * NP) * 8 + 127) / 128 * 128;
     constexpr size_t BSZ = (sizeof(B) + 127) / 128 * 128;
     auto batch = [&](int p) { return reinterpret_cast<B *>(bbase + (size_t)p * BSZ); };
     __shared__ int sabort;
@@ -731,8 +792,8 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int n = A.n, ncx = A.nbx, ncol = A.nbx * A.nby;
     const int ncomp = A.ncomp, clo = A.comp_lo;
-    const int PS = ncomp * BOX;                       // floats per plane in a slab
-    const int SLABF = SPL * PS;                       // floats of a slab actually used
+    const int PS = ncomp * BOX;                       // elements per plane in a slab
+    const int SLABF = SPL * PS;                       // elements of a slab actually used
     if (threadIdx.x == 0) {
         for (int s = 0; s < NSL; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         for (int p = 0; p < NP; p++) {
@@ -841,7 +902,7 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
                     if (s % NPROD != pw) continue;
                     if (j >= (unsigned)NSL && !mbar_wait(&empty[s], ((j / NSL) - 1) & 1)) { fail(); ok = false; break; }
                     if (aborted()) { ok = false; break; }
-                    mbar_arrive_expect_tx(&full[s], (unsigned)(SLABF * 4));
+                    mbar_arrive_expect_tx(&full[s], (unsigned)(SLABF * sizeof(T)));
                     // padded coordinates (grid + DL_PAD_LO) of the box origin: x, y, component, z
                     tma_load_4d(ring + (size_t)s * SLAB, &tmap, &full[s], cx * CX, cy * CY + DL_PAD_LO - 3, c0,
                                 za - 3 + SPL * k + DL_PAD_LO);
@@ -931,19 +992,28 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
                     S->cnt[lane] = 0;
                     if (lane == 0) S->meta[3] = 0;
                     __syncwarp();
-                    // nodes, fractions and corners; each task goes into the bucket of the bank
-                    // its stencil starts in (a task's value does not depend on its slot)
+                    // nodes, fractions (FP64: the weights) and corners; each task is counted in
+                    // the bucket of the bank its stencil starts in and keeps its entry there
+                    int ent[QN][3];
 #pragma unroll
                     for (int q = 0; q < QN; q++) {
+#pragma unroll
+                        for (int cc = 0; cc < 3; cc++) ent[q][cc] = -1;
                         const int i = q * 32 + lane;
                         if (i >= nd) continue;
                         int node[3];
-                        float fr[3];
+                        T fr[3];
 #pragma unroll
                         for (int a = 0; a < 3; a++) {
-                            const double t = P[q][a] * A.inv_dx;
-                            node[a] = (int)floor(t);
-                            fr[a] = (float)(t - (double)node[a]);
+                            if constexpr (F64) {
+                                double z;
+                                node[a] = node_frac(P[q][a], A.dx, &z);   // the reference's division
+                                fr[a] = z;
+                            } else {
+                                const double t = P[q][a] * A.inv_dx;
+                                node[a] = (int)floor(t);
+                                fr[a] = (float)(t - (double)node[a]);
+                            }
                         }
                         // a droplet that crossed a face of the periodic box since the last sort
                         // keeps its place in the order: its periodic image (node +- n) lies in
@@ -953,43 +1023,80 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
                         if (ly < 0) ly += n; else if (ly + 5 >= EY) ly -= n;
                         if (nz < zp - 1) nz += n; else if (nz > zq) nz -= n;
                         const bool in = lx >= 0 && lx + 5 < EX && ly >= 0 && ly + 5 < EY && nz >= zp - 1 && nz <= zq;
+                        T bx[6], by[6], bz[6];
+                        if (F64 || !in) {
+                            lagrange6(fr[0], bx);
+                            lagrange6(fr[1], by);
+                            lagrange6(fr[2], bz);
+                        }
+                        if constexpr (F64) {
+#pragma unroll
+                            for (int q6 = 0; q6 < 6; q6++) {
+                                S->w[i][q6] = bx[q6];
+                                S->w[i][6 + q6] = by[q6];
+                                S->w[i][12 + q6] = bz[q6];
+                            }
+                        } else {
+                            S->w[i][0] = fr[0]; S->w[i][1] = fr[1]; S->w[i][2] = fr[2];
+                        }
                         int co = -1;
                         if (in) {
                             const unsigned u0 = useg + (unsigned)(nz - 2 - (za - 3));   // plane of the corner
                             const int corner = ly * EX + lx;
                             co = corner | (int)(u0 << 12);
-                            for (int cc = 0; cc < ncomp; cc++) {
-                                const int key = (corner + cc * BOX + PS * (int)(u0 & 3u)) & 31;
-                                const unsigned short tk = (unsigned short)((i << 2) | cc);
-                                const int slot = atomicAdd(&S->cnt[key], 1);
-                                if (slot < CAP) S->task[slot * 32 + key] = tk;
-                                else S->ovf[atomicAdd(&S->meta[3], 1)] = tk;
+#pragma unroll
+                            for (int cc = 0; cc < 3; cc++) {
+                                if (cc >= ncomp) break;
+                                const int key = (corner + cc * BOX + PS * (int)(u0 % SPL)) & (NBK - 1);
+                                ent[q][cc] = (atomicAdd(&S->cnt[key], 1) << 8) | key;
                             }
                         } else {
                             // outside the staged planes: the padded field in global memory
-                            float bx[6], by[6], bz[6];
-                            lagrange6(fr[0], bx);
-                            lagrange6(fr[1], by);
-                            lagrange6(fr[2], bz);
                             const int x0 = wrapi(node[0], n) - 2 + DL_PAD_LO;
                             const int y0 = wrapi(node[1], n) - 2 + DL_PAD_LO;
                             const int z0 = wrapi(node[2], n) - 2 + DL_PAD_LO;
                             for (int cc = 0; cc < ncomp; cc++) {
-                                GlobalLoaderPad<float> ld;
+                                GlobalLoaderPad<T> ld;
                                 ld.f = A.fpad + (clo + cc) * A.fpc + x0 + A.fpy * y0 + A.fpz * z0;
                                 ld.py = A.fpy;
                                 ld.pz = A.fpz;
-                                A.vp[clo + cc][d0 + i] = stencil_planes(ld, bx, by, bz);
+                                if constexpr (F64) A.vp[clo + cc][d0 + i] = col_stencil_w(ld, S->w[i]);
+                                else A.vp[clo + cc][d0 + i] = col_stencil(ld, bx, by, bz);
                             }
                         }
-                        S->fr[i] = make_float4(fr[0], fr[1], fr[2], __int_as_float(co));
+                        S->co[i] = co;
                     }
                     __syncwarp();
-                    int nrf = min(S->cnt[lane], CAP);
+                    // the layers of the buckets: layer e holds entry e of every bucket that has
+                    // one, in bucket order.  Any 32 consecutive tasks of that order (16 for FP64,
+                    // a half-warp's share) take each bucket at most once from a full layer, and
+                    // at most twice where the layers thin out; every round is full.
+                    const int cown = lane < NBK ? min(S->cnt[lane], CAP) : 0;
+                    int nl = cown;
 #pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) nrf = max(nrf, __shfl_xor_sync(0xffffffffu, nrf, o));
+                    for (int o = 16; o > 0; o >>= 1) nl = max(nl, __shfl_xor_sync(0xffffffffu, nl, o));
+                    int ndense = 0;
+                    for (int e = 0; e < nl; e++) {
+                        const unsigned m = __ballot_sync(0xffffffffu, cown > e);
+                        if (lane == 0) { S->lmask[e] = m; S->loff[e] = ndense; }
+                        ndense += __popc(m);
+                    }
+                    __syncwarp();
+#pragma unroll
+                    for (int q = 0; q < QN; q++)
+#pragma unroll
+                        for (int cc = 0; cc < 3; cc++) {
+                            const int ek = ent[q][cc];
+                            if (ek < 0) continue;
+                            const int e = ek >> 8, key = ek & 0xff;
+                            const unsigned short tk = (unsigned short)(((q * 32 + lane) << 2) | cc);
+                            const int pos = e < CAP ? S->loff[e] + __popc(S->lmask[e] & ((1u << key) - 1u))
+                                                    : ndense + atomicAdd(&S->meta[3], 1);
+                            S->task[pos] = tk;
+                        }
+                    __syncwarp();
                     if (lane == 0) {
-                        S->meta[0] = d0; S->meta[1] = nd; S->meta[2] = nrf;
+                        S->meta[0] = d0; S->meta[1] = nd; S->meta[2] = ndense + S->meta[3];
                         S->meta[5] = last ? rel_hi : 0;
                         S->meta[6] = 0;
                         S->meta[7] = 0;
@@ -1026,36 +1133,33 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
         // waited for by this warp, so the slot's barrier is in this slab's phase.
         for (const unsigned jhi = (unsigned)S->meta[8] / SPL; jw <= jhi; jw++)
             if (!mbar_wait(&full[jw % NSL], (jw / NSL) & 1)) { fail(); return; }
-        const int nrf = S->meta[2], novf = S->meta[3], d0 = S->meta[0];
-        const int total = nrf + (novf + 31) / 32;
-        const int mycnt = min(S->cnt[lane], CAP);
+        const int ntask = S->meta[2], d0 = S->meta[0];
+        const int total = (ntask + 31) / 32;
         for (;;) {
             int g = 0;
             if (lane == 0) g = atomicAdd(&S->meta[7], 1);
             g = __shfl_sync(0xffffffffu, g, 0);
             if (g >= total) break;
-            int t = -1;
-            if (g < nrf) {
-                if (g < mycnt) t = S->task[g * 32 + lane];
-            } else {
-                const int q = (g - nrf) * 32 + lane;
-                if (q < novf) t = S->ovf[q];
-            }
-            if (t >= 0) {
+            const int q = g * 32 + lane;
+            if (q < ntask) {
+                const int t = S->task[q];
                 const int i = t >> 2, cc = t & 3;
-                const float4 f = S->fr[i];
-                const int co = __float_as_int(f.w);
-                float bx[6], by[6], bz[6];
-                lagrange6(f.x, bx);
-                lagrange6(f.y, by);
-                lagrange6(f.z, bz);
-                RingLoader ld;
+                const int co = S->co[i];
+                RingLoader<T> ld;
                 const int off = cc * BOX + (co & 0xfff);
                 unsigned u = (unsigned)co >> 12;
 #pragma unroll
                 for (int k = 0; k < 6; k++, u++)
                     ld.pl[k] = ring + (size_t)((u / SPL) % NSL) * SLAB + (u % SPL) * PS + off;
-                A.vp[clo + cc][d0 + i] = stencil_planes(ld, bx, by, bz);
+                if constexpr (F64) {
+                    A.vp[clo + cc][d0 + i] = col_stencil_w(ld, S->w[i]);
+                } else {
+                    T bx[6], by[6], bz[6];
+                    lagrange6(S->w[i][0], bx);
+                    lagrange6(S->w[i][1], by);
+                    lagrange6(S->w[i][2], bz);
+                    A.vp[clo + cc][d0 + i] = col_stencil(ld, bx, by, bz);
+                }
             }
         }
         __syncwarp();
@@ -1363,15 +1467,26 @@ __global__ void k_mean_vel(int nps, const T *ux, const T *uy, const T *uz, const
         if (sacc[i] != 0.0) atomicAdd(&acc[i], sacc[i]);
 }
 
-// brick / pipeline configuration per precision: brick cells, component shifts (bank
-// spreading), TMA stages, droplets per chunk, consumer groups x warps per group
-// mixed precision: column sweep (columns of colk::CX x colk::CY cells), ring of COL_NSL
-// slabs of colk::SPL planes, batches of COL_PZ planes (three consecutive batch windows of
-// COL_PZ + 7 planes fit the ring) and at most COL_MAXD droplets, COL_NP batch slots,
-// COL_NSW stencil warps
-constexpr int COL_NSL = 7, COL_PZ = 8, COL_MAXD = 160, COL_NP = 3, COL_NSW = 11;
-constexpr int F64_BX = 8, F64_BY = 8, F64_BZ = 8, F64_XS = 2, F64_YS = 0, F64_M = 1, F64_S = 5, F64_MAXD = 64;
-constexpr int F64_NG = 2, F64_GW = 6;
+// Column sweep configuration per precision (columns of ColGeo<T>::CX x CY cells): a ring
+// of NSL slabs of colk::SPL planes, batches of PZ planes and at most MAXD droplets, NP
+// batch slots, NSW stencil warps.  A batch's window (PZ + 7 planes) spans at most
+// (PZ + 9) / 4 + 1 slabs, which must leave the ring a slab to fill ahead.
+template <typename T>
+struct ColCfg;
+template <>
+struct ColCfg<float> {
+    static constexpr int NSL = 7, PZ = 8, MAXD = 160, NP = 3, NSW = 11;
+};
+template <>
+struct ColCfg<double> {
+    static constexpr int NSL = 5, PZ = 6, MAXD = 64, NP = 3, NSW = 11;
+};
+template <typename T>
+constexpr bool col_cfg_ok()
+{
+    return (ColCfg<T>::PZ + 9) / colk::SPL + 1 < ColCfg<T>::NSL;
+}
+static_assert(col_cfg_ok<float>() && col_cfg_ok<double>(), "a batch window leaves a slab of the ring free");
 
 template <typename T>
 T *tp(void *p) { return reinterpret_cast<T *>(p); }
@@ -1395,7 +1510,7 @@ int launch_brick_sort(dl_ctx *c)
     DL_CUDA(c, cudaMemsetAsync(c->brick_cnt, 0, sizeof(int) * nkeys, c->stream));
     const double *P[3] = {c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2]};
     k_brick_keys<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, P[0], P[1], P[2], c->dc.dx, c->dc.n, c->bx, c->by,
-                                                         c->bz, c->nbx, c->nby, c->nbz, c->mixed, c->keys,
+                                                         c->bz, c->nbx, c->nby, c->nbz, c->bz == 1, c->keys,
                                                          c->brick_cnt, c->rad, c->has_dead ? c->nbricks : -1);
     DL_CHECK_LAUNCH(c);
     k_scan_single<<<1, 1024, 0, c->stream>>>(c->brick_cnt, c->brick_start, nkeys);
@@ -1473,9 +1588,9 @@ static int make_tmap(dl_ctx *c, CUtensorMap *map, int box_x, int box_y, int box_
     return 0;
 }
 
-// TMA descriptor of the FP32 halo-padded field with the dimensions ordered x, y, component,
-// z (strides need not grow with the dimension), so that a box of several planes lands in
-// shared memory as [plane][component][y][x]
+// TMA descriptor of the halo-padded field (FP32 or FP64) with the dimensions ordered x, y,
+// component, z (strides need not grow with the dimension), so that a box of several planes
+// lands in shared memory as [plane][component][y][x]
 static int make_tmap_zc(dl_ctx *c, CUtensorMap *map, int box_x, int box_y, int box_c, int box_z)
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -1493,7 +1608,8 @@ static int make_tmap_zc(dl_ctx *c, CUtensorMap *map, int box_x, int box_y, int b
     cuuint64_t strides[3] = {(cuuint64_t)c->fp_pitch * es, (cuuint64_t)c->fp_comp * es, (cuuint64_t)c->fp_plane * es};
     cuuint32_t box[4] = {(cuuint32_t)box_x, (cuuint32_t)box_y, (cuuint32_t)box_c, (cuuint32_t)box_z};
     cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, c->fpad, dims, strides, box, estr,
+    CUresult r = encode(map, c->mixed ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
+                        c->fpad, dims, strides, box, estr,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return dl_fail(c, DL_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
@@ -1580,17 +1696,19 @@ static int launch_interp_t(dl_ctx *c, int comp_lo, int ncomp, int fused)
     return 0;
 }
 
+template <typename T>
 static int launch_interp_col(dl_ctx *c, int comp_lo, int ncomp, int fused)
 {
+    using Cf = ColCfg<T>;
     if (c->tmap_base != c->fpad) {
         // one box per slab: colk::SPL planes of all three components, or of the single
         // component of a one-component INTERPOLATE call; dimensions ordered x, y, component, z
-        int r = make_tmap_zc(c, &c->tmap, colk::EX, colk::EY, 3, colk::SPL);
-        if (!r) r = make_tmap_zc(c, &c->tmap1, colk::EX, colk::EY, 1, colk::SPL);
+        int r = make_tmap_zc(c, &c->tmap, colk::G<T>::EX, colk::G<T>::EY, 3, colk::SPL);
+        if (!r) r = make_tmap_zc(c, &c->tmap1, colk::G<T>::EX, colk::G<T>::EY, 1, colk::SPL);
         if (r) return r;
         c->tmap_base = c->fpad;
     }
-    InterpArgs<float> A;
+    InterpArgs<T> A;
     memset(&A, 0, sizeof(A));
     A.n = c->dc.n;
     A.nps = c->nps;
@@ -1600,13 +1718,13 @@ static int launch_interp_col(dl_ctx *c, int comp_lo, int ncomp, int fused)
     A.px = c->pos[c->pcur][0]; A.py = c->pos[c->pcur][1]; A.pz = c->pos[c->pcur][2];
     A.brick_start = c->brick_start;
     A.nbx = c->nbx; A.nby = c->nby; A.nbricks = c->nbricks;
-    A.fpad = tp<float>(c->fpad);
+    A.fpad = tp<T>(c->fpad);
     A.fpy = c->fp_pitch;
     A.fpz = c->fp_plane;
     A.fpc = c->fp_comp;
-    for (int k = 0; k < 3; k++) A.vp[k] = tp<float>(c->vpv[k]);
+    for (int k = 0; k < 3; k++) A.vp[k] = tp<T>(c->vpv[k]);
     if (fused)   // the interpolated velocity goes straight into fdp(:,0) = F[fnew]
-        for (int k = 0; k < 3; k++) A.vp[k] = tp<float>(c->flu[(c->fcur + 3) % 4][k]);
+        for (int k = 0; k < 3; k++) A.vp[k] = tp<T>(c->flu[(c->fcur + 3) % 4][k]);
     A.comp_lo = comp_lo;
     A.ncomp = ncomp;
     A.err = c->d_err;
@@ -1626,41 +1744,41 @@ static int launch_interp_col(dl_ctx *c, int comp_lo, int ncomp, int fused)
         int nb = 0;
         for (int k = 0; k < nzs - 1; k++) A.band[nb++] = std::min(n, k * A.zseg);
         const int z0 = (nzs - 1) * A.zseg, rest = n - z0;
-        const int nthin = rest >= 4 * COL_PZ ? 4 : 1;
+        const int nthin = rest >= 4 * Cf::PZ ? 4 : 1;
         for (int k = 0; k < nthin; k++) A.band[nb++] = z0 + (int)((int64_t)rest * k / nthin);
         A.band[nb] = n;
         A.nband = nb;
-        A.zbatch = COL_PZ;
+        A.zbatch = Cf::PZ;
     }
-    constexpr size_t sm = col_smem<COL_NSL, COL_MAXD, COL_NP>();
+    constexpr size_t sm = col_smem<T, Cf::NSL, Cf::MAXD, Cf::NP>();
     static_assert(sm + 64 <= 227 * 1024, "shared memory budget");
-    auto kern = k_interp_col<COL_NSL, COL_MAXD, COL_NP, COL_NSW>;
+    auto kern = k_interp_col<T, Cf::NSL, Cf::MAXD, Cf::NP, Cf::NSW>;
     DL_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const int grid = c->num_sms;
-    kern<<<grid, (COL_NSW + colk::NPROD + 1 + colk::NPREP) * 32, sm, c->stream>>>(ncomp == 3 ? c->tmap : c->tmap1, A);
+    kern<<<grid, (Cf::NSW + colk::NPROD + 1 + colk::NPREP) * 32, sm, c->stream>>>(ncomp == 3 ? c->tmap : c->tmap1, A);
     DL_CHECK_LAUNCH(c);
     dl_mark_interp_end(c);
     if (fused) {
         // the advance epilogue: history, drag, position update, wrap, departure flags
-        InterpArgs<float> E = A;
+        InterpArgs<T> E = A;
         E.fused = 1;
         E.first = c->new_particle;
         E.init_mode = c->p.init_velocity;
         E.ndrag = c->dc.ndrag;
-        E.dt = (float)c->dc.dt; E.tau2 = (float)c->dc.tau2; E.sv = (float)c->dc.sv; E.rnu = (float)c->dc.rnu;
+        E.dt = (T)c->dc.dt; E.tau2 = (T)c->dc.tau2; E.sv = (T)c->dc.sv; E.rnu = (T)c->dc.rnu;
         E.rad = c->rad;
         c->vnew = (c->vcur + 3) % 4;
         c->fnew = (c->fcur + 3) % 4;
         for (int k = 0; k < 3; k++) {
-            E.v0[k] = tp<float>(c->vel[c->vcur][k]);
-            E.v1[k] = tp<float>(c->vel[(c->vcur + 1) % 4][k]);
-            E.v2[k] = tp<float>(c->vel[(c->vcur + 2) % 4][k]);
-            E.vnew[k] = tp<float>(c->vel[c->vnew][k]);
-            E.f1[k] = tp<float>(c->flu[c->fcur][k]);
-            E.f2[k] = tp<float>(c->flu[(c->fcur + 1) % 4][k]);
-            E.f3[k] = tp<float>(c->flu[(c->fcur + 2) % 4][k]);
-            E.fnew[k] = tp<float>(c->flu[c->fnew][k]);
-            E.dmv[k] = tp<float>(c->dmv[k]);
+            E.v0[k] = tp<T>(c->vel[c->vcur][k]);
+            E.v1[k] = tp<T>(c->vel[(c->vcur + 1) % 4][k]);
+            E.v2[k] = tp<T>(c->vel[(c->vcur + 2) % 4][k]);
+            E.vnew[k] = tp<T>(c->vel[c->vnew][k]);
+            E.f1[k] = tp<T>(c->flu[c->fcur][k]);
+            E.f2[k] = tp<T>(c->flu[(c->fcur + 1) % 4][k]);
+            E.f3[k] = tp<T>(c->flu[(c->fcur + 2) % 4][k]);
+            E.fnew[k] = tp<T>(c->flu[c->fnew][k]);
+            E.dmv[k] = tp<T>(c->dmv[k]);
         }
         E.qx = c->pos[1 - c->pcur][0]; E.qy = c->pos[1 - c->pcur][1]; E.qz = c->pos[1 - c->pcur][2];
         E.ref_of_dev = c->ref_of_dev;
@@ -1669,11 +1787,11 @@ static int launch_interp_col(dl_ctx *c, int comp_lo, int ncomp, int fused)
         E.lv_n = c->lv_n;
         static bool carve = false;
         if (!carve) {
-            cudaFuncSetAttribute(k_advance_fused<float>, cudaFuncAttributePreferredSharedMemoryCarveout,
+            cudaFuncSetAttribute(k_advance_fused<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  (int)cudaSharedmemCarveoutMaxShared);
             carve = true;
         }
-        k_advance_fused<float><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(E);
+        k_advance_fused<T><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(E);
         DL_CHECK_LAUNCH(c);
     }
     return 0;
@@ -1683,15 +1801,14 @@ int launch_interp(dl_ctx *c, int icpt, int fused)
 {
     if (c->nps == 0) return 0;
     int lo = icpt > 0 ? icpt - 1 : 0, nc = icpt > 0 ? 1 : 3;
-    if (c->mixed) return launch_interp_col(c, lo, nc, fused);
-    return launch_interp_t<double, F64_BX, F64_BY, F64_BZ, F64_XS, F64_YS, F64_M, F64_S, F64_MAXD, F64_NG, F64_GW>(
-        c, lo, nc, fused);
+    return c->mixed ? launch_interp_col<float>(c, lo, nc, fused) : launch_interp_col<double>(c, lo, nc, fused);
 }
 
 void dl_brick_dims(int mixed, int *bx, int *by, int *bz)
 {
-    if (mixed) { *bx = colk::CX; *by = colk::CY; *bz = 1; }   // columns, sorted by z plane
-    else { *bx = F64_BX; *by = F64_BY; *bz = F64_BZ; }
+    // columns, sorted by z plane
+    if (mixed) { *bx = ColGeo<float>::CX; *by = ColGeo<float>::CY; *bz = 1; }
+    else { *bx = ColGeo<double>::CX; *by = ColGeo<double>::CY; *bz = 1; }
 }
 
 int launch_prepare_interp(dl_ctx *c)
