@@ -1162,6 +1162,28 @@ def run_only(args):
         ms, kms, launches, ims, ams = _time_update(g, stream, args.steps, args.warmup, torch)
         out.update(ms_per_step=ms, kernel_ms=kms, launches=launches, interp_ms=ims, advance_ms=ams)
         g.close()
+    elif args.only == "step":
+        # the full mixed particle substep without HDI (cell list, collision detection and
+        # statistics) on the headline workload
+        field = spectral_field(N_GRID, seed=1234, device="cuda:0")
+        g = _make("mixed", 0)
+        stream = torch.cuda.Stream()
+        g.set_stream(stream)
+        g.set_fields(*field)
+        g.sync()
+        for _ in range(args.warmup):
+            g.particle_step()
+        ts, ph = [], []
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rep, _ = g.particle_step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+            ph.append(g.phase_times().tolist())
+        out.update(step_ms=statistics.median(ts), phase_ms=ph[-1], candidates=int(rep.candidate_pairs))
+        g.close()
     elif args.only == "adjoint":
         out.update(adjoint_bench(0, torch))
     elif args.only == "full":
@@ -1212,7 +1234,7 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="skip the 64^3 and 128^3 workloads")
     ap.add_argument("--ref-sample", type=int, default=200_000,
                     help="droplets per step of the reference arm's CPU sample")
-    ap.add_argument("--only", choices=["update", "update-fp64", "adjoint", "full", "config4", "configs"],
+    ap.add_argument("--only", choices=["update", "update-fp64", "step", "adjoint", "full", "config4", "configs"],
                     help="run one workload alone (for profilers)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

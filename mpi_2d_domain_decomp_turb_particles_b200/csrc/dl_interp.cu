@@ -673,7 +673,6 @@ namespace colk {
 constexpr int M = 1;                             // y drift tolerated since the last sort (cells)
 constexpr int SPL = 4;                           // planes per slab (one TMA box)
 constexpr int NPROD = 1;                         // producer warps (slab j goes to the producer of slot j % NSL)
-constexpr int NPREP = 3;                         // prep warps (batches go round them)
 template <typename T>
 struct G {
     static constexpr int CX = ColGeo<T>::CX, CY = ColGeo<T>::CY;
@@ -688,17 +687,26 @@ struct G {
 };
 }  // namespace colk
 
+// Round order of a batch's tasks (droplet << 2 | component slot):
+//  * FP32, per bucket: round g gives lane r entry g of bucket r (conflict-free; a round has
+//    idle lanes where buckets hold fewer than the fullest one), then the overflow tasks;
+//  * FP64, dense layer-major: entry 0 of every bucket holding one, buckets ascending, then
+//    entry 1, ...  Any 16 consecutive tasks (a half-warp's share) take each bucket at most
+//    once from a full layer and at most twice where the layers thin out, and every round is
+//    full: an FP64 term costs four FP64-pipe instructions against one 64-bit load, so full
+//    warps matter more there than the two-way conflicts.
 template <typename T, int MAXD>
 struct ColBatch {   // per-batch shared-memory area
+    static constexpr bool DENSE = sizeof(T) == 8;
+    static constexpr int CAP = ColGeo<T>::CAP;
     T w[MAXD][ColGeo<T>::NW];                 // FP32: x, y, z fractions; FP64: the weights
     int co[MAXD];                             // corner | first plane << 12, or -1 (global-memory path)
-    int meta[16];   // d0, nd, tasks, overflow tasks, release lo, hi, end, next round, window end
+    int meta[16];   // d0, nd, rounds or tasks, overflow tasks, release lo, hi, end, next round, window end
     int cnt[32];                              // tasks per bank bucket
-    unsigned lmask[ColGeo<T>::CAP];           // layer e: the buckets holding an entry e
-    int loff[ColGeo<T>::CAP];                 // layer e: its first position in the task list
-    // the tasks (droplet << 2 | component slot) in layer-major order: entry 0 of every
-    // bucket holding one, buckets ascending, then entry 1, ...; then the overflow tasks
-    unsigned short task[MAXD * 3];
+    unsigned lmask[DENSE ? CAP : 1];          // layer e: the buckets holding an entry e
+    int loff[DENSE ? CAP : 1];                // layer e: its first position in the task list
+    unsigned short task[DENSE ? MAXD * 3 : 32 * CAP];   // per bucket: entry e of bucket r at e * 32 + r
+    unsigned short ovf[DENSE ? 1 : MAXD * 3];           // per bucket: the overflow tasks
 };
 
 template <typename T, int NSL, int MAXD, int NP>
@@ -762,12 +770,17 @@ struct RingLoader {
     __device__ __forceinline__ T operator()(int a, int b, int k) const { return pl[k][b * colk::G<T>::EX + a]; }
 };
 
-template <typename T, int NSL, int MAXD, int NP, int NSW>
-__global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
+template <typename T, int NSL, int MAXD, int NP, int NSW, int NPREP>
+__global__ void __launch_bounds__((NSW + colk::NPROD + 1 + NPREP) * 32, 1)
     k_interp_col(const __grid_constant__ CUtensorMap tmap, InterpArgs<T> A)
 {
     using namespace colk;
     using B = ColBatch<T, MAXD>;
+    // A prep warp waits for batch b's slot by the parity of the slot's previous release
+    // (batch b - NP).  That wait is exact only when the same warp prepared batch b - NP (it
+    // then knows that the release before it completed): batches go round the prep warps, so
+    // NP must be a multiple of NPREP.
+    static_assert(NP % NPREP == 0, "batch slots per prep warp");
     constexpr int CX = G<T>::CX, CY = G<T>::CY, EX = G<T>::EX, EY = G<T>::EY, BOX = G<T>::BOX;
     constexpr int SLAB = G<T>::SLAB, NBK = G<T>::NBK, CAP = G<T>::CAP;
     constexpr bool F64 = sizeof(T) == 8;
@@ -1067,36 +1080,51 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
                         S->co[i] = co;
                     }
                     __syncwarp();
-                    // the layers of the buckets: layer e holds entry e of every bucket that has
-                    // one, in bucket order.  Any 32 consecutive tasks of that order (16 for FP64,
-                    // a half-warp's share) take each bucket at most once from a full layer, and
-                    // at most twice where the layers thin out; every round is full.
                     const int cown = lane < NBK ? min(S->cnt[lane], CAP) : 0;
                     int nl = cown;
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) nl = max(nl, __shfl_xor_sync(0xffffffffu, nl, o));
-                    int ndense = 0;
-                    for (int e = 0; e < nl; e++) {
-                        const unsigned m = __ballot_sync(0xffffffffu, cown > e);
-                        if (lane == 0) { S->lmask[e] = m; S->loff[e] = ndense; }
-                        ndense += __popc(m);
-                    }
-                    __syncwarp();
-#pragma unroll
-                    for (int q = 0; q < QN; q++)
-#pragma unroll
-                        for (int cc = 0; cc < 3; cc++) {
-                            const int ek = ent[q][cc];
-                            if (ek < 0) continue;
-                            const int e = ek >> 8, key = ek & 0xff;
-                            const unsigned short tk = (unsigned short)(((q * 32 + lane) << 2) | cc);
-                            const int pos = e < CAP ? S->loff[e] + __popc(S->lmask[e] & ((1u << key) - 1u))
-                                                    : ndense + atomicAdd(&S->meta[3], 1);
-                            S->task[pos] = tk;
+                    int nround = 0;
+                    if constexpr (B::DENSE) {
+                        // layer e: entry e of every bucket holding one, in bucket order
+                        int ndense = 0;
+                        for (int e = 0; e < nl; e++) {
+                            const unsigned m = __ballot_sync(0xffffffffu, cown > e);
+                            if (lane == 0) { S->lmask[e] = m; S->loff[e] = ndense; }
+                            ndense += __popc(m);
                         }
-                    __syncwarp();
+                        __syncwarp();
+#pragma unroll
+                        for (int q = 0; q < QN; q++)
+#pragma unroll
+                            for (int cc = 0; cc < 3; cc++) {
+                                const int ek = ent[q][cc];
+                                if (ek < 0) continue;
+                                const int e = ek >> 8, key = ek & 0xff;
+                                const unsigned short tk = (unsigned short)(((q * 32 + lane) << 2) | cc);
+                                const int pos = e < CAP ? S->loff[e] + __popc(S->lmask[e] & ((1u << key) - 1u))
+                                                        : ndense + atomicAdd(&S->meta[3], 1);
+                                S->task[pos] = tk;
+                            }
+                        __syncwarp();
+                        nround = ndense + S->meta[3];   // tasks
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < QN; q++)
+#pragma unroll
+                            for (int cc = 0; cc < 3; cc++) {
+                                const int ek = ent[q][cc];
+                                if (ek < 0) continue;
+                                const int e = ek >> 8, key = ek & 0xff;
+                                const unsigned short tk = (unsigned short)(((q * 32 + lane) << 2) | cc);
+                                if (e < CAP) S->task[e * 32 + key] = tk;
+                                else S->ovf[atomicAdd(&S->meta[3], 1)] = tk;
+                            }
+                        __syncwarp();
+                        nround = nl;   // full rounds (lane r: bucket r)
+                    }
                     if (lane == 0) {
-                        S->meta[0] = d0; S->meta[1] = nd; S->meta[2] = ndense + S->meta[3];
+                        S->meta[0] = d0; S->meta[1] = nd; S->meta[2] = nround;
                         S->meta[5] = last ? rel_hi : 0;
                         S->meta[6] = 0;
                         S->meta[7] = 0;
@@ -1133,16 +1161,26 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + colk::NPREP) * 32, 1)
         // waited for by this warp, so the slot's barrier is in this slab's phase.
         for (const unsigned jhi = (unsigned)S->meta[8] / SPL; jw <= jhi; jw++)
             if (!mbar_wait(&full[jw % NSL], (jw / NSL) & 1)) { fail(); return; }
-        const int ntask = S->meta[2], d0 = S->meta[0];
-        const int total = (ntask + 31) / 32;
+        const int d0 = S->meta[0];
+        // DENSE: meta[2] tasks; per bucket: meta[2] full rounds, then the overflow tasks
+        const int ntask = S->meta[2], novf = S->meta[3];
+        const int mycnt = B::DENSE ? 0 : min(S->cnt[lane], CAP);
+        const int total = B::DENSE ? (ntask + 31) / 32 : ntask + (novf + 31) / 32;
         for (;;) {
             int g = 0;
             if (lane == 0) g = atomicAdd(&S->meta[7], 1);
             g = __shfl_sync(0xffffffffu, g, 0);
             if (g >= total) break;
-            const int q = g * 32 + lane;
-            if (q < ntask) {
-                const int t = S->task[q];
+            int t = -1;
+            if constexpr (B::DENSE) {
+                if (g * 32 + lane < ntask) t = S->task[g * 32 + lane];
+            } else if (g < ntask) {
+                if (g < mycnt) t = S->task[g * 32 + lane];
+            } else {
+                const int q = (g - ntask) * 32 + lane;
+                if (q < novf) t = S->ovf[q];
+            }
+            if (t >= 0) {
                 const int i = t >> 2, cc = t & 3;
                 const int co = S->co[i];
                 RingLoader<T> ld;
@@ -1469,17 +1507,17 @@ __global__ void k_mean_vel(int nps, const T *ux, const T *uy, const T *uz, const
 
 // Column sweep configuration per precision (columns of ColGeo<T>::CX x CY cells): a ring
 // of NSL slabs of colk::SPL planes, batches of PZ planes and at most MAXD droplets, NP
-// batch slots, NSW stencil warps.  A batch's window (PZ + 7 planes) spans at most
-// (PZ + 9) / 4 + 1 slabs, which must leave the ring a slab to fill ahead.
+// batch slots, NSW stencil warps, NPREP prep warps.  A batch's window (PZ + 7 planes) spans
+// at most (PZ + 9) / 4 + 1 slabs, which must leave the ring a slab to fill ahead.
 template <typename T>
 struct ColCfg;
 template <>
 struct ColCfg<float> {
-    static constexpr int NSL = 7, PZ = 8, MAXD = 160, NP = 3, NSW = 11;
+    static constexpr int NSL = 7, PZ = 8, MAXD = 160, NP = 3, NSW = 11, NPREP = 3;
 };
 template <>
 struct ColCfg<double> {
-    static constexpr int NSL = 5, PZ = 6, MAXD = 64, NP = 3, NSW = 11;
+    static constexpr int NSL = 5, PZ = 6, MAXD = 64, NP = 4, NSW = 10, NPREP = 4;
 };
 template <typename T>
 constexpr bool col_cfg_ok()
@@ -1752,10 +1790,10 @@ static int launch_interp_col(dl_ctx *c, int comp_lo, int ncomp, int fused)
     }
     constexpr size_t sm = col_smem<T, Cf::NSL, Cf::MAXD, Cf::NP>();
     static_assert(sm + 64 <= 227 * 1024, "shared memory budget");
-    auto kern = k_interp_col<T, Cf::NSL, Cf::MAXD, Cf::NP, Cf::NSW>;
+    auto kern = k_interp_col<T, Cf::NSL, Cf::MAXD, Cf::NP, Cf::NSW, Cf::NPREP>;
     DL_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const int grid = c->num_sms;
-    kern<<<grid, (Cf::NSW + colk::NPROD + 1 + colk::NPREP) * 32, sm, c->stream>>>(ncomp == 3 ? c->tmap : c->tmap1, A);
+    kern<<<grid, (Cf::NSW + colk::NPROD + 1 + Cf::NPREP) * 32, sm, c->stream>>>(ncomp == 3 ? c->tmap : c->tmap1, A);
     DL_CHECK_LAUNCH(c);
     dl_mark_interp_end(c);
     if (fused) {
