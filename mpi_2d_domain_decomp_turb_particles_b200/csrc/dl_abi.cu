@@ -513,7 +513,7 @@ extern "C" int dl_destroy(dl_ctx *c)
     F(c->ent_row); F(c->ent_ix); F(c->row_start); F(c->row_fill); F(c->row_ent); F(c->leave_nid);
     F(c->lv_refs); F(c->lv_old); F(c->lv_new); F(c->lv_dev); F(c->lv_dep); F(c->d_err); F(c->col_work);
     F(c->xfer64); F(c->xfer_i); F(c->hist_i); F(c->hist_d); F(c->acc_i); F(c->acc_d); F(c->out_i); F(c->out_d);
-    F(c->counts); F(c->cand); F(c->pairs); F(c->contacts); F(c->remove_dev); F(c->pair_buf); F(c->pair_ibuf); F(c->mv_acc);
+    F(c->counts); F(c->cand); F(c->coll_list); F(c->coll_n); F(c->coll_flag); F(c->pairs); F(c->contacts); F(c->remove_dev); F(c->pair_buf); F(c->pair_ibuf); F(c->mv_acc);
     F(c->ovl_list); F(c->ovl_cnt); F(c->fpad_own);
     F(c->nei_cnt); F(c->nei_start); F(c->nei_idx); F(c->nei_coef); F(c->nei_coef64); F(c->overlap_flag);
     F(c->kry); F(c->xg); F(c->rg); F(c->bg64); F(c->tmp64); F(c->wv); F(c->xt); F(c->dots); F(c->arn); F(c->co_buf); F(c->scan_buf); F(c->rmax_dev);

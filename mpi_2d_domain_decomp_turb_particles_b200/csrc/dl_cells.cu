@@ -341,34 +341,55 @@ struct CollArgs {
     int contact_cap;
     int *remove;
     int remove_cap;
+    int4 *clist;          // candidate pairs: sorted entry of the owner, of the partner, loop key, x shift
+    int *cn;              // candidates written (may exceed ccap: then the list is enlarged)
+    int ccap;
+    int *cflag;           // owner already on the removal list
 };
 
-// COLLISION_DET body for one owned droplet ih1 (partlib.f90:1233-1590), the droplet of
-// sorted entry sa; returns the candidates it visited.
+constexpr int COLL_SBUF = 1024;   // block buffer of the search pass (candidates)
+
+// COLLISION_DET (partlib.f90:1233-1590) in two passes over the sorted entries.
+//
+// Search: one thread per owned droplet ih1 (sorted entry sa) visits the partner entries of
+// the (2 imax + 1) x (2 jmax + 1) x (2 kmax + 1) cells the reference visits, owned partners
+// only with ih2 > ih1, and appends to a compact list every partner within the statistics
+// reach (10 (a_i + a_j), which holds the contact shell) or, in a neighbouring cell, within
+// the detection reach a_i + a_j + |dmove_i| + |dmove_j| -- the same expressions the
+// evaluation tests, so the list holds exactly the pairs that contribute.  The thread
+// reads only the packed positions (and a partner's displacement in the rare case beyond
+// the statistics reach), and the list goes through a block-local buffer in shared memory.
+//
+// Evaluation: one thread per listed pair computes the statistics, the contact record and
+// the trajectory tests with the reference's arithmetic; every output slot is taken by an
+// atomic and the detection order is restored afterwards by the loop key, as before.  An
+// owner goes on the removal list once (flag per droplet), after its first collision.
 template <typename T>
-__device__ __forceinline__ unsigned collision_owner(const CollArgs<T> &A, int sa)
+__device__ __forceinline__ unsigned coll_search(const CollArgs<T> &A, int sa, int4 *sbuf, int *sn)
 {
     const int4 ida = A.pk_id[sa];
     if (ida.w != 0) return 0u;   // a ghost owns no search
     const double4 pa = A.pk_x[sa];
     const int a = ida.x;
     const DevConst &D = A.D;
-    const int nset = D.nset;
-    double xa[3] = {pa.x, pa.y, pa.z}, xan[3], va[3], van[3], ua[3];
-    for (int i = 0; i < 3; i++) {
-        xan[i] = xa[i] + (double)A.dm[i][a];
-        va[i] = (double)A.vo[i][a];
-        van[i] = (double)A.vn[i][a];
-        ua[i] = (double)A.up[i][a];
-    }
+    const double xa[3] = {pa.x, pa.y, pa.z};
     const double ra = pa.w;
     const int refa = ida.y;
     const double dma[3] = {(double)A.dm[0][a], (double)A.dm[1][a], (double)A.dm[2][a]};
+    const double dmove_a = sqrt(dma[0] * dma[0] + dma[1] * dma[1] + dma[2] * dma[2]);
     int ix, iy, iz;
     own_cell(D, xa[0], xa[1], xa[2], ix, iy, iz);
-    int ncollip1 = 0;
     unsigned ncand = 0;
     const int nj = 2 * A.jmax + 1, nk = 2 * A.kmax + 1;
+    auto emit = [&](int4 r) {
+        const int k = atomicAdd(sn, 1);
+        if (k < COLL_SBUF) {
+            sbuf[k] = r;
+        } else {
+            const int g = atomicAdd(A.cn, 1);
+            if (g < A.ccap) A.clist[g] = r;
+        }
+    };
 
     for (int jj = -A.jmax; jj <= A.jmax; jj++) {
         const int iy2 = iy + jj;
@@ -383,17 +404,17 @@ __device__ __forceinline__ unsigned collision_owner(const CollArgs<T> &A, int sa
             const int lo_raw = ix - A.imax, hi_raw = ix + A.imax;
 #pragma unroll 1
             for (int q = 0; q < 3; q++) {
-                int lo, hi;
-                double sx;
+                int lo, hi, isx;
                 if (q == 0) {
-                    lo = max(1, lo_raw); hi = min(D.ncd, hi_raw); sx = 0.0;
+                    lo = max(1, lo_raw); hi = min(D.ncd, hi_raw); isx = 0;
                 } else if (q == 1) {
                     if (lo_raw >= 1) continue;
-                    lo = lo_raw + D.ncd; hi = D.ncd; sx = -1.0;
+                    lo = lo_raw + D.ncd; hi = D.ncd; isx = -1;
                 } else {
                     if (hi_raw <= D.ncd) continue;
-                    lo = 1; hi = hi_raw - D.ncd; sx = 1.0;
+                    lo = 1; hi = hi_raw - D.ncd; isx = 1;
                 }
+                const double sx = (double)isx;
                 int s0, s1;
                 cell_range(A.cell_start, D, row, lo, hi, s0, s1);
                 for (int s = s0; s < s1; s++) {
@@ -401,167 +422,229 @@ __device__ __forceinline__ unsigned collision_owner(const CollArgs<T> &A, int sa
                     const int ix2 = idb.z;
                     if (ix2 < lo) continue;
                     if (ix2 > hi) break;
-                    const int src = idb.x, jid = idb.w;
-                    if (jid == 0 && idb.y <= refa) continue;   // ih2 <= ih1
-                    const int e = jid == 0 ? src : idb.y;      // entry index (ghosts: nps + slot order)
-                    const double4 pb = A.pk_x[s];
-                    const double xb0[3] = {pb.x, pb.y, pb.z};
-                    const int ii = (sx == 0.0) ? ix2 - ix : (sx < 0.0 ? ix2 - D.ncd - ix : ix2 + D.ncd - ix);
+                    if (idb.w == 0 && idb.y <= refa) continue;   // ih2 <= ih1
+                    const int ii = isx == 0 ? ix2 - ix : (isx < 0 ? ix2 - D.ncd - ix : ix2 + D.ncd - ix);
                     ncand++;
-                    double xb[3], xbn[3], vb[3], xd[3];
-                    xb[0] = xb0[0] + sx * D.hx;
-                    xb[1] = xb0[1];
-                    xb[2] = xb0[2];
-                    const double dmb[3] = {(double)A.dm[0][src], (double)A.dm[1][src], (double)A.dm[2][src]};
-                    for (int i = 0; i < 3; i++) {
-                        xbn[i] = xb[i] + dmb[i];
-                        vb[i] = (double)A.vo[i][src];
-                        xd[i] = xa[i] - xb[i];
-                    }
+                    const double4 pb = A.pk_x[s];
+                    double xd[3];
+                    xd[0] = xa[0] - (pb.x + sx * D.hx);
+                    xd[1] = xa[1] - pb.y;
+                    xd[2] = xa[2] - pb.z;
                     const double dnij0 = sqrt(xd[0] * xd[0] + xd[1] * xd[1] + xd[2] * xd[2]);
-                    const double rb = pb.w;
-                    const double rcoll = ra + rb;
-                    const double rcolla = D.hdi ? rcoll : rcoll * (1.0 - D.st / 100.0);
-                    const double rcollb = rcoll * (1.0 + D.st / 100.0);
-                    int index1 = 1, index2 = 1;
-                    double wr = 0.0;
-                    const int loopkey = ((ii + A.imax) * nj + (jj + A.jmax)) * nk + (kk + A.kmax);
-                    if (dnij0 > rcolla && dnij0 <= 10 * rcoll) {
-                        if (dnij0 > rcoll) {
-                            for (int i = 0; i < 3; i++) xd[i] = xd[i] / dnij0;
-                            double vr1 = dot3(va, xd), vr2 = dot3(vb, xd);
-                            wr = vr1 - vr2;
-                            int ir = (int)((dnij0 - rcoll) / ((9.0 / (double)DL_NBIN) * rcoll));
-                            if (ir > DL_NBIN - 1) ir = DL_NBIN - 1;
-                            if (ir < 0) ir = 0;
-                            findindex(D, ra, rb, index1, index2);
-                            const int hb = (index1 - 1) + nset * ((index2 - 1) + nset * ir);
-                            atomicAdd(&A.hist_i[hb], 1);
-                            double dwx = 0.0, dwy = 0.0, dwz = 0.0;
-                            if (index2 == index1) { dwx = va[0] - vb[0]; dwy = va[1] - vb[1]; dwz = va[2] - vb[2]; }
-                            if (ra > rb) {
-                                dwx = dwx + (va[0] - vb[0]); dwy = dwy + (va[1] - vb[1]); dwz = dwz + (va[2] - vb[2]);
-                            } else if (ra < rb) {
-                                dwx = dwx + (vb[0] - va[0]); dwy = dwy + (vb[1] - va[1]); dwz = dwz + (vb[2] - va[2]);
-                            }
-                            double *H = A.hist_d;
-                            const int nb = A.nbinsz;
-                            atomicAdd(&H[0 * nb + hb], wr);
-                            atomicAdd(&H[1 * nb + hb], dwx);
-                            atomicAdd(&H[2 * nb + hb], dwy);
-                            atomicAdd(&H[3 * nb + hb], dwz);
-                            double du[3], dv[3];
-                            for (int i = 0; i < 3; i++) {
-                                du[i] = ua[i] - (double)A.up[i][src];
-                                dv[i] = va[i] - vb[i];
-                            }
-                            atomicAdd(&H[4 * nb + hb], dot3(du, xd));
-                            double aaa = dot3(dv, xd);
-                            double bbb = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
-                            if (bbb != 0.0) {
-                                double vangle = acos(fabs(aaa / bbb));
-                                atomicAdd(&H[5 * nb + hb], vangle);
-                                double sv = bbb * sin(vangle);
-                                atomicAdd(&H[6 * nb + hb], sv * sv / dnij0);
-                            }
-                        }
-                        if (dnij0 <= rcollb) {
-                            if (dnij0 <= rcoll) {
-                                for (int i = 0; i < 3; i++) xd[i] = xd[i] / dnij0;
-                                double vr1 = dot3(va, xd), vr2 = dot3(vb, xd);
-                                wr = vr1 - vr2;
-                                findindex(D, ra, rb, index1, index2);
-                            }
-                            atomicAdd(&A.counts[8 + nset * nset + (index1 - 1) + nset * (index2 - 1)], 1);
-                            int slot = atomicAdd(&A.counts[4], 1);
-                            if (slot < A.contact_cap) {
-                                ContactRec &cr = A.contacts[slot];
-                                cr.a = a; cr.b = e; cr.loopkey = loopkey; cr.pad = 0;
-                                cr.rec[0] = (double)index1;
-                                cr.rec[1] = (double)index2;
-                                for (int i = 0; i < 3; i++) {
-                                    cr.rec[2 + i] = va[i];
-                                    cr.rec[5 + i] = vb[i];
-                                    cr.rec[8 + i] = xd[i];
-                                }
-                                cr.rec[11] = wr;
-                            } else {
-                                A.counts[6] = 1;
-                            }
-                        }
+                    const double rcoll = ra + pb.w;
+                    bool keep = dnij0 <= 10 * rcoll;
+                    if (!keep && abs(ii) <= 1 && abs(jj) <= 1 && abs(kk) <= 1) {
+                        const int src = idb.x;
+                        const double dmb[3] = {(double)A.dm[0][src], (double)A.dm[1][src], (double)A.dm[2][src]};
+                        const double dmove_b = sqrt(dmb[0] * dmb[0] + dmb[1] * dmb[1] + dmb[2] * dmb[2]);
+                        keep = dnij0 <= rcoll + dmove_a + dmove_b;
                     }
-                    // detection, neighbouring cells only (partlib.f90:1445-1518)
-                    if (abs(ii) > 1 || abs(jj) > 1 || abs(kk) > 1) continue;
-                    const double dmove_a = sqrt(dma[0] * dma[0] + dma[1] * dma[1] + dma[2] * dma[2]);
-                    const double dmove_b = sqrt(dmb[0] * dmb[0] + dmb[1] * dmb[1] + dmb[2] * dmb[2]);
-                    const double tmove = rcoll + dmove_a + dmove_b;
-                    if (dnij0 > tmove) continue;
-                    for (int i = 0; i < 3; i++) xd[i] = xan[i] - xbn[i];
-                    const double dnij1 = sqrt(xd[0] * xd[0] + xd[1] * xd[1] + xd[2] * xd[2]);
-                    if (dnij0 < rcoll && dnij1 > rcoll) continue;
-                    int hit = 0;
-                    if (dnij0 > rcoll && dnij1 <= rcoll) {
-                        hit = 1;
-                    } else {
-                        double vbn[3];
-                        for (int i = 0; i < 3; i++) vbn[i] = (double)A.vn[i][src];
-                        for (int icheck = 1; icheck <= 19; icheck++) {
-                            const double tfac = 0.05 * (double)icheck;
-                            const double tfac1 = D.dt * tfac;
-                            const double tfac2 = tfac * tfac;
-                            const double tfac3 = tfac2 * tfac;
-                            double dd[3];
-                            for (int i = 0; i < 3; i++) {
-                                double xta = xa[i] + va[i] * tfac1 + (3.0 * dma[i] - (2.0 * va[i] + van[i]) * D.dt) * tfac2 +
-                                             ((van[i] + va[i]) * D.dt - 2.0 * dma[i]) * tfac3;
-                                double xtb = xb[i] + vb[i] * tfac1 + (3.0 * dmb[i] - (2.0 * vb[i] + vbn[i]) * D.dt) * tfac2 +
-                                             ((vbn[i] + vb[i]) * D.dt - 2.0 * dmb[i]) * tfac3;
-                                dd[i] = xta - xtb;
-                            }
-                            const double dnij = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
-                            if (dnij0 > rcoll && dnij < rcoll) { hit = 2; break; }
-                            if (dnij1 <= rcoll && dnij > rcoll) { hit = 3; break; }
-                        }
-                    }
-                    if (!hit) continue;
-                    ncollip1++;
-                    atomicAdd(&A.counts[hit - 1], 1);
-                    findindex(D, ra, rb, index1, index2);
-                    atomicAdd(&A.counts[8 + (index1 - 1) + nset * (index2 - 1)], 1);
-                    int ps = atomicAdd(&A.counts[3], 1);
-                    if (ps < A.pair_cap) {
-                        A.pairs[ps].a = a; A.pairs[ps].b = e; A.pairs[ps].type = hit; A.pairs[ps].loopkey = loopkey;
-                    } else {
-                        A.counts[6] = 1;
-                    }
-                    // removal lists (partlib.f90:1527-1553): owned partner, or a ghost of slots 5..8
-                    if (jid == 0 || jid >= 5) {
-                        int rs2 = atomicAdd(&A.counts[5], 1);
-                        if (rs2 < A.remove_cap) A.remove[rs2] = A.ref[src] + 1;
-                        else A.counts[6] = 1;
+                    if (keep) {
+                        const int loopkey = ((ii + A.imax) * nj + (jj + A.jmax)) * nk + (kk + A.kmax);
+                        emit(make_int4(sa, s, loopkey, isx));
                     }
                 }
             }
         }
     }
-    if (ncollip1 != 0) {
+    return ncand;
+}
+
+template <typename T>
+__device__ __forceinline__ void coll_pair(const CollArgs<T> &A, int4 r)
+{
+    const int sa = r.x, s = r.y, loopkey = r.z;
+    const double sx = (double)r.w;
+    const int nj = 2 * A.jmax + 1, nk = 2 * A.kmax + 1;
+    const int kk = loopkey % nk - A.kmax, jj = (loopkey / nk) % nj - A.jmax, ii = loopkey / (nk * nj) - A.imax;
+    const int4 ida = A.pk_id[sa];
+    const double4 pa = A.pk_x[sa];
+    const int a = ida.x;
+    const DevConst &D = A.D;
+    const int nset = D.nset;
+    double xa[3] = {pa.x, pa.y, pa.z}, xan[3], va[3], van[3], ua[3];
+    for (int i = 0; i < 3; i++) {
+        xan[i] = xa[i] + (double)A.dm[i][a];
+        va[i] = (double)A.vo[i][a];
+        van[i] = (double)A.vn[i][a];
+        ua[i] = (double)A.up[i][a];
+    }
+    const double ra = pa.w;
+    const int refa = ida.y;
+    const double dma[3] = {(double)A.dm[0][a], (double)A.dm[1][a], (double)A.dm[2][a]};
+    const int4 idb = A.pk_id[s];
+    const int src = idb.x, jid = idb.w;
+    const int e = jid == 0 ? src : idb.y;      // entry index (ghosts: nps + slot order)
+    const double4 pb = A.pk_x[s];
+    const double xb0[3] = {pb.x, pb.y, pb.z};
+    double xb[3], xbn[3], vb[3], xd[3];
+    xb[0] = xb0[0] + sx * D.hx;
+    xb[1] = xb0[1];
+    xb[2] = xb0[2];
+    const double dmb[3] = {(double)A.dm[0][src], (double)A.dm[1][src], (double)A.dm[2][src]};
+    for (int i = 0; i < 3; i++) {
+        xbn[i] = xb[i] + dmb[i];
+        vb[i] = (double)A.vo[i][src];
+        xd[i] = xa[i] - xb[i];
+    }
+    const double dnij0 = sqrt(xd[0] * xd[0] + xd[1] * xd[1] + xd[2] * xd[2]);
+    const double rb = pb.w;
+    const double rcoll = ra + rb;
+    const double rcolla = D.hdi ? rcoll : rcoll * (1.0 - D.st / 100.0);
+    const double rcollb = rcoll * (1.0 + D.st / 100.0);
+    int index1 = 1, index2 = 1;
+    double wr = 0.0;
+    if (dnij0 > rcolla && dnij0 <= 10 * rcoll) {
+        if (dnij0 > rcoll) {
+            for (int i = 0; i < 3; i++) xd[i] = xd[i] / dnij0;
+            double vr1 = dot3(va, xd), vr2 = dot3(vb, xd);
+            wr = vr1 - vr2;
+            int ir = (int)((dnij0 - rcoll) / ((9.0 / (double)DL_NBIN) * rcoll));
+            if (ir > DL_NBIN - 1) ir = DL_NBIN - 1;
+            if (ir < 0) ir = 0;
+            findindex(D, ra, rb, index1, index2);
+            const int hb = (index1 - 1) + nset * ((index2 - 1) + nset * ir);
+            atomicAdd(&A.hist_i[hb], 1);
+            double dwx = 0.0, dwy = 0.0, dwz = 0.0;
+            if (index2 == index1) { dwx = va[0] - vb[0]; dwy = va[1] - vb[1]; dwz = va[2] - vb[2]; }
+            if (ra > rb) {
+                dwx = dwx + (va[0] - vb[0]); dwy = dwy + (va[1] - vb[1]); dwz = dwz + (va[2] - vb[2]);
+            } else if (ra < rb) {
+                dwx = dwx + (vb[0] - va[0]); dwy = dwy + (vb[1] - va[1]); dwz = dwz + (vb[2] - va[2]);
+            }
+            double *H = A.hist_d;
+            const int nb = A.nbinsz;
+            atomicAdd(&H[0 * nb + hb], wr);
+            atomicAdd(&H[1 * nb + hb], dwx);
+            atomicAdd(&H[2 * nb + hb], dwy);
+            atomicAdd(&H[3 * nb + hb], dwz);
+            double du[3], dv[3];
+            for (int i = 0; i < 3; i++) {
+                du[i] = ua[i] - (double)A.up[i][src];
+                dv[i] = va[i] - vb[i];
+            }
+            atomicAdd(&H[4 * nb + hb], dot3(du, xd));
+            double aaa = dot3(dv, xd);
+            double bbb = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+            if (bbb != 0.0) {
+                double vangle = acos(fabs(aaa / bbb));
+                atomicAdd(&H[5 * nb + hb], vangle);
+                double svv = bbb * sin(vangle);
+                atomicAdd(&H[6 * nb + hb], svv * svv / dnij0);
+            }
+        }
+        if (dnij0 <= rcollb) {
+            if (dnij0 <= rcoll) {
+                for (int i = 0; i < 3; i++) xd[i] = xd[i] / dnij0;
+                double vr1 = dot3(va, xd), vr2 = dot3(vb, xd);
+                wr = vr1 - vr2;
+                findindex(D, ra, rb, index1, index2);
+            }
+            atomicAdd(&A.counts[8 + nset * nset + (index1 - 1) + nset * (index2 - 1)], 1);
+            int slot = atomicAdd(&A.counts[4], 1);
+            if (slot < A.contact_cap) {
+                ContactRec &cr = A.contacts[slot];
+                cr.a = a; cr.b = e; cr.loopkey = loopkey; cr.pad = 0;
+                cr.rec[0] = (double)index1;
+                cr.rec[1] = (double)index2;
+                for (int i = 0; i < 3; i++) {
+                    cr.rec[2 + i] = va[i];
+                    cr.rec[5 + i] = vb[i];
+                    cr.rec[8 + i] = xd[i];
+                }
+                cr.rec[11] = wr;
+            } else {
+                A.counts[6] = 1;
+            }
+        }
+    }
+    // detection, neighbouring cells only (partlib.f90:1445-1518)
+    if (abs(ii) > 1 || abs(jj) > 1 || abs(kk) > 1) return;
+    const double dmove_a = sqrt(dma[0] * dma[0] + dma[1] * dma[1] + dma[2] * dma[2]);
+    const double dmove_b = sqrt(dmb[0] * dmb[0] + dmb[1] * dmb[1] + dmb[2] * dmb[2]);
+    const double tmove = rcoll + dmove_a + dmove_b;
+    if (dnij0 > tmove) return;
+    for (int i = 0; i < 3; i++) xd[i] = xan[i] - xbn[i];
+    const double dnij1 = sqrt(xd[0] * xd[0] + xd[1] * xd[1] + xd[2] * xd[2]);
+    if (dnij0 < rcoll && dnij1 > rcoll) return;
+    int hit = 0;
+    if (dnij0 > rcoll && dnij1 <= rcoll) {
+        hit = 1;
+    } else {
+        double vbn[3];
+        for (int i = 0; i < 3; i++) vbn[i] = (double)A.vn[i][src];
+        for (int icheck = 1; icheck <= 19; icheck++) {
+            const double tfac = 0.05 * (double)icheck;
+            const double tfac1 = D.dt * tfac;
+            const double tfac2 = tfac * tfac;
+            const double tfac3 = tfac2 * tfac;
+            double dd[3];
+            for (int i = 0; i < 3; i++) {
+                double xta = xa[i] + va[i] * tfac1 + (3.0 * dma[i] - (2.0 * va[i] + van[i]) * D.dt) * tfac2 +
+                             ((van[i] + va[i]) * D.dt - 2.0 * dma[i]) * tfac3;
+                double xtb = xb[i] + vb[i] * tfac1 + (3.0 * dmb[i] - (2.0 * vb[i] + vbn[i]) * D.dt) * tfac2 +
+                             ((vbn[i] + vb[i]) * D.dt - 2.0 * dmb[i]) * tfac3;
+                dd[i] = xta - xtb;
+            }
+            const double dnij = sqrt(dd[0] * dd[0] + dd[1] * dd[1] + dd[2] * dd[2]);
+            if (dnij0 > rcoll && dnij < rcoll) { hit = 2; break; }
+            if (dnij1 <= rcoll && dnij > rcoll) { hit = 3; break; }
+        }
+    }
+    if (!hit) return;
+    atomicAdd(&A.counts[hit - 1], 1);
+    findindex(D, ra, rb, index1, index2);
+    atomicAdd(&A.counts[8 + (index1 - 1) + nset * (index2 - 1)], 1);
+    int ps = atomicAdd(&A.counts[3], 1);
+    if (ps < A.pair_cap) {
+        A.pairs[ps].a = a; A.pairs[ps].b = e; A.pairs[ps].type = hit; A.pairs[ps].loopkey = loopkey;
+    } else {
+        A.counts[6] = 1;
+    }
+    // removal lists (partlib.f90:1527-1553): owned partner, or a ghost of slots 5..8
+    if (jid == 0 || jid >= 5) {
+        int rs2 = atomicAdd(&A.counts[5], 1);
+        if (rs2 < A.remove_cap) A.remove[rs2] = A.ref[src] + 1;
+        else A.counts[6] = 1;
+    }
+    // the owner, once (the reference adds ih1 after its loop when it collided at all)
+    if (atomicExch(&A.cflag[a], 1) == 0) {
         int rs2 = atomicAdd(&A.counts[5], 1);
         if (rs2 < A.remove_cap) A.remove[rs2] = refa + 1;
         else A.counts[6] = 1;
     }
-    return ncand;
 }
 
-// One thread per sorted entry that is an owned droplet: consecutive threads own
-// neighbouring droplets of one cell row and stream overlapping ranges of the packed
-// entries.  The candidate count takes one atomic per warp.
+// Search pass: one thread per sorted entry (owners in cell order share their neighbour rows
+// in L1); the list goes through a block buffer, one global atomic per block
 template <typename T>
-__global__ void __launch_bounds__(128) k_collision(CollArgs<T> A)
+__global__ void __launch_bounds__(128) k_coll_search(CollArgs<T> A)
 {
+    __shared__ int4 sbuf[COLL_SBUF];
+    __shared__ int sn, sbase;
+    if (threadIdx.x == 0) sn = 0;
+    __syncthreads();
     const int sa = blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned ncand = sa < A.ne ? collision_owner(A, sa) : 0u;
+    const unsigned ncand = sa < A.ne ? coll_search(A, sa, sbuf, &sn) : 0u;
     const unsigned tot = __reduce_add_sync(0xffffffffu, ncand);
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(A.cand, (unsigned long long)tot);
+    __syncthreads();
+    const int nloc = min(sn, COLL_SBUF);
+    if (threadIdx.x == 0) sbase = nloc ? atomicAdd(A.cn, nloc) : 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < nloc; k += blockDim.x)
+        if (sbase + k < A.ccap) A.clist[sbase + k] = sbuf[k];
+}
+
+// Evaluation pass over the listed pairs; nothing is evaluated when the list overflowed (the
+// host enlarges it and searches again)
+template <typename T>
+__global__ void __launch_bounds__(256) k_coll_eval(CollArgs<T> A)
+{
+    const int n = *(volatile int *)A.cn;
+    if (n > A.ccap) return;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        coll_pair(A, A.clist[k]);
 }
 
 __global__ void k_accumulate(int nbinsz, const int *hi, const double *hd, int *acc_i, double *acc_d)
@@ -1093,24 +1176,77 @@ static int collision_t(dl_ctx *c, dl_coll_report *rep)
     A.remove = c->remove_dev;
     A.remove_cap = c->remove_cap;
     const int ncount = 8 + 2 * nset * nset;
-    DL_CUDA(c, cudaMemsetAsync(c->hist_i, 0, sizeof(int) * nbz, c->stream));
-    DL_CUDA(c, cudaMemsetAsync(c->hist_d, 0, sizeof(double) * 7 * nbz, c->stream));
-    DL_CUDA(c, cudaMemsetAsync(c->counts, 0, sizeof(int) * ncount, c->stream));
-    DL_CUDA(c, cudaMemsetAsync(c->cand, 0, sizeof(unsigned long long), c->stream));
-    if (c->nps > 0) {
-        k_collision<T><<<dl_blocks(A.ne, t), t, 0, c->stream>>>(A);
-        DL_CHECK_LAUNCH(c);
+    // the candidate list (enlarged, and both passes run again, when a step has more
+    // candidates than it holds) and the owners' removal flags
+    auto dev_alloc = [&](void **ptr, size_t bytes) -> int {
+        if (cudaMalloc(ptr, bytes) != cudaSuccess) {
+            *ptr = nullptr;
+            return dl_fail(c, DL_E_ALLOC, "COLLISION_DET: cudaMalloc of the candidate list failed");
+        }
+        return 0;
+    };
+    if (!c->coll_n) {
+        int r = dev_alloc((void **)&c->coll_n, 2 * sizeof(int));
+        if (r) return r;
+    }
+    const int want = std::max(1 << 16, 2 * c->nps);
+    if (c->coll_cap < want) {
+        if (c->coll_list) cudaFree(c->coll_list);
+        c->coll_cap = 0;
+        int r = dev_alloc((void **)&c->coll_list, sizeof(int4) * (size_t)want);
+        if (r) return r;
+        c->coll_cap = want;
+    }
+    if (c->coll_flag_cap < c->nps) {
+        if (c->coll_flag) cudaFree(c->coll_flag);
+        c->coll_flag_cap = 0;
+        const int m = std::max(c->nps, c->p.msize);
+        int r = dev_alloc((void **)&c->coll_flag, sizeof(int) * (size_t)m);
+        if (r) return r;
+        c->coll_flag_cap = m;
+    }
+    char *hs = nullptr;
+    for (int attempt = 0;; attempt++) {
+        A.clist = c->coll_list;
+        A.cn = c->coll_n;
+        A.ccap = c->coll_cap;
+        A.cflag = c->coll_flag;
+        DL_CUDA(c, cudaMemsetAsync(c->hist_i, 0, sizeof(int) * nbz, c->stream));
+        DL_CUDA(c, cudaMemsetAsync(c->hist_d, 0, sizeof(double) * 7 * nbz, c->stream));
+        DL_CUDA(c, cudaMemsetAsync(c->counts, 0, sizeof(int) * ncount, c->stream));
+        DL_CUDA(c, cudaMemsetAsync(c->cand, 0, sizeof(unsigned long long), c->stream));
+        DL_CUDA(c, cudaMemsetAsync(c->coll_n, 0, 2 * sizeof(int), c->stream));
+        if (c->nps > 0) {
+            DL_CUDA(c, cudaMemsetAsync(c->coll_flag, 0, sizeof(int) * (size_t)c->nps, c->stream));
+            k_coll_search<T><<<dl_blocks(A.ne, t), t, 0, c->stream>>>(A);
+            DL_CHECK_LAUNCH(c);
+            k_coll_eval<T><<<4 * c->num_sms, 256, 0, c->stream>>>(A);
+            DL_CHECK_LAUNCH(c);
+        }
+        // counts, the list length and the candidate total in one batch of copies into
+        // pinned staging (with everything the host bookkeeping needs)
+        hs = static_cast<char *>(dl_host_stage(c, sizeof(int) * ncount + 16));
+        if (!hs) return dl_fail(c, DL_E_ALLOC, "cudaHostAlloc of the staging buffer failed");
+        DL_CUDA(c, cudaMemcpyAsync(hs, c->cand, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaMemcpyAsync(hs + 8, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaMemcpyAsync(hs + 12, c->coll_n, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaMemcpyAsync(hs + 16, c->counts, sizeof(int) * ncount, cudaMemcpyDeviceToHost, c->stream));
+        DL_CUDA(c, cudaStreamSynchronize(c->stream));
+        int nlist = 0;
+        memcpy(&nlist, hs + 12, sizeof(int));
+        if (nlist <= c->coll_cap) break;
+        // the list overflowed and nothing was evaluated: enlarge it and search again
+        if (attempt >= 2) return dl_fail(c, DL_E_CAPACITY, "COLLISION_DET: candidate list overflow");
+        cudaFree(c->coll_list);
+        c->coll_list = nullptr;
+        c->coll_cap = 0;
+        const int cap = (int)std::min<int64_t>((int64_t)nlist + nlist / 4 + 1024, 0x7fffffff / 16);
+        int r = dev_alloc((void **)&c->coll_list, sizeof(int4) * (size_t)cap);
+        if (r) return r;
+        c->coll_cap = cap;
     }
     k_accumulate<<<dl_blocks(7 * nbz, 256), 256, 0, c->stream>>>(nbz, c->hist_i, c->hist_d, c->acc_i, c->acc_d);
     DL_CHECK_LAUNCH(c);
-    // counts and the candidate total, then everything the host bookkeeping needs in one
-    // batch of copies into pinned staging
-    char *hs = static_cast<char *>(dl_host_stage(c, sizeof(int) * ncount + 16));
-    if (!hs) return dl_fail(c, DL_E_ALLOC, "cudaHostAlloc of the staging buffer failed");
-    DL_CUDA(c, cudaMemcpyAsync(hs, c->cand, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
-    DL_CUDA(c, cudaMemcpyAsync(hs + 8, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    DL_CUDA(c, cudaMemcpyAsync(hs + 16, c->counts, sizeof(int) * ncount, cudaMemcpyDeviceToHost, c->stream));
-    DL_CUDA(c, cudaStreamSynchronize(c->stream));
     unsigned long long cand;
     memcpy(&cand, hs, sizeof(cand));
     int derr;

@@ -169,6 +169,10 @@ struct dl_ctx {
     double *acc_d, *out_d;
     int *counts;                 // icc[3], colltype[nset^2], nir[nset^2], npairs, ncontact, overflow, ...
     unsigned long long *cand;
+    int4 *coll_list;             // candidate pairs of the collision search (sorted entries, loop key, x shift)
+    int *coll_n;                 // [0] candidates written, [1] unused
+    int *coll_flag;              // [msize] owner already on the removal list
+    int coll_cap, coll_flag_cap;
     PairRec *pairs;
     int pair_cap;
     ContactRec *contacts;
