@@ -493,6 +493,9 @@ static int allocate_state(dl_ctx *c)
     // test hook: DL_ARN_SPIN_LIMIT (read here, once per context) lowers the polling limit of
     // the cooperative FP32 solve's grid barrier so that a test can make the barrier give up
     if (const char *lim = getenv("DL_ARN_SPIN_LIMIT")) c->arn_spin_limit = atoll(lim);
+    // test hook: DL_COLL_LIST_CAP sets the first capacity of COLLISION_DET's candidate list,
+    // so that a test can make it overflow (it is then enlarged and the search run again)
+    if (const char *cap = getenv("DL_COLL_LIST_CAP")) c->coll_cap_first = atoi(cap);
     return 0;
 }
 

@@ -1189,8 +1189,8 @@ static int collision_t(dl_ctx *c, dl_coll_report *rep)
         int r = dev_alloc((void **)&c->coll_n, 2 * sizeof(int));
         if (r) return r;
     }
-    const int want = std::max(1 << 16, 2 * c->nps);
-    if (c->coll_cap < want) {
+    const int want = c->coll_cap_first > 0 ? c->coll_cap_first : std::max(1 << 16, 2 * c->nps);
+    if (c->coll_cap < want && !(c->coll_cap_first > 0 && c->coll_list)) {
         if (c->coll_list) cudaFree(c->coll_list);
         c->coll_cap = 0;
         int r = dev_alloc((void **)&c->coll_list, sizeof(int4) * (size_t)want);

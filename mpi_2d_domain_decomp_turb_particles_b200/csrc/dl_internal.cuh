@@ -173,6 +173,7 @@ struct dl_ctx {
     int *coll_n;                 // [0] candidates written, [1] unused
     int *coll_flag;              // [msize] owner already on the removal list
     int coll_cap, coll_flag_cap;
+    int coll_cap_first;          // first capacity of the list (0: twice the droplets, at least 65536)
     PairRec *pairs;
     int pair_cap;
     ContactRec *contacts;

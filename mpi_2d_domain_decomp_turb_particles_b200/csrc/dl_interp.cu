@@ -5,19 +5,17 @@
 // PART_HISTORY_FVP (553-595), PART_HISTORY_FDP (599-625), PART_ADVANCE (629-726),
 // UPDATE_PART_POSITION (730-757), the wrap of PERIODIC (1142-1151) and MEAN_VEL (1889-1980).
 //
-// Design (B200):
-// * Mixed precision (k_interp_col): droplets are kept sorted by (column of 16 x 16 cells,
-//   z plane); each CTA sweeps work items (a column over a range of planes) in z, the field
-//   streaming through a ring of shared-memory slabs (four planes, three components, one
-//   TMA box each), with warp-specialised producer, prep, stencil and release warps.  The
-//   stencil warps evaluate the 216-point stencil of every (droplet, component) task out of
-//   shared memory in rounds of 32 tasks that start in 32 distinct banks, so every load is
-//   conflict-free; the FP32 tensor-product sum is taken separably with FMA.
-// * FP64 (k_interp): droplets are kept sorted by brick (a BX x BY x BZ block of cells).  One
-//   CTA handles one brick at a time: it stages the brick's field region plus the 6-point
-//   stencil halo in shared memory with TMA and evaluates the tasks in half-warp groups that
-//   start in distinct banks.  The sum is taken in the reference's order (x outer, y, z
-//   inner, vp = vp + v*bx*by*bz, no FMA contraction), bit-identical to the CPU restatement.
+// Design (B200): one kernel for both precisions, k_interp_col<T>.  Droplets are kept sorted
+// by (column of CX x CY cells, z plane) -- 16 x 16 cells for FP32, 16 x 8 for FP64 -- and
+// each CTA sweeps work items (a column over a range of planes) in z, the field streaming
+// through a ring of shared-memory slabs (four planes, three components, one TMA box each),
+// with warp-specialised producer, prep, stencil and release warps.  The stencil warps
+// evaluate the 216-point stencil of every (droplet, component) task out of shared memory in
+// rounds whose loads start in distinct banks.
+// * FP32: the tensor-product sum is taken separably with FMA.
+// * FP64: the sum is taken in the reference's order (x outer, y, z inner, vp = vp +
+//   v*bx*by*bz, no FMA contraction), bit-identical to the CPU restatement; the weights are
+//   computed once per droplet with the reference's divisions.
 // A droplet whose stencil is not inside the staged field (it drifted beyond the margins
 // since the last re-sort) is evaluated from the padded field in global memory with the same
 // arithmetic.
@@ -152,35 +150,6 @@ struct InterpArgs {
     signed char *leave_nid;         // PERIODIC departure flags by reference index
     int *lv_list, *lv_n;            // departing reference indices (appended) and their count
     int *err;                       // device error flags
-};
-
-// Shared-memory bank geometry of one stencil load: conflict-free groups are 32 lanes of
-// 4-byte words (FP32) or 16 lanes of 8-byte words (FP64, one half-warp per wavefront).
-template <typename T>
-struct Elems;
-template <>
-struct Elems<double> {
-    static constexpr int R = 16;
-    static constexpr int LANES = 16;
-};
-
-// Field tile of one component of one brick, as one TMA box.  Component c's box starts
-// XS*c cells lower in x and YS*c cells lower in y than component 0's, which moves the
-// three components' copies of a stencil into different banks (corner offset shift CSHIFT)
-// while keeping the TMA x coordinate 16-byte aligned.  The box reaches M cells beyond the
-// brick in y and z (x has 2 below and 1 above by its alignment), so droplets that drifted
-// that far since the last spatial re-sort still read their stencil from the tile.
-template <typename T, int BX, int BY, int BZ, int XS, int YS, int M>
-struct Geo {
-    static constexpr int EX = BX + 8 + 2 * XS, EY = BY + 5 + 2 * YS + 2 * M, EZ = BZ + 5 + 2 * M;
-    static constexpr int PLANE = EX * EY;
-    static constexpr int VOL = PLANE * EZ;
-    static constexpr int BOX_BYTES = VOL * (int)sizeof(T);
-    static constexpr int STAGE_BYTES = (BOX_BYTES + 127) / 128 * 128;
-    static constexpr int STAGE_ELEMS = STAGE_BYTES / (int)sizeof(T);
-    static constexpr int CSHIFT = YS * EX + XS;
-    static_assert((EX * sizeof(T)) % 16 == 0, "TMA box rows must be whole 16-byte units");
-    static_assert((XS * sizeof(T)) % 16 == 0, "component x shift must keep 16-byte alignment");
 };
 
 // PERIODIC's neighbour code of a droplet that left the single pencil (partlib.f90:874-1060)
@@ -368,257 +337,7 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, u
 
 
 // ---------------------------------------------------------------------------------------
-// The brick kernel: persistent, warp-specialised.  The last warp is the producer: it
-// streams the field tile of every component of every (non-empty) brick of this CTA into a
-// ring of S shared-memory stages with TMA.  NG consumer groups of GW warps take the CTA's
-// bricks in turn (brick k goes to group k % NG), so one group's serial phases overlap
-// another group's stencil phase and the producer's prefetch.  Per brick a group computes
-// weights and corners, groups the (droplet, component) stencil tasks by starting bank,
-// evaluates them from shared memory, releases the stages and runs the advance epilogue.
-// ---------------------------------------------------------------------------------------
-template <typename T, int MAXD>
-struct GroupAux {
-    static constexpr int R = Elems<T>::R;
-    static constexpr int NSW = (sizeof(T) == 8) ? 18 : 3;   // FP64 weights, FP32 fractions
-    static constexpr int CAP = 64;   // tasks per bank bucket; overflow goes to the slow list
-    static constexpr size_t BYTES =
-        ((sizeof(T) * (MAXD * NSW + MAXD * 3) + sizeof(int) * (MAXD + MAXD * 3 + R + 4) +
-          sizeof(unsigned short) * (R * CAP + MAXD * 3)) + 127) / 128 * 128;
-};
-
-template <typename T, int BX, int BY, int BZ, int XS, int YS, int M, int S, int MAXD, int NG, int GW>
-__global__ void __launch_bounds__((NG * GW + 1) * 32, 1) k_interp(const __grid_constant__ CUtensorMap tmap,
-                                                                    InterpArgs<T> A)
-{
-    using G = Geo<T, BX, BY, BZ, XS, YS, M>;
-    using X = GroupAux<T, MAXD>;
-    constexpr int R = Elems<T>::R;
-    constexpr int NSW = X::NSW;
-    constexpr int NT = GW * 32;   // threads per consumer group
-    extern __shared__ __align__(1024) unsigned char smem_raw[];
-    T *stage = reinterpret_cast<T *>(smem_raw);
-    unsigned long long *full = reinterpret_cast<unsigned long long *>(smem_raw + S * G::STAGE_BYTES);
-    unsigned long long *empty = full + S;
-    int *sabort = reinterpret_cast<int *>(empty + S);
-    unsigned char *aux0 = smem_raw + S * G::STAGE_BYTES + 128;
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n = A.n;
-    const int ncomp = A.ncomp, clo = A.comp_lo;
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < S; s++) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
-        *sabort = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    }
-    __syncthreads();
-
-    if (warp == NG * GW) {
-        // ================= producer =================
-        if (lane == 0) {
-            int it = 0;
-            bool ok = true;
-            for (int b = blockIdx.x; b < A.nbricks && ok; b += gridDim.x) {
-                if (A.brick_start[b] == A.brick_start[b + 1]) continue;
-                const int bxi = b % A.nbx, byi = (b / A.nbx) % A.nby, bzi = b / (A.nbx * A.nby);
-                for (int cc = 0; cc < ncomp; cc++, it++) {
-                    const int s = it % S;
-                    if (it >= S && !mbar_wait(&empty[s], ((it / S) - 1) & 1)) {
-                        atomicOr(A.err, DL_DERR_TMA_TIMEOUT);
-                        *(volatile int *)sabort = 1;
-                        ok = false;
-                        break;
-                    }
-                    const int c = clo + cc;
-                    mbar_arrive_expect_tx(&full[s], (unsigned)G::BOX_BYTES);
-                    // padded coordinates of the box origin (grid origin + DL_PAD_LO)
-                    tma_load_4d(stage + s * G::STAGE_ELEMS, &tmap, &full[s], bxi * BX - XS * c,
-                                byi * BY + 2 - YS * c - M, bzi * BZ + 2 - M, c);
-                }
-            }
-            // wait (bounded) for the copies still in flight before leaving
-            for (int k = (it > S ? it - S : 0); k < it; k++) mbar_wait(&full[k % S], (k / S) & 1);
-        }
-        return;
-    }
-
-    // ================= consumer group gi =================
-    const int gi = warp / GW, gw = warp % GW, tid = threadIdx.x - gi * NT;
-    const int bar_id = 1 + gi;
-    unsigned char *aux = aux0 + gi * X::BYTES;
-    T *sw = reinterpret_cast<T *>(aux);                             // [MAXD][NSW]
-    T *sv = sw + MAXD * NSW;                                        // [MAXD][3] results
-    int *scorner = reinterpret_cast<int *>(sv + MAXD * 3);          // [MAXD] corner offset (comp 0) or -1
-    int *snode = scorner + MAXD;                                    // [MAXD][3]
-    int *scnt = snode + MAXD * 3;                                   // [R] tasks per bank bucket
-    int *smisc = scnt + R;                                          // [0] slow-list length
-    constexpr int CAP = X::CAP;
-    unsigned short *stask = reinterpret_cast<unsigned short *>(smisc + 4);   // [R][CAP] bucketed tasks
-    unsigned short *sfbt = stask + R * CAP;                                   // [MAXD*3] slow list
-    auto gsync = [&]() { asm volatile("bar.sync %0, %1;\n" ::"r"(bar_id), "r"(NT) : "memory"); };
-
-    if (tid < R) scnt[tid] = 0;
-    if (tid == 0) smisc[0] = 0;
-    gsync();
-    int k = 0;   // index of the brick among this CTA's non-empty bricks
-    for (int b = blockIdx.x; b < A.nbricks; b += gridDim.x) {
-        const int d0 = A.brick_start[b], d1 = A.brick_start[b + 1];
-        if (d0 == d1) continue;
-        const int mine = (k % NG) == gi;
-        const int it = k * ncomp;
-        k++;
-        if (!mine) continue;
-        const int bxi = b % A.nbx, byi = (b / A.nbx) % A.nby, bzi = b / (A.nbx * A.nby);
-        bool waited = false;
-        for (int c0 = d0; c0 < d1; c0 += MAXD) {
-            const int nd = min(MAXD, d1 - c0);
-            // ---- Phase A: nodes, weights (FP64) or fractions (FP32), corners ----
-            for (int i = tid; i < nd; i += NT) {
-                const int d = c0 + i;
-                double pos[3] = {A.px[d], A.py[d], A.pz[d]};
-                int node[3];
-#pragma unroll
-                for (int q3 = 0; q3 < 3; q3++) {
-                    double z;
-                    if constexpr (sizeof(T) == 8) {
-                        node[q3] = node_frac(pos[q3], A.dx, &z);   // the reference's division
-                    } else {
-                        // FP32 weights: a multiply by 1/dx (no FP64 division in the per-brick
-                        // critical path); a node that differs by one at a cell face gives the
-                        // same interpolant (z = 1 on node n is z = 0 on node n + 1)
-                        const double u = pos[q3] * A.inv_dx;
-                        node[q3] = (int)floor(u);
-                        z = u - (double)node[q3];
-                    }
-                    if constexpr (sizeof(T) == 8) {
-                        double w[6];
-                        lagrange6(z, w);
-#pragma unroll
-                        for (int q = 0; q < 6; q++) sw[i * NSW + q3 * 6 + q] = w[q];
-                    } else {
-                        sw[i * NSW + q3] = (T)z;
-                    }
-                    snode[i * 3 + q3] = node[q3];
-                }
-                // stencil corner in component 0's tile (origin bxi*BX-4, byi*BY-2, bzi*BZ-2); in
-                // component c's tile the same stencil starts CSHIFT*c words further on
-                const int lx = node[0] - bxi * BX + 2, ly = node[1] - byi * BY, lz = node[2] - bzi * BZ;
-                const bool in = lx >= 0 && lx + 2 * XS + 5 < G::EX && ly >= -M && ly < BY + M && lz >= -M &&
-                                lz < BZ + M;
-                const int cr = in ? ((lz + M) * G::EY + (ly + M)) * G::EX + lx : -1;
-                scorner[i] = cr;
-                // bucket this droplet's tasks by starting bank (stages start on 128-byte
-                // boundaries, so the bank is set by the offset alone)
-                // the slot a task gets in its bucket is the count before it: no scan needed
-                for (int cc = 0; cc < ncomp; cc++) {
-                    const int t = i * ncomp + cc;
-                    bool slow = cr < 0;
-                    if (!slow) {
-                        const int r = (cr + G::CSHIFT * (clo + cc)) % R;
-                        const int slot = atomicAdd(&scnt[r], 1);
-                        if (slot < CAP) stask[r * CAP + slot] = (unsigned short)t;
-                        else slow = true;
-                    }
-                    if (slow) sfbt[atomicAdd(&smisc[0], 1)] = (unsigned short)t;
-                }
-            }
-            // ---- wait for this brick's tiles (once per brick) ----
-            if (!waited) {
-                for (int cc = 0; cc < ncomp; cc++) {
-                    const int q = it + cc;
-                    if (!mbar_wait(&full[q % S], (q / S) & 1)) {
-                        *(volatile int *)sabort = 1;
-                        atomicOr(A.err, DL_DERR_TMA_TIMEOUT);
-                    }
-                }
-                waited = true;
-            }
-            gsync();
-            if (*(volatile int *)sabort) return;   // uniform within the group after the barrier
-            // ---- conflict-free groups: lane r of group g takes the g-th task of bucket r ----
-            {
-                constexpr int GPW = 32 / Elems<T>::LANES;
-                const int sub = lane / Elems<T>::LANES, r = lane % Elems<T>::LANES;
-                const int mycnt = min(scnt[r], CAP);
-                int Gn = mycnt;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) Gn = max(Gn, __shfl_xor_sync(0xffffffffu, Gn, o));
-                for (int g = gw * GPW + sub; g < Gn; g += GW * GPW) {
-                    if (g < mycnt) {
-                        const int t = stask[r * CAP + g];
-                        const int i = t / ncomp, cc = t - i * ncomp;
-                        const T *base = stage + ((it + cc) % S) * G::STAGE_ELEMS + scorner[i] + G::CSHIFT * (clo + cc);
-                        SmemLoader<T> ld{base, G::EX, G::PLANE};
-                        T bx[6], by[6], bz[6];
-                        if constexpr (sizeof(T) == 8) {
-                            const T *w = sw + i * NSW;
-#pragma unroll
-                            for (int q = 0; q < 6; q++) { bx[q] = w[q]; by[q] = w[6 + q]; bz[q] = w[12 + q]; }
-                        } else {
-                            lagrange6(sw[i * NSW + 0], bx);
-                            lagrange6(sw[i * NSW + 1], by);
-                            lagrange6(sw[i * NSW + 2], bz);
-                        }
-                        sv[i * 3 + clo + cc] = stencil(ld, bx, by, bz);
-                    }
-                }
-            }
-            // ---- slow list: bucket overflow (shared memory, bank conflicts possible) and
-            //      droplets outside the staged tile (padded field in global memory) ----
-            for (int q = tid; q < smisc[0]; q += NT) {
-                const int t = sfbt[q];
-                const int i = t / ncomp, cc = t - i * ncomp, comp = clo + cc;
-                if (scorner[i] >= 0) {
-                    const T *base = stage + ((it + cc) % S) * G::STAGE_ELEMS + scorner[i] + G::CSHIFT * comp;
-                    SmemLoader<T> ld{base, G::EX, G::PLANE};
-                    T bx[6], by[6], bz[6];
-                    if constexpr (sizeof(T) == 8) {
-                        const T *w = sw + i * NSW;
-#pragma unroll
-                        for (int q6 = 0; q6 < 6; q6++) { bx[q6] = w[q6]; by[q6] = w[6 + q6]; bz[q6] = w[12 + q6]; }
-                    } else {
-                        lagrange6(sw[i * NSW + 0], bx);
-                        lagrange6(sw[i * NSW + 1], by);
-                        lagrange6(sw[i * NSW + 2], bz);
-                    }
-                    sv[i * 3 + comp] = stencil(ld, bx, by, bz);
-                    continue;
-                }
-                T bx[6], by[6], bz[6];
-                if constexpr (sizeof(T) == 8) {
-                    const T *w = sw + i * NSW;
-#pragma unroll
-                    for (int q6 = 0; q6 < 6; q6++) { bx[q6] = w[q6]; by[q6] = w[6 + q6]; bz[q6] = w[12 + q6]; }
-                } else {
-                    lagrange6(sw[i * NSW + 0], bx);
-                    lagrange6(sw[i * NSW + 1], by);
-                    lagrange6(sw[i * NSW + 2], bz);
-                }
-                GlobalLoaderPad<T> ld;
-                const int x0 = wrapi(snode[i * 3 + 0], n) - 2 + DL_PAD_LO;
-                const int y0 = wrapi(snode[i * 3 + 1], n) - 2 + DL_PAD_LO;
-                const int z0 = wrapi(snode[i * 3 + 2], n) - 2 + DL_PAD_LO;
-                ld.f = A.fpad + comp * A.fpc + x0 + A.fpy * y0 + A.fpz * z0;
-                ld.py = A.fpy;
-                ld.pz = A.fpz;
-                sv[i * 3 + comp] = stencil(ld, bx, by, bz);
-            }
-            gsync();
-            if (c0 + MAXD >= d1 && tid == 0) {
-                // last chunk of this brick: hand the stages back to the producer
-                for (int cc = 0; cc < ncomp; cc++) mbar_arrive(&empty[(it + cc) % S]);
-            }
-            // ---- write the interpolated velocity (coalesced); reset the bucket counters ----
-            for (int i = tid; i < nd; i += NT)
-                for (int comp = clo; comp < clo + ncomp; comp++) A.vp[comp][c0 + i] = sv[i * 3 + comp];
-            if (tid < R) scnt[tid] = 0;
-            if (tid == 0) smisc[0] = 0;
-            gsync();
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------------------
-// Column sweep (mixed precision).  The device order is sorted by (column, z plane), a
+// Column sweep (both precisions).  The device order is sorted by (column, z plane), a
 // column being CX x CY cells in x-y.  The work items are (column, segment of zseg planes);
 // each CTA sweeps its items in z:
 //  * the producer warp streams the field through a ring of NSL slabs, a slab being four
@@ -626,12 +345,11 @@ __global__ void __launch_bounds__((NG * GW + 1) * 32, 1) k_interp(const __grid_c
 //    in one TMA box (a TMA copy costs about the same issue time whatever its size, so the
 //    boxes are made large);
 //  * prep warps (batches go round them) take the droplets of PZ consecutive planes at a
-//    time (a batch, at most MAXD droplets), compute their nodes, fractions and stencil
-//    corners, and sort the (droplet, component) tasks into 32 buckets by the shared-memory
-//    bank their stencil starts in;
+//    time (a batch, at most MAXD droplets), compute their nodes, fractions (FP64: weights)
+//    and stencil corners, and sort the (droplet, component) tasks into buckets by the
+//    shared-memory bank their stencil starts in;
 //  * NSW stencil warps wait for the slabs of a batch's window, then take rounds of its
-//    buckets (lane r evaluates the round's task of bucket r, so each of the round's 216
-//    shared-memory loads is conflict-free, and stores the result) until the batch has none
+//    tasks (see ColBatch for the round order of each precision) until the batch has none
 //    left, and move on to the next batch without a block barrier;
 //  * a release warp hands the slabs no finished batch needs any more back to the producer
 //    and the batch slot back to the prep warps.
@@ -642,11 +360,11 @@ __global__ void __launch_bounds__((NG * GW + 1) * 32, 1) k_interp(const __grid_c
 // global memory with the same arithmetic.
 //
 // Slab layout in shared memory: [plane 0..3][component][y][x] (the tensor map orders the
-// field's dimensions x, y, component, z).  With BOX = EX * EY floats per component plane
-// and PS = ncomp * BOX per plane, BOX = 8 (mod 32) and PS = 24 (mod 32) for three
-// components, 8 for one, and 4 * PS = 0 (mod 32): plane u of the sweep starts at bank
-// PS * u (mod 32) whatever slab slot holds it, so the bank of a stencil's start plus
-// PS * k is the bank of its plane k, the same shift for every lane of a round.
+// field's dimensions x, y, component, z).  With BOX = EX * EY elements per component plane,
+// PS = ncomp * BOX per plane and NBK banks of one element (32 for FP32, 16 double-banks for
+// FP64), 4 * PS = 0 (mod NBK) and every slab slot starts at bank 0: plane u of the sweep
+// starts at bank PS * u (mod NBK) whatever slab slot holds it, so the bank of a stencil's
+// start plus PS * k is the bank of its plane k, the same shift for every lane of a round.
 // ---------------------------------------------------------------------------------------
 // Per-precision geometry of the column sweep.  FP32: columns of 16 x 16 cells, 32 bank
 // buckets of one word; FP64: columns of 16 x 8 cells (a slab of four planes of three
@@ -1206,18 +924,6 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + NPREP) * 32, 1)
     }
 }
 
-template <typename T, int BX, int BY, int BZ, int XS, int YS, int M, int S, int MAXD, int NG>
-constexpr size_t interp_smem()
-{
-    using G = Geo<T, BX, BY, BZ, XS, YS, M>;
-    return (size_t)S * G::STAGE_BYTES + 128 + NG * GroupAux<T, MAXD>::BYTES;
-}
-
-// ---------------------------------------------------------------------------------------
-// Brick sort of the device order
-// ---------------------------------------------------------------------------------------
-// Sort key of a droplet: its brick, bricks numbered x fastest then y then z; with
-// colmajor (bz = 1: columns of bx x by cells) the key is (column, z plane), planes fastest.
 __global__ void k_brick_keys(int nps, const double *px, const double *py, const double *pz, double dx, int n,
                              int bx, int by, int bz, int nbx, int nby, int nbz, int colmajor, int *keys, int *cnt,
                              const double *rad, int dead_key)
@@ -1600,32 +1306,6 @@ int launch_brick_sort(dl_ctx *c)
     return 0;
 }
 
-// TMA descriptor of the halo-padded field: 4D (x, y, z, component), box = box_c component tiles
-static int make_tmap(dl_ctx *c, CUtensorMap *map, int box_x, int box_y, int box_z, int box_c = 1)
-{
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    if (!encode) {
-        void *fn = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        DL_CUDA(c, cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
-        if (!fn || q != cudaDriverEntryPointSuccess)
-            return dl_fail(c, DL_E_CUDA, "cuTensorMapEncodeTiled not available");
-        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
-    }
-    const cuuint64_t e = (cuuint64_t)c->dc.n + DL_PAD_LO + DL_PAD_HI;
-    const cuuint64_t es = c->esz;
-    cuuint64_t dims[4] = {(cuuint64_t)c->fp_pitch, e, e, 3};
-    cuuint64_t strides[3] = {(cuuint64_t)c->fp_pitch * es, (cuuint64_t)c->fp_plane * es, (cuuint64_t)c->fp_comp * es};
-    cuuint32_t box[4] = {(cuuint32_t)box_x, (cuuint32_t)box_y, (cuuint32_t)box_z, (cuuint32_t)box_c};
-    cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = encode(map, c->mixed ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
-                        c->fpad, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return dl_fail(c, DL_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
-    return 0;
-}
-
 // TMA descriptor of the halo-padded field (FP32 or FP64) with the dimensions ordered x, y,
 // component, z (strides need not grow with the dimension), so that a box of several planes
 // lands in shared memory as [plane][component][y][x]
@@ -1651,86 +1331,6 @@ static int make_tmap_zc(dl_ctx *c, CUtensorMap *map, int box_x, int box_y, int b
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return dl_fail(c, DL_E_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
-    return 0;
-}
-
-template <typename T, int BX, int BY, int BZ, int XS, int YS, int M, int S, int MAXD, int NG, int GW>
-static int launch_interp_t(dl_ctx *c, int comp_lo, int ncomp, int fused)
-{
-    using G = Geo<T, BX, BY, BZ, XS, YS, M>;
-    if (c->tmap_base != c->fpad) {
-        int r = make_tmap(c, &c->tmap, G::EX, G::EY, G::EZ);
-        if (r) return r;
-        c->tmap_base = c->fpad;
-    }
-    InterpArgs<T> A;
-    memset(&A, 0, sizeof(A));
-    A.n = c->dc.n;
-    A.nps = c->nps;
-    A.dx = c->dc.dx;
-    A.inv_dx = 1.0 / c->dc.dx;
-    A.pi2 = c->dc.pi2;
-    A.px = c->pos[c->pcur][0]; A.py = c->pos[c->pcur][1]; A.pz = c->pos[c->pcur][2];
-    A.brick_start = c->brick_start;
-    A.nbx = c->nbx; A.nby = c->nby; A.nbricks = c->nbricks;
-    A.fpad = tp<T>(c->fpad);
-    A.fpy = c->fp_pitch;
-    A.fpz = c->fp_plane;
-    A.fpc = c->fp_comp;
-    for (int k = 0; k < 3; k++) A.vp[k] = tp<T>(c->vpv[k]);
-    if (fused)   // the interpolated velocity goes straight into fdp(:,0) = F[fnew]
-        for (int k = 0; k < 3; k++) A.vp[k] = tp<T>(c->flu[(c->fcur + 3) % 4][k]);
-    A.comp_lo = comp_lo;
-    A.ncomp = ncomp;
-    A.fused = fused;
-    A.err = c->d_err;
-    if (fused) {
-        A.first = c->new_particle;
-        A.init_mode = c->p.init_velocity;
-        A.ndrag = c->dc.ndrag;
-        A.dt = (T)c->dc.dt; A.tau2 = (T)c->dc.tau2; A.sv = (T)c->dc.sv; A.rnu = (T)c->dc.rnu;
-        A.rad = c->rad;
-        c->vnew = (c->vcur + 3) % 4;
-        c->fnew = (c->fcur + 3) % 4;
-        for (int k = 0; k < 3; k++) {
-            A.v0[k] = tp<T>(c->vel[c->vcur][k]);
-            A.v1[k] = tp<T>(c->vel[(c->vcur + 1) % 4][k]);
-            A.v2[k] = tp<T>(c->vel[(c->vcur + 2) % 4][k]);
-            A.vnew[k] = tp<T>(c->vel[c->vnew][k]);
-            A.f1[k] = tp<T>(c->flu[c->fcur][k]);
-            A.f2[k] = tp<T>(c->flu[(c->fcur + 1) % 4][k]);
-            A.f3[k] = tp<T>(c->flu[(c->fcur + 2) % 4][k]);
-            A.fnew[k] = tp<T>(c->flu[c->fnew][k]);
-            A.dmv[k] = tp<T>(c->dmv[k]);
-        }
-        A.qx = c->pos[1 - c->pcur][0]; A.qy = c->pos[1 - c->pcur][1]; A.qz = c->pos[1 - c->pcur][2];
-        A.ref_of_dev = c->ref_of_dev;
-        A.leave_nid = c->leave_nid;
-        A.lv_list = c->lv_list;
-        A.lv_n = c->lv_n;
-    }
-    constexpr size_t sm = interp_smem<T, BX, BY, BZ, XS, YS, M, S, MAXD, NG>();
-    static_assert(sm <= 227 * 1024, "shared memory budget");
-    auto kern = k_interp<T, BX, BY, BZ, XS, YS, M, S, MAXD, NG, GW>;
-    DL_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    static bool carve = false;
-    if (!carve) {
-        // the kernels between two k_interp launches keep the shared-memory carveout that
-        // k_interp needs, so the SMs are not reconfigured at every kernel boundary
-        cudaFuncSetAttribute(k_advance_fused<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             (int)cudaSharedmemCarveoutMaxShared);
-        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             (int)cudaSharedmemCarveoutMaxShared);
-        carve = true;
-    }
-    const int grid = std::min(c->nbricks, c->num_sms);
-    kern<<<grid, (NG * GW + 1) * 32, sm, c->stream>>>(c->tmap, A);
-    DL_CHECK_LAUNCH(c);
-    dl_mark_interp_end(c);
-    if (fused) {
-        k_advance_fused<T><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(A);
-        DL_CHECK_LAUNCH(c);
-    }
     return 0;
 }
 

@@ -149,3 +149,34 @@ def test_overfull_cell_row_is_an_error():
     with pytest.raises(DropletError, match="one row of cells"):
         g.particle_step()
     g.close()
+
+
+def test_collision_candidate_list_overflow_is_enlarged(monkeypatch):
+    """COLLISION_DET's candidate list started at 16 entries (DL_COLL_LIST_CAP, read when the
+    context is created): the first search overflows, nothing is evaluated, the list is
+    enlarged and both passes run again.  Steps in FP64 and mixed precision equal the
+    oracle's (pairs, collist order, contacts, counts; the FP64 state bit for bit)."""
+    from test_gpu_parity import _compare_collision, gpu_state, oracle_state
+    n = 32
+    for precision in ("fp64", "mixed"):
+        p = dense_params(n=n, npart=6000, precision=precision)
+        monkeypatch.setenv("DL_COLL_LIST_CAP", "16")
+        g = Partlib(p)
+        monkeypatch.delenv("DL_COLL_LIST_CAP")
+        g.part_init()
+        o = orc.Oracle(**p.oracle_kwargs())
+        o.part_init()
+        f = smooth_field(n)
+        g.set_fields(*f)
+        cand = 0
+        for _ in range(3):
+            if precision == "fp64":
+                rep, _ = g.particle_step()
+                o.particle_step(*f)
+                _compare_collision(g, o, rep, True)
+                assert np.array_equal(gpu_state(g), oracle_state(o))
+            else:
+                rep, _ = g.particle_step()
+            cand += rep.candidate_pairs
+        assert cand > 16
+        g.close()
