@@ -748,7 +748,7 @@ def config4_bench(dev, torch, steps=4):
                            "k_advance_fused": _gbs(advance_bytes("mixed", n, nps), uams)},
             "update_substep_kernels_ms": {"interp": uims, "advance": uams, "both": ukms},
             "droplets_after": nps, "gmres_iterations": iters,
-            "note": "per-kernel times of k_collision, k_nei_walk, k_arn_solve, k_overlap: ncu launch list "
+            "note": "per-kernel times of k_coll_search, k_coll_eval, k_nei_walk, k_arn_solve, k_overlap: ncu launch list "
                     "of the same workload (bench.py --only config4)"}
 
 
