@@ -296,7 +296,8 @@ class _Hist:
 def run_ours(args):
     import torch
     import torch.distributed as dist
-    from mpi_2d_domain_decomp_turb_particles_b200.bytes_model import advance_bytes, interp_bytes, update_bytes
+    from mpi_2d_domain_decomp_turb_particles_b200.bytes_model import (advance_bytes, collision_bytes, interp_bytes,
+                                                                      update_bytes)
 
     ws, rank, local = _dist()
     if ws > 1:
@@ -414,6 +415,12 @@ def run_ours(args):
                          "algorithmic_bytes": alg64}},
             "full_step_ms": full_ms, "collision_ms": coll_ms,
             "collision_candidate_pairs_per_s": cand / (coll_ms * 1e-3) if coll_ms > 0 else None,
+            "collision_roofline": {"algorithmic_bytes": collision_bytes("mixed", N_PART),
+                                   "achieved_gbs": _gbs(collision_bytes("mixed", N_PART), coll_ms),
+                                   "frac": _gbs(collision_bytes("mixed", N_PART), coll_ms) / peak,
+                                   "candidate_pairs": cand,
+                                   "note": "COLLISION_DET phase (search + evaluation + host bookkeeping); "
+                                           "latency-bound cell search, bytes a lower bound"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": f"{kind} (burst copy)",
                          "kernel": "k_interp_col + k_advance_fused, per update step",

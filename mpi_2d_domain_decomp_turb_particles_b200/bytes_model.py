@@ -40,3 +40,11 @@ def flow_update_bytes(n: int) -> int:
 
 def flow_cross_bytes(n: int, emit_precision: str = "mixed") -> int:
     return (72 + 3 * FIELD_WORD[emit_precision]) * n ** 3
+
+
+def collision_bytes(precision: str, npart: int) -> int:
+    """COLLISION_DET reads every owned droplet's packed cell-list entry once (x, y, z,
+    radius as FP64 and four ints: 48 B) and its state once (displacement, old and new
+    velocity, fluid velocity: 12 words).  A lower bound: the ghost entries (a few per cent
+    of the droplets) and the cell start table are not counted."""
+    return (48 + 12 * FIELD_WORD[precision]) * npart
