@@ -440,6 +440,7 @@ static int allocate_state(dl_ctx *c)
     ALLOC(c->d_nghost, sizeof(int));
     ALLOC(c->gh_blk, sizeof(int) * (8 * (m / 1024 + 1) + 8));
     ALLOC(c->gh_start, sizeof(int) * (8 * (m / 1024 + 1) + 8));
+    ALLOC(c->gh_tag, (size_t)m + 16);
     ALLOC(c->ent_row, sizeof(int) * (m + c->gcap));
     ALLOC(c->ent_ix, sizeof(int) * (m + c->gcap));
     c->nrows = c->dc.nyh * c->dc.nzh;
@@ -512,7 +513,7 @@ extern "C" int dl_destroy(dl_ctx *c)
     for (int k = 0; k < 3; k++) { F(c->vpv[k]); F(c->dmv[k]); F(c->pert[k]); F(c->f64_own[k]); }
     F(c->rad); F(c->gid); F(c->ref_of_dev); F(c->dev_of_ref); F(c->keys); F(c->perm); F(c->perm_scratch);
     F(c->long_rows); F(c->n_long);
-    F(c->brick_start); F(c->brick_cnt); F(c->lhnode); F(c->bg); F(c->ghosts); F(c->d_nghost); F(c->gh_blk); F(c->gh_start); F(c->pert_tmp); F(c->lv_src); F(c->lv_list); F(c->lv_n);
+    F(c->brick_start); F(c->brick_cnt); F(c->lhnode); F(c->bg); F(c->ghosts); F(c->d_nghost); F(c->gh_blk); F(c->gh_start); F(c->gh_tag); F(c->pert_tmp); F(c->lv_src); F(c->lv_list); F(c->lv_n);
     F(c->ent_row); F(c->ent_ix); F(c->row_start); F(c->row_fill); F(c->row_ent); F(c->leave_nid);
     F(c->lv_refs); F(c->lv_old); F(c->lv_new); F(c->lv_dev); F(c->lv_dep); F(c->d_err); F(c->col_work);
     F(c->xfer64); F(c->xfer_i); F(c->hist_i); F(c->hist_d); F(c->acc_i); F(c->acc_d); F(c->out_i); F(c->out_d);

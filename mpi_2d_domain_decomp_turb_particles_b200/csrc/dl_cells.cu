@@ -63,8 +63,11 @@ __device__ __forceinline__ int row_of(const DevConst &D, int iy, int iz)
 // ---------------------------------------------------------------------------------------
 // Ghosts, partlib.f90:2211-2394 (single rank: every shift applies).  The ghost array is
 // built in the reference's ypn order: slot jid = 1..8, inside a slot ascending source
-// reference index, so ghost g has ypn index nps + g + 1.  Threads run over reference
-// indices; one count pass per 1024 references, a scan over (slot, block), one scatter.
+// reference index, so ghost g has ypn index nps + g + 1.  A pass in device order (coalesced
+// positions) writes each droplet's eight slot tags into a byte array by reference index;
+// then threads run over reference indices reading the tags (coalesced): one count pass per
+// 1024 references, a scan over (slot, block), one scatter that reads the positions of the
+// few droplets with ghosts only.
 // ---------------------------------------------------------------------------------------
 __device__ __forceinline__ unsigned ghost_tags(const DevConst &D, double y, double z, double dist)
 {
@@ -84,16 +87,18 @@ __device__ __forceinline__ unsigned ghost_tags(const DevConst &D, double y, doub
     return t;
 }
 
+__global__ void k_ghost_tags(DevConst D, int nps, const int *ref_of_dev, const double *py, const double *pz,
+                             double dist, unsigned char *tag)
+{
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d < nps) tag[ref_of_dev[d]] = (unsigned char)ghost_tags(D, py[d], pz[d], dist);
+}
+
 // per (slot, block of 1024 references) ghost counts, slot-major
-__global__ void __launch_bounds__(1024) k_ghost_count(DevConst D, int nps, const int *dev_of_ref, const double *py,
-                                                      const double *pz, double dist, int nblk, int *cnt)
+__global__ void __launch_bounds__(1024) k_ghost_count(int nps, const unsigned char *tag, int nblk, int *cnt)
 {
     const int r = blockIdx.x * 1024 + threadIdx.x;
-    unsigned t = 0;
-    if (r < nps) {
-        const int d = dev_of_ref[r];
-        t = ghost_tags(D, py[d], pz[d], dist);
-    }
+    const unsigned t = r < nps ? tag[r] : 0u;
     for (int k = 0; k < 8; k++) {
         const int n = __syncthreads_count((t >> k) & 1u);
         if (threadIdx.x == 0) cnt[k * nblk + blockIdx.x] = n;
@@ -101,19 +106,18 @@ __global__ void __launch_bounds__(1024) k_ghost_count(DevConst D, int nps, const
 }
 
 __global__ void __launch_bounds__(1024) k_ghost_scatter(DevConst D, int nps, const int *dev_of_ref, const double *py,
-                                                        const double *pz, double dist, int nblk, const int *start,
-                                                        Ghost *g, int cap)
+                                                        const double *pz, const unsigned char *tag, int nblk,
+                                                        const int *start, Ghost *g, int cap)
 {
     __shared__ int woff[8][32];
     const int r = blockIdx.x * 1024 + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    unsigned t = 0;
+    const unsigned t = r < nps ? tag[r] : 0u;
     int d = 0;
     double y = 0.0, z = 0.0;
-    if (r < nps) {
+    if (t) {
         d = dev_of_ref[r];
         y = py[d];
         z = pz[d];
-        t = ghost_tags(D, y, z, dist);
     }
     unsigned bal[8];
     for (int k = 0; k < 8; k++) {
@@ -180,38 +184,60 @@ __global__ void k_row_scatter(int ne, const int *ent_row, const int *ent_ix, con
     row_ent[s] = ((long long)ent_ix[e] << 32) | (unsigned)e;
 }
 
-// Sort each row by (ix, entry).  Rows hold tens of entries for uniformly spread droplets;
-// a warp sorts a row of up to kShortRow entries (each lane ranks its one or two keys
-// against the row's, the keys being distinct), longer rows are handed to k_row_sort_long.
+// Sort each row by (ix, entry) (the keys are distinct).  A warp takes 32 / G rows: a row of
+// up to G entries is ranked by its G-lane group (G = 8, 16 or 32, chosen from the mean row
+// length), a row of up to kShortRow entries by the whole warp (each lane ranks its one or
+// two keys against the row's), and longer rows are handed to k_row_sort_long.
 constexpr int kShortRow = 64;
 constexpr int kLongRowMax = 4096;   // entries a CTA can sort in (static) shared memory
 
+template <int G>
 __global__ void k_row_sort(int nrows, const int *row_start, long long *row_ent, int *long_rows, int *n_long)
 {
-    const int r = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-    if (r >= nrows) return;   // the whole warp
-    const int s = row_start[r], len = row_start[r + 1] - s;
-    if (len <= 1) return;
-    if (len > kShortRow) {
-        if (lane == 0) long_rows[atomicAdd(n_long, 1)] = r;
-        return;
+    constexpr int RPW = 32 / G;   // rows per warp
+    const int wid = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    const int r0 = wid * RPW;
+    if (r0 >= nrows) return;   // the whole warp
+    const int gl = lane & (G - 1), r = r0 + lane / G;
+    int s = 0, len = 0;
+    if (r < nrows) {
+        s = row_start[r];
+        len = row_start[r + 1] - s;
     }
-    const long long v0 = lane < len ? row_ent[s + lane] : LLONG_MAX;
-    const long long v1 = lane + 32 < len ? row_ent[s + 32 + lane] : LLONG_MAX;
-    int r0 = 0, r1 = 0;
-    for (int i = 0; i < min(len, 32); i++) {
-        const long long u = __shfl_sync(0xffffffffu, v0, i);
-        r0 += u < v0;
-        r1 += u < v1;
-    }
-    for (int i = 32; i < len; i++) {
-        const long long u = __shfl_sync(0xffffffffu, v1, i - 32);
-        r0 += u < v0;
-        r1 += u < v1;
-    }
+    const bool small = len <= G;
+    const long long v = (small && gl < len) ? row_ent[s + gl] : LLONG_MAX;
+    int rk = 0;
+#pragma unroll
+    for (int i = 0; i < G; i++) rk += __shfl_sync(0xffffffffu, v, i, G) < v;
     __syncwarp();
-    if (lane < len) row_ent[s + r0] = v0;
-    if (lane + 32 < len) row_ent[s + r1] = v1;
+    if (small && len > 1 && gl < len) row_ent[s + rk] = v;
+    unsigned big = __ballot_sync(0xffffffffu, gl == 0 && !small);
+    while (big) {
+        const int src = __ffs(big) - 1;
+        big &= big - 1;
+        const int rs = __shfl_sync(0xffffffffu, s, src), rl = __shfl_sync(0xffffffffu, len, src);
+        if (rl > kShortRow) {
+            if (lane == 0) long_rows[atomicAdd(n_long, 1)] = r0 + src / G;
+            continue;
+        }
+        const long long v0 = lane < rl ? row_ent[rs + lane] : LLONG_MAX;
+        const long long v1 = lane + 32 < rl ? row_ent[rs + 32 + lane] : LLONG_MAX;
+        int q0 = 0, q1 = 0;
+        for (int i = 0; i < min(rl, 32); i++) {
+            const long long u = __shfl_sync(0xffffffffu, v0, i);
+            q0 += u < v0;
+            q1 += u < v1;
+        }
+        for (int i = 32; i < rl; i++) {
+            const long long u = __shfl_sync(0xffffffffu, v1, i - 32);
+            q0 += u < v0;
+            q1 += u < v1;
+        }
+        __syncwarp();
+        if (lane < rl) row_ent[rs + q0] = v0;
+        if (lane + 32 < rl) row_ent[rs + q1] = v1;
+        __syncwarp();
+    }
 }
 
 // The long rows, one per CTA of a fixed grid (the count stays on the device): bitonic sort
@@ -1057,11 +1083,13 @@ int launch_headlist(dl_ctx *c, double dist)
     c->nei_valid = 0;   // the neighbour lists index this cell list
     if (nps > 0) {
         const int nblk = dl_blocks(nps, 1024);
-        k_ghost_count<<<nblk, 1024, 0, c->stream>>>(D, nps, c->dev_of_ref, P[1], P[2], dist, nblk, c->gh_blk);
+        k_ghost_tags<<<dl_blocks(nps, t), t, 0, c->stream>>>(D, nps, c->ref_of_dev, P[1], P[2], dist, c->gh_tag);
+        DL_CHECK_LAUNCH(c);
+        k_ghost_count<<<nblk, 1024, 0, c->stream>>>(nps, c->gh_tag, nblk, c->gh_blk);
         DL_CHECK_LAUNCH(c);
         int r = dl_scan(c, c->gh_blk, c->gh_start, 8 * nblk);
         if (r) return r;
-        k_ghost_scatter<<<nblk, 1024, 0, c->stream>>>(D, nps, c->dev_of_ref, P[1], P[2], dist, nblk, c->gh_start,
+        k_ghost_scatter<<<nblk, 1024, 0, c->stream>>>(D, nps, c->dev_of_ref, P[1], P[2], c->gh_tag, nblk, c->gh_start,
                                                       c->ghosts, c->gcap);
         DL_CHECK_LAUNCH(c);
         DL_CUDA(c, cudaMemcpyAsync(&ng, c->gh_start + 8 * nblk, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -1084,8 +1112,15 @@ int launch_headlist(dl_ctx *c, double dist)
                                                              (long long *)c->row_ent);
         DL_CHECK_LAUNCH(c);
         DL_CUDA(c, cudaMemsetAsync(c->n_long, 0, sizeof(int), c->stream));
-        k_row_sort<<<(int)(((int64_t)c->nrows * 32 + t - 1) / t), t, 0, c->stream>>>(
-            c->nrows, c->row_start, (long long *)c->row_ent, c->long_rows, c->n_long);
+        // group width from the mean row length (a Poisson row of mean m rarely exceeds 2 m)
+        const double mean = (double)ne / (double)std::max(c->nrows, 1);
+        const int g = mean <= 3.5 ? 8 : (mean <= 7.5 ? 16 : 32);
+        const int64_t nthr = ((int64_t)c->nrows + 32 / g - 1) / (32 / g) * 32;
+        const int nb = (int)((nthr + t - 1) / t);
+        auto *rs = (long long *)c->row_ent;
+        if (g == 8) k_row_sort<8><<<nb, t, 0, c->stream>>>(c->nrows, c->row_start, rs, c->long_rows, c->n_long);
+        else if (g == 16) k_row_sort<16><<<nb, t, 0, c->stream>>>(c->nrows, c->row_start, rs, c->long_rows, c->n_long);
+        else k_row_sort<32><<<nb, t, 0, c->stream>>>(c->nrows, c->row_start, rs, c->long_rows, c->n_long);
         DL_CHECK_LAUNCH(c);
         // crowded rows (none for uniformly spread droplets): a fixed grid reads their count
         // on the device; an over-long row is reported through the device error flags

@@ -136,6 +136,7 @@ struct dl_ctx {
     Ghost *ghosts;               // in the reference's ypn order (slot, then source reference index)
     int gcap, nghost;
     int *gh_blk, *gh_start;      // [8 * nblk + 1] ghost counts per (slot, 1024 references) and offsets
+    unsigned char *gh_tag;       // [msize] ghost slots of each droplet, by reference index
     int *d_nghost;
     int *ent_row;                // row of each entry (owned + ghosts)
     int *ent_ix;                 // ix of each entry
