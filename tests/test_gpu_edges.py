@@ -180,3 +180,38 @@ def test_collision_candidate_list_overflow_is_enlarged(monkeypatch):
             cand += rep.candidate_pairs
         assert cand > 16
         g.close()
+
+
+def test_device_timers():
+    """dl_timing / dl_timing_split over update steps, the eight phase times of a particle
+    step, and the flow step's four timed parts."""
+    import torch
+    from mpi_2d_domain_decomp_turb_particles_b200.flow import Flow
+    n = 32
+    g = Partlib(dense_params(n=n, npart=6000, precision="mixed"))
+    g.part_init()
+    g.set_fields(*smooth_field(n))
+    for _ in range(3):
+        g.update_step()
+    g.timing(reset=True)
+    for _ in range(4):
+        g.update_step()
+    ims, ams = g.timing_split()
+    kms, steps, launches = g.timing(reset=True)
+    assert steps == 4 and launches > 0
+    assert ims > 0 and ams > 0 and abs(ims + ams - kms) <= 0.05 * kms + 1e-3
+    g.particle_step()
+    ph = g.phase_times()
+    assert ph.shape == (8,) and (ph >= 0).all() and ph[0] > 0 and ph[7] > 0 and ph[7] <= ph[0] + 1e-3
+    g.close()
+    fl = Flow(n, 0.01, 1e-3, forcing=0, device=0)
+    u = np.zeros((3, n, n, n))
+    u[0] = np.sin(np.arange(n) * 2 * np.pi / n)[None, :, None]
+    fl.set_velocity(u)
+    fl.timing(True)
+    for _ in range(3):
+        fl.step()
+    t = fl.timing(False)
+    assert t["steps"] == 3 and all(t[k] > 0 for k in ("fft_inverse", "cross", "fft_forward", "update"))
+    fl.close()
+    torch.cuda.synchronize()
