@@ -73,7 +73,7 @@ typedef struct dl_params {
     /* ---- B200 build choices (no reference counterpart) ---- */
     int precision;               /* DL_FP64 or DL_MIXED */
     int init_velocity;           /* 0: terminal velocity (partlib.f90:564-566); 1: fluid velocity; 2: fluid + terminal */
-    int resort_interval;         /* steps between spatial re-sorts of the device order; 0 -> 16 (mixed), 8 (FP64) */
+    int resort_interval;         /* steps between spatial re-sorts of the device order; 0 -> 16 */
     int device;                  /* CUDA device ordinal */
     int gmres_launch;            /* mixed FP32 GMRES: 0 -> one cooperative launch when the grid fits; 1 -> launches per iteration */
 } dl_params;

@@ -385,7 +385,7 @@ extern "C" int dl_create(const dl_params *p, dl_ctx **out)
     if (c->p.mevent <= 0) c->p.mevent = std::max(4096, p->npart / 8);
     c->msize = c->p.msize;
     // FP32 bricks hold a droplet for ~16 steps of drift, the smaller FP64 bricks for ~8
-    c->resort_interval = p->resort_interval > 0 ? p->resort_interval : (p->precision == DL_MIXED ? 16 : 8);
+    c->resort_interval = p->resort_interval > 0 ? p->resort_interval : 16;   // measured best for both precisions at 256^3/1M
     c->nps = 0;
     c->istep = 0;
     c->time = 0.0;

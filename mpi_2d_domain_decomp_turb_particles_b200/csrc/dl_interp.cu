@@ -945,44 +945,6 @@ __global__ void k_brick_keys(int nps, const double *px, const double *py, const 
     atomicAdd(&cnt[key], 1);
 }
 
-// Exclusive scan of cnt[0..m) into start[0..m] by one CTA of 1024 threads.
-__global__ void k_scan_single(const int *cnt, int *start, int m)
-{
-    __shared__ int warp_sums[32];
-    __shared__ int carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int base = 0; base < m; base += blockDim.x) {
-        int i = base + threadIdx.x;
-        int v = i < m ? cnt[i] : 0;
-        int incl = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        if (lane == 31) warp_sums[w] = incl;
-        __syncthreads();
-        if (w == 0) {
-            int s = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
-            int si = s;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int y = __shfl_up_sync(0xffffffffu, si, o);
-                if (lane >= o) si += y;
-            }
-            warp_sums[lane] = si - s;
-        }
-        __syncthreads();
-        int excl = carry + warp_sums[w] + incl - v;
-        if (i < m) start[i] = excl;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry = excl + v;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) start[m] = carry;
-}
 
 // Slots within a brick: lanes of a warp that share a brick take consecutive slots in lane
 // order (one atomic per brick per warp), so runs of droplets that stay in their brick
@@ -1257,8 +1219,10 @@ int launch_brick_sort(dl_ctx *c)
                                                          c->bz, c->nbx, c->nby, c->nbz, c->bz == 1, c->keys,
                                                          c->brick_cnt, c->rad, c->has_dead ? c->nbricks : -1);
     DL_CHECK_LAUNCH(c);
-    k_scan_single<<<1, 1024, 0, c->stream>>>(c->brick_cnt, c->brick_start, nkeys);
-    DL_CHECK_LAUNCH(c);
+    {
+        const int r = dl_scan(c, c->brick_cnt, c->brick_start, nkeys);   // multi-block exclusive scan
+        if (r) return r;
+    }
     DL_CUDA(c, cudaMemsetAsync(c->brick_cnt, 0, sizeof(int) * nkeys, c->stream));
     k_brick_scatter<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, c->keys, c->brick_start, c->brick_cnt, c->perm);
     DL_CHECK_LAUNCH(c);
