@@ -423,7 +423,6 @@ static int allocate_state(dl_ctx *c)
     ALLOC(c->perm, m * 4);
     // re-sort scratch: positions, radius, id (8 bytes), 3x3 + 3x3 + 3 + 3 + 3 history/state arrays
     // (element size of the precision) and the reference index (4 bytes)
-    ALLOC(c->perm_scratch, m * (5 * 8 + 27 * c->esz + 4 + 8));
     dl_brick_dims(c->mixed, &c->bx, &c->by, &c->bz);
     const int n = c->dc.n;
     c->nbx = (n + c->bx - 1) / c->bx;
@@ -511,12 +510,18 @@ extern "C" int dl_destroy(dl_ctx *c)
     for (int s = 0; s < 4; s++)
         for (int k = 0; k < 3; k++) { F(c->vel[s][k]); F(c->flu[s][k]); }
     for (int k = 0; k < 3; k++) { F(c->vpv[k]); F(c->dmv[k]); F(c->pert[k]); F(c->f64_own[k]); }
-    F(c->rad); F(c->gid); F(c->ref_of_dev); F(c->dev_of_ref); F(c->keys); F(c->perm); F(c->perm_scratch);
+    F(c->rad); F(c->gid); F(c->ref_of_dev); F(c->dev_of_ref); F(c->keys); F(c->perm);
     F(c->long_rows); F(c->n_long);
     F(c->brick_start); F(c->brick_cnt); F(c->lhnode); F(c->bg); F(c->ghosts); F(c->d_nghost); F(c->gh_blk); F(c->gh_start); F(c->gh_tag); F(c->pert_tmp); F(c->lv_src); F(c->lv_list); F(c->lv_n);
     F(c->ent_row); F(c->ent_ix); F(c->row_start); F(c->row_fill); F(c->row_ent); F(c->leave_nid);
     F(c->lv_refs); F(c->lv_old); F(c->lv_new); F(c->lv_dev); F(c->lv_dep); F(c->d_err); F(c->col_work);
     F(c->xfer64); F(c->xfer_i); F(c->hist_i); F(c->hist_d); F(c->acc_i); F(c->acc_d); F(c->out_i); F(c->out_d);
+    for (int b = 0; b < 2; b++)
+        for (int k = 0; k < 3; k++) F(c->sh_pos[b][k]);
+    for (int q = 0; q < 4; q++)
+        for (int k = 0; k < 3; k++) { F(c->sh_vel[q][k]); F(c->sh_flu[q][k]); }
+    for (int k = 0; k < 3; k++) { F(c->sh_vpv[k]); F(c->sh_dmv[k]); F(c->sh_pert[k]); }
+    F(c->sh_rad); F(c->sh_gid); F(c->sh_ref);
     F(c->counts); F(c->cand); F(c->coll_list); F(c->coll_n); F(c->coll_flag); F(c->pairs); F(c->contacts); F(c->remove_dev); F(c->pair_buf); F(c->pair_ibuf); F(c->mv_acc);
     F(c->ovl_list); F(c->ovl_cnt); F(c->fpad_own);
     F(c->nei_cnt); F(c->nei_start); F(c->nei_idx); F(c->nei_coef); F(c->nei_coef64); F(c->overlap_flag);

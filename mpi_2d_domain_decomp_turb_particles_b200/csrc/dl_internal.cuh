@@ -103,7 +103,13 @@ struct dl_ctx {
     int *brick_start;            // nbricks + 1
     int *brick_cnt;              // nbricks
     int *keys, *perm;            // per droplet
-    void *perm_scratch;          // re-sort scratch: every permuted array once (msize each)
+    // re-sort targets: one buffer per permuted array (allocated at the first re-sort); the
+    // permutation gathers each array into its shadow and the two pointers swap
+    double *sh_pos[2][3];
+    void *sh_vel[4][3], *sh_flu[4][3], *sh_vpv[3], *sh_dmv[3], *sh_pert[3];
+    double *sh_rad, *sh_gid;
+    int *sh_ref;
+    int have_shadows;
     int steps_since_sort;
     int resort_interval;
     int sorted;

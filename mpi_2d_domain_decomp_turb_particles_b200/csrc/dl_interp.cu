@@ -996,11 +996,10 @@ __global__ void k_gather(int nps, const int *perm, const E *in, E *out)
 
 struct PermTable {
     int n8, n4;
-    long long m;                         // stride of the scratch slices (msize)
-    unsigned long long *a8[40];
-    unsigned int *a4[40];
-    unsigned long long *s8;
-    unsigned int *s4;
+    const unsigned long long *a8[40];   // sources
+    const unsigned int *a4[40];
+    unsigned long long *d8[40];         // targets (the arrays' shadows)
+    unsigned int *d4[40];
 };
 
 __global__ void __launch_bounds__(256) k_permute_gather(int nps, const int *perm, PermTable t)
@@ -1008,16 +1007,8 @@ __global__ void __launch_bounds__(256) k_permute_gather(int nps, const int *perm
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nps) return;
     const int j = perm[i];
-    for (int a = 0; a < t.n8; a++) t.s8[a * t.m + i] = t.a8[a][j];
-    for (int a = 0; a < t.n4; a++) t.s4[a * t.m + i] = t.a4[a][j];
-}
-
-__global__ void __launch_bounds__(256) k_permute_copyback(int nps, PermTable t)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nps) return;
-    for (int a = 0; a < t.n8; a++) t.a8[a][i] = t.s8[a * t.m + i];
-    for (int a = 0; a < t.n4; a++) t.a4[a][i] = t.s4[a * t.m + i];
+    for (int a = 0; a < t.n8; a++) t.d8[a][i] = t.a8[a][j];
+    for (int a = 0; a < t.n4; a++) t.d4[a][i] = t.a4[a][j];
 }
 
 __global__ void k_inverse(int nps, const int *ref_of_dev, int *dev_of_ref)
@@ -1231,31 +1222,64 @@ int launch_brick_sort(dl_ctx *c)
                                                                                  c->keys);
     DL_CHECK_LAUNCH(c);
     int *perm = c->keys;
-    // permute every live array in two passes: gather all of them into the scratch region,
-    // then copy back (coalesced); one index load per droplet for ~30 arrays
+    // permute every live array: one gather pass into the array's shadow buffer (one index
+    // load per droplet for ~30 arrays), then the pointers of array and shadow swap
+    if (!c->have_shadows) {
+        const size_t m = (size_t)c->msize, es = (size_t)c->esz;
+        auto al = [&](void **p, size_t bytes) -> int {
+            if (cudaMalloc(p, bytes) != cudaSuccess) {
+                *p = nullptr;
+                return dl_fail(c, DL_E_ALLOC, "re-sort: cudaMalloc of the shadow buffers failed");
+            }
+            return 0;
+        };
+        int r = 0;
+        for (int b = 0; b < 2 && !r; b++)
+            for (int k = 0; k < 3 && !r; k++) r = al((void **)&c->sh_pos[b][k], m * 8);
+        for (int q = 0; q < 4 && !r; q++)
+            for (int k = 0; k < 3 && !r; k++) {
+                r = al(&c->sh_vel[q][k], m * es);
+                if (!r) r = al(&c->sh_flu[q][k], m * es);
+            }
+        for (int k = 0; k < 3 && !r; k++) {
+            r = al(&c->sh_vpv[k], m * es);
+            if (!r) r = al(&c->sh_dmv[k], m * es);
+            if (!r && c->pert[k]) r = al(&c->sh_pert[k], m * es);
+        }
+        if (!r) r = al((void **)&c->sh_rad, m * 8);
+        if (!r) r = al((void **)&c->sh_gid, m * 8);
+        if (!r) r = al((void **)&c->sh_ref, m * 4);
+        if (r) return r;
+        c->have_shadows = 1;
+    }
     PermTable tb;
     memset(&tb, 0, sizeof(tb));
-    auto add8 = [&](void *a) { tb.a8[tb.n8++] = (unsigned long long *)a; };
-    auto add4 = [&](void *a) { tb.a4[tb.n4++] = (unsigned int *)a; };
-    auto addT = [&](void *a) { if (c->mixed) add4(a); else add8(a); };
+    std::vector<std::pair<void **, void **>> swaps;   // (array pointer, shadow pointer)
+    auto add = [&](void **arr, void **sh, size_t esz) {
+        if (esz == 8) {
+            tb.a8[tb.n8] = (const unsigned long long *)*arr;
+            tb.d8[tb.n8++] = (unsigned long long *)*sh;
+        } else {
+            tb.a4[tb.n4] = (const unsigned int *)*arr;
+            tb.d4[tb.n4++] = (unsigned int *)*sh;
+        }
+        swaps.emplace_back(arr, sh);
+    };
+    const size_t es = (size_t)c->esz;
     for (int k = 0; k < 3; k++) {
-        add8(c->pos[c->pcur][k]);
-        for (int l = 0; l < 3; l++) addT(c->vel[(c->vcur + l) % 4][k]);
-        for (int l = 0; l < 3; l++) addT(c->flu[(c->fcur + l) % 4][k]);
-        addT(c->vpv[k]);
-        addT(c->dmv[k]);
-        if (c->pert[k]) addT(c->pert[k]);
+        add((void **)&c->pos[c->pcur][k], (void **)&c->sh_pos[c->pcur][k], 8);
+        for (int l = 0; l < 3; l++) add(&c->vel[(c->vcur + l) % 4][k], &c->sh_vel[(c->vcur + l) % 4][k], es);
+        for (int l = 0; l < 3; l++) add(&c->flu[(c->fcur + l) % 4][k], &c->sh_flu[(c->fcur + l) % 4][k], es);
+        add(&c->vpv[k], &c->sh_vpv[k], es);
+        add(&c->dmv[k], &c->sh_dmv[k], es);
+        if (c->pert[k]) add(&c->pert[k], &c->sh_pert[k], es);
     }
-    add8(c->rad);
-    add8(c->gid);
-    add4(c->ref_of_dev);
-    tb.s8 = (unsigned long long *)c->perm_scratch;
-    tb.s4 = (unsigned int *)((unsigned long long *)c->perm_scratch + (size_t)tb.n8 * c->msize);
-    tb.m = c->msize;
+    add((void **)&c->rad, (void **)&c->sh_rad, 8);
+    add((void **)&c->gid, (void **)&c->sh_gid, 8);
+    add((void **)&c->ref_of_dev, (void **)&c->sh_ref, 4);
     k_permute_gather<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, perm, tb);
     DL_CHECK_LAUNCH(c);
-    k_permute_copyback<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, tb);
-    DL_CHECK_LAUNCH(c);
+    for (auto &sw : swaps) std::swap(*sw.first, *sw.second);
     if (c->has_dead) {
         int live = 0;
         DL_CUDA(c, cudaMemcpyAsync(&live, c->brick_start + c->nbricks, sizeof(int), cudaMemcpyDeviceToHost,
