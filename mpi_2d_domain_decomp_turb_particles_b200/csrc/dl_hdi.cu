@@ -90,7 +90,7 @@ __device__ __forceinline__ void stokes_tensor(double arad, double dnij, const do
 struct NeiApp {
     int owner, partner;
     unsigned long long key;
-    double coef[6];
+    double arad, dnij, xd[3];   // the Stokes coefficients' inputs (computed when scattered)
 };
 
 struct NeiArgs {
@@ -124,10 +124,14 @@ __device__ __forceinline__ void nei_emit(const NeiArgs &A, int owner, int partne
     e.owner = owner;
     e.partner = partner;
     e.key = key;
-    stokes_tensor(arad, dnij, xd, e.coef);
+    e.arad = arad;
+    e.dnij = dnij;
+    e.xd[0] = xd[0]; e.xd[1] = xd[1]; e.xd[2] = xd[2];
 }
 
-// appended entries -> CSR slots of their owners (order fixed afterwards by k_nei_sort)
+// appended entries -> CSR slots of their owners (order fixed afterwards by k_nei_sort),
+// with their Stokes coefficients: computed here, one thread per entry, rather than in the
+// divergent walk
 __global__ void k_nei_scatter(int nnz, const NeiApp *app, const int *start, int *fill, int *partner,
                               unsigned long long *key, double *coef)
 {
@@ -137,7 +141,9 @@ __global__ void k_nei_scatter(int nnz, const NeiApp *app, const int *start, int 
     const int slot = start[e.owner] + atomicAdd(&fill[e.owner], 1);
     partner[slot] = e.partner;
     key[slot] = e.key;
-    for (int t = 0; t < 6; t++) coef[(int64_t)slot * 6 + t] = e.coef[t];
+    double c6[6];
+    stokes_tensor(e.arad, e.dnij, e.xd, c6);
+    for (int t = 0; t < 6; t++) coef[(int64_t)slot * 6 + t] = c6[t];
 }
 
 // One thread per sorted entry that is an owned droplet: consecutive threads own
