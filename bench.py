@@ -297,7 +297,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
     from mpi_2d_domain_decomp_turb_particles_b200.bytes_model import (advance_bytes, collision_bytes, interp_bytes,
-                                                                      update_bytes)
+                                                                      interp_onchip, update_bytes)
 
     ws, rank, local = _dist()
     if ws > 1:
@@ -319,6 +319,7 @@ def run_ours(args):
         dist.barrier()
     ms_step, kernel_ms, launches, interp_ms, adv_ms = _time_update(g, stream, args.steps, args.warmup, torch)
     clocks = _clock_summary(clk)
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
     ms_step, kernel_ms = max_over_ranks([ms_step, kernel_ms], ws, device=f"cuda:{dev}")
     value = replica_value(ws, N_PART, ms_step)
 
@@ -408,10 +409,12 @@ def run_ours(args):
             "kernels": {
                 "mixed": {"interp_ms": interp_ms, "advance_ms": adv_ms,
                           "interp_gbs": _gbs(interp_bytes("mixed", N_GRID, N_PART), interp_ms),
-                          "advance_gbs": _gbs(advance_bytes("mixed", N_GRID, N_PART), adv_ms)},
+                          "advance_gbs": _gbs(advance_bytes("mixed", N_GRID, N_PART), adv_ms),
+                          "interp_onchip": interp_onchip("mixed", N_PART, interp_ms, nsm, clocks)},
                 "fp64": {"update_kernels_ms": kms64, "interp_ms": ims64, "advance_ms": ams64,
                          "interp_gbs": _gbs(interp_bytes("fp64", N_GRID, N_PART), ims64),
                          "advance_gbs": _gbs(advance_bytes("fp64", N_GRID, N_PART), ams64),
+                         "interp_onchip": interp_onchip("fp64", N_PART, ims64, nsm, clocks),
                          "algorithmic_bytes": alg64}},
             "full_step_ms": full_ms, "collision_ms": coll_ms,
             "collision_candidate_pairs_per_s": cand / (coll_ms * 1e-3) if coll_ms > 0 else None,

@@ -48,3 +48,35 @@ def collision_bytes(precision: str, npart: int) -> int:
     velocity, fluid velocity: 12 words).  A lower bound: the ghost entries (a few per cent
     of the droplets) and the cell start table are not counted."""
     return (48 + 12 * FIELD_WORD[precision]) * npart
+
+
+# The interpolation's on-chip floor.  Every (droplet, component) evaluates a 6 x 6 x 6
+# stencil out of shared memory: 216 loads and 216 FMAs (FP32), or 216 loads, 648 DMUL and
+# 216 DADD (FP64, the reference's order ((v * wx) * wy) * wz added term by term).
+# Shared memory returns one 128-byte wavefront per SM per clock, one warp-wide FP32 load
+# when the lanes fall in distinct banks; the FP64 pipe retires 64 operations per SM per
+# clock on B200 (37 TFLOP/s of FP64 FMA over 148 SMs at 1.965 GHz).
+STENCIL_POINTS = 216
+FP64_OPS_PER_SM_CLOCK = 64
+
+
+def interp_onchip(precision: str, npart: int, measured_ms: float, num_sms: int, clocks: dict | None) -> dict:
+    """Lower bound of the interpolation kernel set by the on-chip unit it leans on (shared
+    memory for FP32, the FP64 pipe for FP64) at the SM clock sampled during the run, and
+    the fraction of it the measured kernel time reaches."""
+    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz") or 1965.0
+    hz = float(mhz) * 1e6
+    tasks = 3 * npart
+    if precision == "mixed":
+        units = tasks * STENCIL_POINTS / 32.0               # wavefronts at full lane use
+        floor_s = units / (num_sms * hz)
+        bound = "shared-memory wavefronts (one 32-lane FP32 load per SM per clock)"
+        unit_name = "wavefronts"
+    else:
+        units = tasks * STENCIL_POINTS * 4.0                # 3 DMUL + 1 DADD per term
+        floor_s = units / (num_sms * FP64_OPS_PER_SM_CLOCK * hz)
+        bound = "FP64 pipe (64 operations per SM per clock)"
+        unit_name = "fp64_ops"
+    floor_ms = floor_s * 1e3
+    return {"bound": bound, unit_name: units, "sm_mhz": float(mhz), "floor_ms": floor_ms,
+            "frac": floor_ms / measured_ms if measured_ms and measured_ms > 0 else None}

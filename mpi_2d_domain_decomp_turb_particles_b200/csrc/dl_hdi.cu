@@ -153,9 +153,9 @@ __global__ void k_nei_scatter(int nnz, const NeiApp *app, const int *start, int 
 // a radius) and every overlap (below the sum of two radii) lies there, and the entries
 // keep the keys of the full box.  The reach uses the largest radius of the current
 // droplets (coalescence can grow droplets past the largest initial radius).  The walk is
-// bound by memory latency: 64 registers and 8 CTAs per SM (a few bytes spilled) hide it
-// better than 80 registers and 6 CTAs.
-__global__ void __launch_bounds__(128, 8) k_nei_walk(NeiArgs A)
+// bound by memory latency: 48 registers and 10 CTAs per SM (32 bytes spilled) hide it
+// better than 64 registers and 8 CTAs or 80 and 6; at 12 CTAs the spills grow to 72 bytes.
+__global__ void __launch_bounds__(128, 10) k_nei_walk(NeiArgs A)
 {
     const int sa = blockIdx.x * blockDim.x + threadIdx.x;
     if (sa >= A.ne) return;

@@ -8,7 +8,8 @@
 // Design (B200): one kernel for both precisions, k_interp_col<T>.  Droplets are kept sorted
 // by (column of CX x CY cells, z plane) -- 16 x 16 cells for FP32, 16 x 8 for FP64 -- and
 // each CTA sweeps work items (a column over a range of planes) in z, the field streaming
-// through a ring of shared-memory slabs (four planes, three components, one TMA box each),
+// through a ring of shared-memory slabs (SPL planes: four FP32, two FP64; three components;
+// one TMA box each),
 // with warp-specialised producer, prep, stencil and release warps.  The stencil warps
 // evaluate the 216-point stencil of every (droplet, component) task out of shared memory in
 // rounds whose loads start in distinct banks.
@@ -31,15 +32,35 @@ namespace {
 // ---------------------------------------------------------------------------------------
 // 6-point Lagrange weights, partlib.f90:317-338 (FP64, exact source order)
 // ---------------------------------------------------------------------------------------
+// x / D correctly rounded, for D = 3 * 2^k or 15 * 2^k: one correction step of x * RN(1/D)
+// (Markstein, IBM J. Res. Dev. 34(1), 1990; Brisebarre, Muller and Raina, IEEE Trans.
+// Comput. 53(8), 2004).  q = RN(x * RN(1/D)) is within 1.5 ulp of x / D, the remainder
+// r = x - q * D is exact in one FMA, and q + r * RN(1/D) differs from x / D by at most
+// 2^-52 ulp.  x / D is either representable or at least 1/(2 * 15) ulp away from every
+// rounding boundary (twice the quotient in ulps of the quotient is an integer over 3 or
+// 15), so the final rounding is the correctly rounded quotient; r == 0 keeps the sign of
+// a zero quotient.
+template <int D>
+__device__ __forceinline__ double div_const(double x)
+{
+    static_assert(D == 12 || D == 24 || D == 120, "divisors with a proven one-step correction");
+    constexpr double inv = 1.0 / D;
+    const double q = __dmul_rn(x, inv);
+    const double r = __fma_rn(-q, (double)D, x);
+    return r == 0.0 ? q : __fma_rn(r, inv, q);
+}
+
+// The weights with the reference's numerators, in its order; the divisions by 120, 24 and
+// 12 give the same correctly rounded quotients as the reference's.
 __device__ __forceinline__ void lagrange6(double z, double *b)
 {
     double z2 = z * z, z3 = z2 * z, z4 = z3 * z, z5 = z4 * z;
-    b[0] = (6.0 * z - 5.0 * z2 - 5.0 * z3 + 5.0 * z4 - z5) / 120.0;
-    b[1] = (-12.0 * z + 16.0 * z2 - z3 - 4.0 * z4 + z5) / 24.0;
-    b[2] = (12.0 - 4.0 * z - 15.0 * z2 + 5.0 * z3 + 3.0 * z4 - z5) / 12.0;
-    b[3] = (12.0 * z + 8.0 * z2 - 7.0 * z3 - 2.0 * z4 + z5) / 12.0;
-    b[4] = (-6.0 * z - z2 + 7.0 * z3 + z4 - z5) / 24.0;
-    b[5] = (4.0 * z - 5.0 * z3 + z5) / 120.0;
+    b[0] = div_const<120>(6.0 * z - 5.0 * z2 - 5.0 * z3 + 5.0 * z4 - z5);
+    b[1] = div_const<24>(-12.0 * z + 16.0 * z2 - z3 - 4.0 * z4 + z5);
+    b[2] = div_const<12>(12.0 - 4.0 * z - 15.0 * z2 + 5.0 * z3 + 3.0 * z4 - z5);
+    b[3] = div_const<12>(12.0 * z + 8.0 * z2 - 7.0 * z3 - 2.0 * z4 + z5);
+    b[4] = div_const<24>(-6.0 * z - z2 + 7.0 * z3 + z4 - z5);
+    b[5] = div_const<120>(4.0 * z - 5.0 * z3 + z5);
 }
 
 // FP32 weights (mixed path): the same polynomials in Horner form with FMA.
@@ -340,7 +361,7 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, u
 // Column sweep (both precisions).  The device order is sorted by (column, z plane), a
 // column being CX x CY cells in x-y.  The work items are (column, segment of zseg planes);
 // each CTA sweeps its items in z:
-//  * the producer warp streams the field through a ring of NSL slabs, a slab being four
+//  * the producer warp streams the field through a ring of NSL slabs, a slab being SPL
 //    consecutive planes of the item's column plus the stencil halo, all three components,
 //    in one TMA box (a TMA copy costs about the same issue time whatever its size, so the
 //    boxes are made large);
@@ -354,22 +375,24 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, u
 //  * a release warp hands the slabs no finished batch needs any more back to the producer
 //    and the batch slot back to the prep warps.
 // Each plane of an item enters shared memory once; only the 3 + 3 halo planes at the ends
-// of an item (and up to three padding planes that round it to whole slabs) are extra.
+// of an item (and up to SPL - 1 padding planes that round it to whole slabs) are extra.
 // Droplets whose stencil is not inside the staged planes (drifted further than the
 // margins since the last sort) are evaluated by the prep warp from the padded field in
 // global memory with the same arithmetic.
 //
-// Slab layout in shared memory: [plane 0..3][component][y][x] (the tensor map orders the
+// Slab layout in shared memory: [plane 0..SPL-1][component][y][x] (the tensor map orders the
 // field's dimensions x, y, component, z).  With BOX = EX * EY elements per component plane,
 // PS = ncomp * BOX per plane and NBK banks of one element (32 for FP32, 16 double-banks for
-// FP64), 4 * PS = 0 (mod NBK) and every slab slot starts at bank 0: plane u of the sweep
+// FP64), SPL * PS = 0 (mod NBK) and every slab slot starts at bank 0: plane u of the sweep
 // starts at bank PS * u (mod NBK) whatever slab slot holds it, so the bank of a stencil's
 // start plus PS * k is the bank of its plane k, the same shift for every lane of a round.
 // ---------------------------------------------------------------------------------------
 // Per-precision geometry of the column sweep.  FP32: columns of 16 x 16 cells, 32 bank
-// buckets of one word; FP64: columns of 16 x 8 cells (a slab of four planes of three
-// components is then 34.6 KB), 16 buckets of one double (two banks): a 64-bit shared load
-// is served per half-warp, so lanes L and L + 16 take consecutive entries of bucket L % 16.
+// buckets of one word, slabs of four planes (26.5 KB); FP64: columns of 16 x 8 cells, 16
+// buckets of one double (two banks): a 64-bit shared load is served per half-warp, so
+// lanes L and L + 16 take consecutive entries of bucket L % 16; slabs of two planes (17.3 KB),
+// so that the ring's slabs follow the batches' windows more closely than four-plane slabs
+// of twice the size (the same bytes hold a ring of 11 slabs of two planes, not 5 of four).
 template <typename T>
 struct ColGeo;
 template <>
@@ -378,6 +401,7 @@ struct ColGeo<float> {
     static constexpr int NBK = 32;                  // bank buckets
     static constexpr int CAP = 32;                  // entries per bucket (more go to the overflow list)
     static constexpr int NW = 3;                    // per-droplet words in the batch: x, y, z fractions
+    static constexpr int SPL = 4;                   // planes per slab (one TMA box)
 };
 template <>
 struct ColGeo<double> {
@@ -385,15 +409,15 @@ struct ColGeo<double> {
     static constexpr int NBK = 16;
     static constexpr int CAP = 64;
     static constexpr int NW = 18;                   // the 18 FP64 Lagrange weights, computed once
+    static constexpr int SPL = 2;                   // planes per slab: a finer ring of the larger FP64 planes
 };
 
 namespace colk {
 constexpr int M = 1;                             // y drift tolerated since the last sort (cells)
-constexpr int SPL = 4;                           // planes per slab (one TMA box)
 constexpr int NPROD = 1;                         // producer warps (slab j goes to the producer of slot j % NSL)
 template <typename T>
 struct G {
-    static constexpr int CX = ColGeo<T>::CX, CY = ColGeo<T>::CY;
+    static constexpr int CX = ColGeo<T>::CX, CY = ColGeo<T>::CY, SPL = ColGeo<T>::SPL;
     static constexpr int EX = CX + 8;            // tile row: x from cx*CX - 4 (16-byte aligned x)
     static constexpr int EY = CY + 5 + 2 * M;    // rows: y from cy*CY - 3
     static constexpr int BOX = EX * EY;          // elements of one component plane
@@ -500,7 +524,7 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + NPREP) * 32, 1)
     // NP must be a multiple of NPREP.
     static_assert(NP % NPREP == 0, "batch slots per prep warp");
     constexpr int CX = G<T>::CX, CY = G<T>::CY, EX = G<T>::EX, EY = G<T>::EY, BOX = G<T>::BOX;
-    constexpr int SLAB = G<T>::SLAB, NBK = G<T>::NBK, CAP = G<T>::CAP;
+    constexpr int SLAB = G<T>::SLAB, NBK = G<T>::NBK, CAP = G<T>::CAP, SPL = G<T>::SPL;
     constexpr bool F64 = sizeof(T) == 8;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     T *ring = reinterpret_cast<T *>(smem_raw);
@@ -1165,23 +1189,26 @@ __global__ void k_mean_vel(int nps, const T *ux, const T *uy, const T *uz, const
 }
 
 // Column sweep configuration per precision (columns of ColGeo<T>::CX x CY cells): a ring
-// of NSL slabs of colk::SPL planes, batches of PZ planes and at most MAXD droplets, NP
-// batch slots, NSW stencil warps, NPREP prep warps.  A batch's window (PZ + 7 planes) spans
-// at most (PZ + 9) / 4 + 1 slabs, which must leave the ring a slab to fill ahead.
+// of NSL slabs of SPL planes, batches of PZ planes and at most MAXD droplets, NP batch
+// slots, NSW stencil warps, NPREP prep warps.  A batch's window (PZ + 7 planes) spans at
+// most (PZ + 9) / SPL + 1 slabs, which must leave the ring a slab to fill ahead.  Measured at
+// 256^3 / 1M droplets: two prep warps keep twelve FP32 stencil warps fed (three prep and
+// eleven stencil warps were 2 % slower); FP64 gains 6 % from the eleventh two-plane slab
+// against ten (three batch slots instead of four pay for it).
 template <typename T>
 struct ColCfg;
 template <>
 struct ColCfg<float> {
-    static constexpr int NSL = 7, PZ = 8, MAXD = 160, NP = 3, NSW = 11, NPREP = 3;
+    static constexpr int NSL = 7, PZ = 8, MAXD = 160, NP = 4, NSW = 12, NPREP = 2;
 };
 template <>
 struct ColCfg<double> {
-    static constexpr int NSL = 5, PZ = 6, MAXD = 64, NP = 4, NSW = 10, NPREP = 4;
+    static constexpr int NSL = 11, PZ = 6, MAXD = 64, NP = 3, NSW = 10, NPREP = 3;
 };
 template <typename T>
 constexpr bool col_cfg_ok()
 {
-    return (ColCfg<T>::PZ + 9) / colk::SPL + 1 < ColCfg<T>::NSL;
+    return (ColCfg<T>::PZ + 9) / colk::G<T>::SPL + 1 < ColCfg<T>::NSL;
 }
 static_assert(col_cfg_ok<float>() && col_cfg_ok<double>(), "a batch window leaves a slab of the ring free");
 
@@ -1327,10 +1354,10 @@ static int launch_interp_col(dl_ctx *c, int comp_lo, int ncomp, int fused)
 {
     using Cf = ColCfg<T>;
     if (c->tmap_base != c->fpad) {
-        // one box per slab: colk::SPL planes of all three components, or of the single
+        // one box per slab: SPL planes of all three components, or of the single
         // component of a one-component INTERPOLATE call; dimensions ordered x, y, component, z
-        int r = make_tmap_zc(c, &c->tmap, colk::G<T>::EX, colk::G<T>::EY, 3, colk::SPL);
-        if (!r) r = make_tmap_zc(c, &c->tmap1, colk::G<T>::EX, colk::G<T>::EY, 1, colk::SPL);
+        int r = make_tmap_zc(c, &c->tmap, colk::G<T>::EX, colk::G<T>::EY, 3, colk::G<T>::SPL);
+        if (!r) r = make_tmap_zc(c, &c->tmap1, colk::G<T>::EX, colk::G<T>::EY, 1, colk::G<T>::SPL);
         if (r) return r;
         c->tmap_base = c->fpad;
     }
