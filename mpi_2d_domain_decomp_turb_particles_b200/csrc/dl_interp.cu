@@ -400,6 +400,7 @@ struct ColGeo<float> {
     static constexpr int CX = 16, CY = 16;
     static constexpr int NBK = 32;                  // bank buckets
     static constexpr int CAP = 32;                  // entries per bucket (more go to the overflow list)
+    static constexpr bool DENSE = false;            // round order (see ColBatch)
     static constexpr int NW = 3;                    // per-droplet words in the batch: x, y, z fractions
     static constexpr int SPL = 4;                   // planes per slab (one TMA box)
 };
@@ -407,7 +408,8 @@ template <>
 struct ColGeo<double> {
     static constexpr int CX = 16, CY = 8;
     static constexpr int NBK = 16;
-    static constexpr int CAP = 64;
+    static constexpr int CAP = 64;                  // layers of the dense order (more go to the overflow list)
+    static constexpr bool DENSE = true;             // round order (see ColBatch)
     static constexpr int NW = 18;                   // the 18 FP64 Lagrange weights, computed once
     static constexpr int SPL = 2;                   // planes per slab: a finer ring of the larger FP64 planes
 };
@@ -431,23 +433,28 @@ struct G {
 
 // Round order of a batch's tasks (droplet << 2 | component slot):
 //  * FP32, per bucket: round g gives lane r entry g of bucket r (conflict-free; a round has
-//    idle lanes where buckets hold fewer than the fullest one), then the overflow tasks;
+//    idle lanes where buckets hold fewer than the fullest one), then the overflow tasks
+//    (entries past CAP) in dense rounds.  (The code also serves NBK = 16 with lanes L and
+//    L + 16 on bucket L % 16; for FP64 that measured 12 % slower than the dense order.)
 //  * FP64, dense layer-major: entry 0 of every bucket holding one, buckets ascending, then
-//    entry 1, ...  Any 16 consecutive tasks (a half-warp's share) take each bucket at most
-//    once from a full layer and at most twice where the layers thin out, and every round is
-//    full: an FP64 term costs four FP64-pipe instructions against one 64-bit load, so full
-//    warps matter more there than the two-way conflicts.
+//    entry 1, ...: every round full.  Components 0 and 2 of a droplet start in the same
+//    bank (BOX = 8 mod 16), the buckets are uneven, and a half-warp's 16 tasks often
+//    straddle two layers and collide (98 M shared-memory wavefronts at 256^3 / 1M against
+//    49 M conflict-free: shared memory 71 % busy, the FP64 pipe 38 %).  Still the fastest
+//    order measured: the FP64 prep warps are on the critical path, and packing each
+//    half-warp greedily (13 % fewer wavefronts in a model of the batches) made the prep
+//    slower than the loads it saved (0.63 ms against 0.48 ms per interpolation).
 template <typename T, int MAXD>
 struct ColBatch {   // per-batch shared-memory area
-    static constexpr bool DENSE = sizeof(T) == 8;
-    static constexpr int CAP = ColGeo<T>::CAP;
+    static constexpr bool DENSE = ColGeo<T>::DENSE;
+    static constexpr int CAP = ColGeo<T>::CAP, NBK = ColGeo<T>::NBK;
     T w[MAXD][ColGeo<T>::NW];                 // FP32: x, y, z fractions; FP64: the weights
     int co[MAXD];                             // corner | first plane << 12, or -1 (global-memory path)
     int meta[16];   // d0, nd, rounds or tasks, overflow tasks, release lo, hi, end, next round, window end
     int cnt[32];                              // tasks per bank bucket
     unsigned lmask[DENSE ? CAP : 1];          // layer e: the buckets holding an entry e
     int loff[DENSE ? CAP : 1];                // layer e: its first position in the task list
-    unsigned short task[DENSE ? MAXD * 3 : 32 * CAP];   // per bucket: entry e of bucket r at e * 32 + r
+    unsigned short task[DENSE ? MAXD * 3 : NBK * CAP];  // per bucket: entry e of bucket r at e * NBK + r
     unsigned short ovf[DENSE ? 1 : MAXD * 3];           // per bucket: the overflow tasks
 };
 
@@ -859,7 +866,7 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + NPREP) * 32, 1)
                                 if (ek < 0) continue;
                                 const int e = ek >> 8, key = ek & 0xff;
                                 const unsigned short tk = (unsigned short)(((q * 32 + lane) << 2) | cc);
-                                if (e < CAP) S->task[e * 32 + key] = tk;
+                                if (e < CAP) S->task[e * NBK + key] = tk;
                                 else S->ovf[atomicAdd(&S->meta[3], 1)] = tk;
                             }
                         __syncwarp();
@@ -906,8 +913,11 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + NPREP) * 32, 1)
         const int d0 = S->meta[0];
         // DENSE: meta[2] tasks; per bucket: meta[2] full rounds, then the overflow tasks
         const int ntask = S->meta[2], novf = S->meta[3];
-        const int mycnt = B::DENSE ? 0 : min(S->cnt[lane], CAP);
-        const int total = B::DENSE ? (ntask + 31) / 32 : ntask + (novf + 31) / 32;
+        // per bucket: lane L takes entries (L / NBK) + g * LPB of bucket L % NBK in round g
+        constexpr int LPB = 32 / NBK;   // lanes per bucket
+        const int mycnt = B::DENSE ? 0 : min(S->cnt[lane % NBK], CAP);
+        const int nbr = (ntask + LPB - 1) / LPB;   // per-bucket rounds
+        const int total = B::DENSE ? (ntask + 31) / 32 : nbr + (novf + 31) / 32;
         for (;;) {
             int g = 0;
             if (lane == 0) g = atomicAdd(&S->meta[7], 1);
@@ -916,10 +926,11 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + NPREP) * 32, 1)
             int t = -1;
             if constexpr (B::DENSE) {
                 if (g * 32 + lane < ntask) t = S->task[g * 32 + lane];
-            } else if (g < ntask) {
-                if (g < mycnt) t = S->task[g * 32 + lane];
+            } else if (g < nbr) {
+                const int e = g * LPB + lane / NBK;
+                if (e < mycnt) t = S->task[e * NBK + lane % NBK];
             } else {
-                const int q = (g - ntask) * 32 + lane;
+                const int q = (g - nbr) * 32 + lane;
                 if (q < novf) t = S->ovf[q];
             }
             if (t >= 0) {
