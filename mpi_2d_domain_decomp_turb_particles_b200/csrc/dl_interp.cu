@@ -729,9 +729,17 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + NPREP) * 32, 1)
             const int col = it % ncol;
             const int cx = col % ncx, cy = col / ncx;
             const unsigned npl = (unsigned)seg_planes(za, zb);
-            for (int zp = za; zp < zb; zp += PZ) {
-                const int zq = min(zp + PZ, zb);
-                const int kd0 = A.brick_start[col * n + zp], kd1 = A.brick_start[col * n + zq];
+            for (int zp = za, zq = za; zp < zb; zp = zq) {
+                // a batch takes up to PZ planes, as many as keep it within MAXD droplets (at
+                // least one; a plane of more droplets is cut into batches of MAXD), so where
+                // droplets gather the batches get shorter instead of leaving a small remainder
+                const int kd0 = A.brick_start[col * n + zp];
+                {
+                    const int zmax = min(zp + PZ, zb), z = zp + 1 + lane;
+                    const bool fits = z <= zmax && A.brick_start[col * n + z] - kd0 <= MAXD;
+                    zq = zp + max(1, __popc(__ballot_sync(0xffffffffu, fits)));   // counts grow with z
+                }
+                const int kd1 = A.brick_start[col * n + zq];
                 const unsigned uhi = useg + (unsigned)(zq - za) + 6u;   // last plane of the window
                 // planes no later batch needs: up to the next batch's window, or the item's end
                 const int rel_hi = (int)(zq < zb ? useg + (unsigned)(zq - za) : useg + npl);
