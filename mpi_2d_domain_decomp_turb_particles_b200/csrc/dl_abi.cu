@@ -478,7 +478,7 @@ static int allocate_state(dl_ctx *c)
     ALLOC(c->remove_dev, sizeof(int) * c->remove_cap);
     ALLOC(c->pair_buf, sizeof(double) * 16 * c->pair_cap);
     ALLOC(c->pair_ibuf, sizeof(int) * 8 * c->pair_cap);
-    ALLOC(c->mv_acc, sizeof(double) * (11 * 10 + 16));
+    ALLOC(c->mv_acc, sizeof(double) * (11 * 10 + 16 + 1024 * 44));   // sums, radii, blocks' partial sums
     c->ovl_cap = std::max(4096, c->msize / 16);
     ALLOC(c->ovl_list, sizeof(int2) * c->ovl_cap);
     ALLOC(c->ovl_cnt, sizeof(int));

@@ -1178,33 +1178,76 @@ __global__ void k_convert_field(const double *v, int64_t py, int64_t pz, int n, 
 }
 
 // MEAN_VEL partial sums (partlib.f90:1910-1930) -> 11*nset doubles via FP64 atomics.
+// MEAN_VEL's eleven sums per radius set (partlib.f90:1889-1980): sum, sum of squares and
+// sum of magnitudes of each component, then of |(u_y, u_z)| and |u|.  Each thread adds its
+// droplets (a grid-stride range) into registers for kMvSets sets at a time, the block adds
+// its threads in a fixed order (warp butterflies, then the warps in order) and writes its
+// partial sums, and k_mean_vel_sum adds the blocks in order: no atomics, and the result does
+// not depend on the timing.
+constexpr int kMvSets = 4;         // sets per pass (nset up to 10: up to three passes)
+constexpr int kMvGridMax = 1024;   // blocks of the partial sums
+constexpr int kMvQ = 11;
+
 template <typename T>
-__global__ void k_mean_vel(int nps, const T *ux, const T *uy, const T *uz, const double *rad, int nset,
-                           const double *radius, double *acc)
+__global__ void __launch_bounds__(256) k_mean_vel(int nps, const T *ux, const T *uy, const T *uz, const double *rad,
+                                                  int nset, const double *radius, int set_lo, double *part)
 {
-    __shared__ double sacc[110];
-    for (int i = threadIdx.x; i < 11 * nset; i += blockDim.x) sacc[i] = 0.0;
-    __syncthreads();
-    int d = blockIdx.x * blockDim.x + threadIdx.x;
-    if (d < nps) {
-        double a = rad[d], dmin = 100.0;
-        int idp = 1;
-        for (int ij = 1; ij <= nset; ij++) {
-            double dd = fabs(a - radius[ij - 1]);
+    double acc[kMvQ][kMvSets];
+#pragma unroll
+    for (int q = 0; q < kMvQ; q++)
+#pragma unroll
+        for (int s = 0; s < kMvSets; s++) acc[q][s] = 0.0;
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nps; d += gridDim.x * blockDim.x) {
+        const double a = rad[d];
+        double dmin = 100.0;
+        int idp = 0;   // nearest set (the first of equals), as the reference picks it
+        for (int ij = 0; ij < nset; ij++) {
+            const double dd = fabs(a - radius[ij]);
             if (dd < dmin) { dmin = dd; idp = ij; }
         }
-        double u[3] = {(double)ux[d], (double)uy[d], (double)uz[d]};
-        for (int c = 0; c < 3; c++) {
-            atomicAdd(&sacc[c + 3 * (idp - 1)], u[c]);
-            atomicAdd(&sacc[3 * nset + c + 3 * (idp - 1)], u[c] * u[c]);
-            atomicAdd(&sacc[6 * nset + c + 3 * (idp - 1)], fabs(u[c]));
-        }
-        atomicAdd(&sacc[9 * nset + idp - 1], sqrt(u[1] * u[1] + u[2] * u[2]));
-        atomicAdd(&sacc[10 * nset + idp - 1], sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]));
+        const int s = idp - set_lo;
+        if (s < 0 || s >= kMvSets) continue;
+        const double u0 = (double)ux[d], u1 = (double)uy[d], u2 = (double)uz[d];
+        const double v[kMvQ] = {u0, u1, u2, u0 * u0, u1 * u1, u2 * u2, fabs(u0), fabs(u1), fabs(u2),
+                                sqrt(u1 * u1 + u2 * u2), sqrt(u0 * u0 + u1 * u1 + u2 * u2)};
+#pragma unroll
+        for (int q = 0; q < kMvQ; q++)
+#pragma unroll
+            for (int ss = 0; ss < kMvSets; ss++)
+                if (ss == s) acc[q][ss] += v[q];
     }
+    __shared__ double ws[8][kMvQ * kMvSets];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < kMvQ; q++)
+#pragma unroll
+        for (int ss = 0; ss < kMvSets; ss++) {
+            double t = acc[q][ss];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == 0) ws[w][q * kMvSets + ss] = t;
+        }
     __syncthreads();
-    for (int i = threadIdx.x; i < 11 * nset; i += blockDim.x)
-        if (sacc[i] != 0.0) atomicAdd(&acc[i], sacc[i]);
+    if (threadIdx.x < kMvQ * kMvSets) {
+        double t = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += ws[k][threadIdx.x];
+        part[(int64_t)blockIdx.x * (kMvQ * kMvSets) + threadIdx.x] = t;
+    }
+}
+
+// The blocks' partial sums in block order, into the reference's layout of the sums:
+// [0, 3 nset) sums, [3 nset, 6 nset) squares, [6 nset, 9 nset) magnitudes, 9 nset + set
+// |(u_y, u_z)|, 10 nset + set |u|.
+__global__ void k_mean_vel_sum(int nblk, int nset, int set_lo, const double *part, double *acc)
+{
+    const int i = threadIdx.x;
+    if (i >= kMvQ * kMvSets) return;
+    const int q = i / kMvSets, set = set_lo + i % kMvSets;
+    if (set >= nset) return;
+    double t = 0.0;
+    for (int b = 0; b < nblk; b++) t += part[(int64_t)b * (kMvQ * kMvSets) + i];
+    const int o = q < 9 ? (q / 3) * 3 * nset + q % 3 + 3 * set : q * nset + set;
+    acc[o] = t;
 }
 
 // Column sweep configuration per precision (columns of ColGeo<T>::CX x CY cells): a ring
@@ -1611,11 +1654,16 @@ static int mean_vel_t(dl_ctx *c, double *host_out)
     DL_CUDA(c, cudaMemsetAsync(c->mv_acc, 0, sizeof(double) * 11 * nset, c->stream));
     if (c->nps > 0) {
         double *rad_d = c->mv_acc + 11 * 10;
+        double *part = c->mv_acc + 11 * 10 + 16;   // kMvGridMax blocks' partial sums
         DL_CUDA(c, cudaMemcpyAsync(rad_d, c->dc.radius, sizeof(double) * 10, cudaMemcpyHostToDevice, c->stream));
-        k_mean_vel<T><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(
-            c->nps, tp<T>(c->vel[c->vcur][0]), tp<T>(c->vel[c->vcur][1]), tp<T>(c->vel[c->vcur][2]), c->rad, nset,
-            rad_d, c->mv_acc);
-        DL_CHECK_LAUNCH(c);
+        const int nblk = std::min(kMvGridMax, std::min(2 * c->num_sms, dl_blocks(c->nps, 256)));
+        for (int lo = 0; lo < nset; lo += kMvSets) {
+            k_mean_vel<T><<<nblk, 256, 0, c->stream>>>(c->nps, tp<T>(c->vel[c->vcur][0]), tp<T>(c->vel[c->vcur][1]),
+                                                        tp<T>(c->vel[c->vcur][2]), c->rad, nset, rad_d, lo, part);
+            DL_CHECK_LAUNCH(c);
+            k_mean_vel_sum<<<1, 64, 0, c->stream>>>(nblk, nset, lo, part, c->mv_acc);
+            DL_CHECK_LAUNCH(c);
+        }
     }
     DL_CUDA(c, cudaMemcpyAsync(host_out, c->mv_acc, sizeof(double) * 11 * nset, cudaMemcpyDeviceToHost, c->stream));
     DL_CUDA(c, cudaStreamSynchronize(c->stream));

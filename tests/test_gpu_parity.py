@@ -268,9 +268,11 @@ def test_mixed_trajectories_close_to_fp64():
     assert np.abs(s["yp"][:, :3] - ref[:, :3]).max() < 1e-7
 
 
-def test_mean_vel_matches_oracle():
+@pytest.mark.parametrize("radii", [[20.0, 30.0], [10.0, 15.0, 20.0, 25.0, 30.0, 35.0, 40.0]])
+def test_mean_vel_matches_oracle(radii):
+    """Two sets (one pass of the per-set sums) and seven sets (two passes)."""
     n = 32
-    g, o = make(dense_params(n=n, npart=4000))
+    g, o = make(dense_params(n=n, npart=4000, radius_um=radii))
     f = smooth_field(n)
     g.set_fields(*f)
     for _ in range(3):
@@ -278,6 +280,8 @@ def test_mean_vel_matches_oracle():
         o.update_step(*f)
         o.periodic()
     assert np.allclose(g.mean_vel(), o.mean_vel(), rtol=1e-12, atol=1e-14)
+    for _ in range(2):   # repeated calls: the same sums, bit for bit
+        assert np.array_equal(g.mean_vel(), g.mean_vel())
 
 
 def test_device_resort_is_invisible():
