@@ -860,6 +860,7 @@ __global__ void __launch_bounds__(1024) k_lv_reorder(int n, int *lv_list, int *l
         if (threadIdx.x < kraw) {
             const int v = sP[threadIdx.x];
             int rank = 0;
+#pragma unroll 8
             for (int j = 0; j < kraw; j++) {
                 const int u = sP[j];
                 rank += (u < v) || (u == v && j < (int)threadIdx.x);
