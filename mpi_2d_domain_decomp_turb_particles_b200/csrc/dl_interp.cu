@@ -1506,7 +1506,8 @@ static int launch_interp_col(dl_ctx *c, int comp_lo, int ncomp, int fused)
                                  (int)cudaSharedmemCarveoutMaxShared);
             carve = true;
         }
-        k_advance_fused<T><<<dl_blocks(c->nps, 256), 256, 0, c->stream>>>(E);
+        // blocks of 128 measured a little faster than 256 or 512 (33.0 against 33.8 us at 1M)
+        k_advance_fused<T><<<dl_blocks(c->nps, 128), 128, 0, c->stream>>>(E);
         DL_CHECK_LAUNCH(c);
     }
     return 0;
