@@ -1491,12 +1491,19 @@ extern "C" int dl_coalesce(dl_ctx *c)
         DL_CHECK_LAUNCH(c);
         DL_CUDA(c, cudaStreamSynchronize(c->stream));   // the host vectors are temporaries
     }
-    // deleted droplets (radius -1) are dropped by a compacting re-sort, which also rebuilds
-    // dev_of_ref from ref_of_dev
-    c->has_dead = jj > 0;
-    r = launch_brick_sort(c);
-    if (r) return r;
-    c->nps = newn;
+    // deleted droplets (radius -1) are dropped by moving the tail's survivors into their
+    // slots, which also rebuilds dev_of_ref from ref_of_dev
+    std::vector<int> dead;
+    for (auto &kv : setrad)
+        if (kv.second < 0.0) dead.push_back(kv.first);
+    if ((int)dead.size() != jj) return dl_fail(c, DL_E_STATE, "COALESCE: deleted droplets miscounted");
+    if (jj > 0) {
+        int *d = static_cast<int *>(co_scratch(c, sizeof(int) * 2 * jj));
+        if (!d) return dl_fail(c, DL_E_ALLOC, "COALESCE: cudaMalloc failed");
+        r = launch_compact(c, dead, d);
+        if (r) return r;
+    }
+    if (c->nps != newn) return dl_fail(c, DL_E_STATE, "COALESCE: droplet count after compaction");
     return 0;
 }
 

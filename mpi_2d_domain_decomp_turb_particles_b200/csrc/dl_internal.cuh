@@ -323,6 +323,7 @@ __global__ void k_rad_max(int n, const double *rad, unsigned long long *out)
 // ---------------------------------------------------------------------------------------
 // dl_interp.cu
 int launch_brick_sort(dl_ctx *c);
+int launch_compact(dl_ctx *c, const std::vector<int> &dead, int *scratch);
 int launch_interp(dl_ctx *c, int icpt_or_all, int fused);
 int launch_prepare_interp(dl_ctx *c);
 int launch_history_fvp(dl_ctx *c);

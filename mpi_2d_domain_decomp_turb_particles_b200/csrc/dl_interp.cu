@@ -1282,6 +1282,96 @@ T *tp(void *p) { return reinterpret_cast<T *>(p); }
 // =======================================================================================
 // Launchers
 // =======================================================================================
+// Every per-droplet array that lives from one step to the next, with its shadow buffer:
+// f(array pointer, shadow pointer, element size)
+template <class F>
+static void for_each_droplet_array(dl_ctx *c, F &&f)
+{
+    const size_t es = (size_t)c->esz;
+    for (int k = 0; k < 3; k++) {
+        f((void **)&c->pos[c->pcur][k], (void **)&c->sh_pos[c->pcur][k], (size_t)8);
+        for (int l = 0; l < 3; l++) f(&c->vel[(c->vcur + l) % 4][k], &c->sh_vel[(c->vcur + l) % 4][k], es);
+        for (int l = 0; l < 3; l++) f(&c->flu[(c->fcur + l) % 4][k], &c->sh_flu[(c->fcur + l) % 4][k], es);
+        f(&c->vpv[k], &c->sh_vpv[k], es);
+        f(&c->dmv[k], &c->sh_dmv[k], es);
+        if (c->pert[k]) f(&c->pert[k], &c->sh_pert[k], es);
+    }
+    f((void **)&c->rad, (void **)&c->sh_rad, (size_t)8);
+    f((void **)&c->gid, (void **)&c->sh_gid, (size_t)8);
+    f((void **)&c->ref_of_dev, (void **)&c->sh_ref, (size_t)4);
+}
+
+// Droplet `from[q]` of every array moves to slot `to[q]` (the slots of one call disjoint)
+__global__ void k_move_slots(int k, const int *from, const int *to, PermTable t)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= k) return;
+    const int f = from[q], h = to[q];
+    for (int a = 0; a < t.n8; a++) t.d8[a][h] = t.a8[a][f];
+    for (int a = 0; a < t.n4; a++) t.d4[a][h] = t.a4[a][f];
+}
+
+__global__ void k_clamp_starts(int nb, int *start, int n)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b <= nb && start[b] > n) start[b] = n;
+}
+
+// COALESCE's deletions without a re-sort: the deleted droplets (device slots, ascending,
+// radius already -1 and reference -1) below the new count take, in order, the surviving
+// droplets of the tail [n - k, n); the brick ranges are cut at the new count, and the moved
+// droplets stay outside their columns until the next periodic re-sort (the sweep evaluates
+// such droplets from the field in global memory).  dev_of_ref is rebuilt.  One small
+// gather of index pairs replaces the re-sort's pass over every droplet.
+int launch_compact(dl_ctx *c, const std::vector<int> &dead, int *scratch)
+{
+    const int n = c->nps, k = (int)dead.size(), newn = n - k;
+    std::vector<int> from, to;
+    {
+        size_t t = 0;   // dead is ascending: the dead slots of the tail are its last entries
+        std::vector<int> tail_live;
+        int di = (int)(std::lower_bound(dead.begin(), dead.end(), newn) - dead.begin());
+        for (int d = newn; d < n; d++) {
+            if (di < k && dead[di] == d) { di++; continue; }
+            tail_live.push_back(d);
+        }
+        for (int q = 0; q < k && dead[q] < newn; q++) {
+            if (t >= tail_live.size()) return dl_fail(c, DL_E_STATE, "COALESCE: compaction bookkeeping");
+            to.push_back(dead[q]);
+            from.push_back(tail_live[t++]);
+        }
+        if (t != tail_live.size()) return dl_fail(c, DL_E_STATE, "COALESCE: compaction bookkeeping");
+    }
+    const int m = (int)from.size();
+    if (m > 0) {
+        DL_CUDA(c, cudaMemcpyAsync(scratch, from.data(), sizeof(int) * m, cudaMemcpyHostToDevice, c->stream));
+        DL_CUDA(c, cudaMemcpyAsync(scratch + m, to.data(), sizeof(int) * m, cudaMemcpyHostToDevice, c->stream));
+        PermTable tb;
+        memset(&tb, 0, sizeof(tb));
+        for_each_droplet_array(c, [&](void **arr, void **, size_t esz) {
+            if (esz == 8) {
+                tb.a8[tb.n8] = (const unsigned long long *)*arr;
+                tb.d8[tb.n8++] = (unsigned long long *)*arr;
+            } else {
+                tb.a4[tb.n4] = (const unsigned int *)*arr;
+                tb.d4[tb.n4++] = (unsigned int *)*arr;
+            }
+        });
+        k_move_slots<<<dl_blocks(m, 128), 128, 0, c->stream>>>(m, scratch, scratch + m, tb);
+        DL_CHECK_LAUNCH(c);
+    }
+    c->nps = newn;
+    k_clamp_starts<<<dl_blocks(c->nbricks + 1, 256), 256, 0, c->stream>>>(c->nbricks, c->brick_start, newn);
+    DL_CHECK_LAUNCH(c);
+    if (newn > 0) {
+        k_inverse<<<dl_blocks(newn, 256), 256, 0, c->stream>>>(newn, c->ref_of_dev, c->dev_of_ref);
+        DL_CHECK_LAUNCH(c);
+    }
+    c->hl_valid = 0;
+    DL_CUDA(c, cudaStreamSynchronize(c->stream));   // the index vectors are host temporaries
+    return 0;
+}
+
 int launch_brick_sort(dl_ctx *c)
 {
     const int nps = c->nps;
@@ -1354,18 +1444,7 @@ int launch_brick_sort(dl_ctx *c)
         }
         swaps.emplace_back(arr, sh);
     };
-    const size_t es = (size_t)c->esz;
-    for (int k = 0; k < 3; k++) {
-        add((void **)&c->pos[c->pcur][k], (void **)&c->sh_pos[c->pcur][k], 8);
-        for (int l = 0; l < 3; l++) add(&c->vel[(c->vcur + l) % 4][k], &c->sh_vel[(c->vcur + l) % 4][k], es);
-        for (int l = 0; l < 3; l++) add(&c->flu[(c->fcur + l) % 4][k], &c->sh_flu[(c->fcur + l) % 4][k], es);
-        add(&c->vpv[k], &c->sh_vpv[k], es);
-        add(&c->dmv[k], &c->sh_dmv[k], es);
-        if (c->pert[k]) add(&c->pert[k], &c->sh_pert[k], es);
-    }
-    add((void **)&c->rad, (void **)&c->sh_rad, 8);
-    add((void **)&c->gid, (void **)&c->sh_gid, 8);
-    add((void **)&c->ref_of_dev, (void **)&c->sh_ref, 4);
+    for_each_droplet_array(c, add);
     k_permute_gather<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, perm, tb);
     DL_CHECK_LAUNCH(c);
     for (auto &sw : swaps) std::swap(*sw.first, *sw.second);
