@@ -726,7 +726,6 @@ static int upload_t(dl_ctx *c, int nps, const double *yp, const double *fvp, con
     DL_CUDA(c, cudaFreeAsync(buf, c->stream));
     c->nps = nps;
     c->vp_slot = -1;
-    c->has_dead = 0;
     c->have_vnew = c->have_fnew = c->have_dmove = 0;
     c->hl_valid = 0;
     return launch_brick_sort(c);
@@ -1410,7 +1409,8 @@ static int pert_keep(dl_ctx *c, const std::vector<int> &src, const std::vector<i
 // COALESCE (partlib.f90:3642-3825): the reference's swap-with-last bookkeeping over the
 // collided pairs, run on the host over the few reference positions it touches (looked up
 // on the device), then applied to the device state: new radii and terminal velocities,
-// renumbered reference indices, deleted droplets dropped by a compacting re-sort.
+// renumbered reference indices, deleted droplets replaced in place by the survivors of the
+// device order's tail.
 // pertvel stays at its reference index (COALESCE moves yp, vp, dmove, fvp, fdp only,
 // partlib.f90:3676-3728).
 extern "C" int dl_coalesce(dl_ctx *c)

@@ -90,7 +90,6 @@ struct dl_ctx {
     int fcur, fnew;
     void *vpv[3];                // vp (interpolated fluid velocity) when vp_slot < 0
     int vp_slot;                 // >= 0: vp lives in the fluid-velocity ring slot flu[vp_slot]
-    int has_dead;                // COALESCE removed droplets: the next re-sort compacts
     void *dmv[3];                // dmove
     void *pert[3];               // HDI disturbance velocity
     double *rad, *gid;           // yp(7), yp(8)

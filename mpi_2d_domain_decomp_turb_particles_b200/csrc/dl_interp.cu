@@ -968,16 +968,10 @@ __global__ void __launch_bounds__((NSW + colk::NPROD + 1 + NPREP) * 32, 1)
 }
 
 __global__ void k_brick_keys(int nps, const double *px, const double *py, const double *pz, double dx, int n,
-                             int bx, int by, int bz, int nbx, int nby, int nbz, int colmajor, int *keys, int *cnt,
-                             const double *rad, int dead_key)
+                             int bx, int by, int bz, int nbx, int nby, int nbz, int colmajor, int *keys, int *cnt)
 {
     int d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= nps) return;
-    if (dead_key >= 0 && rad[d] < 0.0) {   // removed by COALESCE: sorted past the last brick
-        keys[d] = dead_key;
-        atomicAdd(&cnt[dead_key], 1);
-        return;
-    }
     int ix = (int)floor(px[d] / dx), iy = (int)floor(py[d] / dx), iz = (int)floor(pz[d] / dx);
     ix = min(max(ix, 0), n - 1);
     iy = min(max(iy, 0), n - 1);
@@ -1382,12 +1376,12 @@ int launch_brick_sort(dl_ctx *c)
         return 0;
     }
     const int t = 256;
-    const int nkeys = c->nbricks + (c->has_dead ? 1 : 0);
+    const int nkeys = c->nbricks;
     DL_CUDA(c, cudaMemsetAsync(c->brick_cnt, 0, sizeof(int) * nkeys, c->stream));
     const double *P[3] = {c->pos[c->pcur][0], c->pos[c->pcur][1], c->pos[c->pcur][2]};
     k_brick_keys<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, P[0], P[1], P[2], c->dc.dx, c->dc.n, c->bx, c->by,
                                                          c->bz, c->nbx, c->nby, c->nbz, c->bz == 1, c->keys,
-                                                         c->brick_cnt, c->rad, c->has_dead ? c->nbricks : -1);
+                                                         c->brick_cnt);
     DL_CHECK_LAUNCH(c);
     {
         const int r = dl_scan(c, c->brick_cnt, c->brick_start, nkeys);   // multi-block exclusive scan
@@ -1448,14 +1442,6 @@ int launch_brick_sort(dl_ctx *c)
     k_permute_gather<<<dl_blocks(nps, t), t, 0, c->stream>>>(nps, perm, tb);
     DL_CHECK_LAUNCH(c);
     for (auto &sw : swaps) std::swap(*sw.first, *sw.second);
-    if (c->has_dead) {
-        int live = 0;
-        DL_CUDA(c, cudaMemcpyAsync(&live, c->brick_start + c->nbricks, sizeof(int), cudaMemcpyDeviceToHost,
-                                   c->stream));
-        DL_CUDA(c, cudaStreamSynchronize(c->stream));
-        c->nps = live;
-        c->has_dead = 0;
-    }
     k_inverse<<<dl_blocks(c->nps, t), t, 0, c->stream>>>(c->nps, c->ref_of_dev, c->dev_of_ref);
     DL_CHECK_LAUNCH(c);
     c->hl_valid = 0;
