@@ -1250,7 +1250,8 @@ __global__ void k_mean_vel_sum(int nblk, int nset, int set_lo, const double *par
 // most (PZ + 9) / SPL + 1 slabs, which must leave the ring a slab to fill ahead.  Measured at
 // 256^3 / 1M droplets: two prep warps keep twelve FP32 stencil warps fed (three prep and
 // eleven stencil warps were 2 % slower); FP64 gains 6 % from the eleventh two-plane slab
-// against ten (three batch slots instead of four pay for it).
+// against ten (three batch slots instead of four pay for it), and 4 % from batches of up
+// to seven planes against six (eight: 4 % slower) now that batches stop at MAXD droplets.
 template <typename T>
 struct ColCfg;
 template <>
@@ -1259,7 +1260,7 @@ struct ColCfg<float> {
 };
 template <>
 struct ColCfg<double> {
-    static constexpr int NSL = 11, PZ = 6, MAXD = 64, NP = 3, NSW = 10, NPREP = 3;
+    static constexpr int NSL = 11, PZ = 7, MAXD = 64, NP = 3, NSW = 10, NPREP = 3;
 };
 template <typename T>
 constexpr bool col_cfg_ok()
