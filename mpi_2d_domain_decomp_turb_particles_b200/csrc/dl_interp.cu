@@ -1251,12 +1251,13 @@ __global__ void k_mean_vel_sum(int nblk, int nset, int set_lo, const double *par
 // 256^3 / 1M droplets: two prep warps keep twelve FP32 stencil warps fed (three prep and
 // eleven stencil warps were 2 % slower); FP64 gains 6 % from the eleventh two-plane slab
 // against ten (three batch slots instead of four pay for it), and 4 % from batches of up
-// to seven planes against six (eight: 4 % slower) now that batches stop at MAXD droplets.
+// to seven planes against six (eight: 4 % slower) now that batches stop at MAXD droplets;
+// FP32 2 % from nine planes against eight (ten: 3 % slower).
 template <typename T>
 struct ColCfg;
 template <>
 struct ColCfg<float> {
-    static constexpr int NSL = 7, PZ = 8, MAXD = 160, NP = 4, NSW = 12, NPREP = 2;
+    static constexpr int NSL = 7, PZ = 9, MAXD = 160, NP = 4, NSW = 12, NPREP = 2;
 };
 template <>
 struct ColCfg<double> {
